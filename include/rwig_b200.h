@@ -1,0 +1,87 @@
+/* rwig_b200.h -- C ABI of the B200 (sm_100a) engine for rwig's entropic-OT path.
+ *
+ * Drop-in replacement for the GPU entry points that rwig's Rcpp glue calls
+ * (inst/include/cuda_interface.cuh:13-39), plus the log-domain and gradient
+ * entries that the reference only has on the CPU.  Every function:
+ *   - takes plain pointers, sizes and scalars (no C++ or framework types);
+ *   - uses column-major FP64 arrays with R's layout (X[i + j*rows]);
+ *   - never throws, never calls R, never prints;
+ *   - returns >= 0 on success, namely the reference's `return_status`
+ *     (0: err <= zero_tol, 1: max_iter reached, 2: otherwise; src/sinkhorn.cpp:88-95),
+ *     or a negative RWIG_E_* code on failure, with a message in rwig_last_error().
+ * Calls are blocking and serialised per device; they may be made from any host
+ * thread.  Host-pointer entries copy inputs in and results out themselves; the
+ * *_dev entries take device pointers (inputs resident in HBM) and a CUDA stream.
+ */
+#ifndef RWIG_B200_H
+#define RWIG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RWIG_B200_VERSION 100
+
+#if defined(__GNUC__)
+#define RWIG_API __attribute__((visibility("default")))
+#else
+#define RWIG_API
+#endif
+
+/* error codes (negative return values) */
+#define RWIG_E_INVALID     (-1) /* bad argument (size, pointer, reg <= 0, ...) */
+#define RWIG_E_CUDA        (-2) /* a CUDA runtime call failed */
+#define RWIG_E_NODEVICE    (-3) /* no usable sm_100 device */
+#define RWIG_E_NOMEM       (-4) /* device allocation failed or admission refused */
+#define RWIG_E_TIMEOUT     (-5) /* a bounded device-side wait expired */
+#define RWIG_E_UNSUPPORTED (-6) /* shape outside what this build supports */
+#define RWIG_E_BUSY        (-7) /* server queue full */
+
+/* Per-call report, filled by every solve (see rwig_last_report). */
+typedef struct rwig_report {
+  int iter;              /* iterations run */
+  int status;            /* reference return_status (0/1/2) */
+  double err;            /* stopping error of the last iteration */
+  double marg_l1_row;    /* || P 1 - a ||_1     (barycenters: || U o KV - A ||_1) */
+  double marg_l1_col;    /* || P^T 1 - b ||_1   (barycenters: 0) */
+  double marg_l2_row;    /* || P 1 - a ||_2 */
+  double marg_l2_col;    /* || P^T 1 - b ||_2 */
+  double device_ms;      /* device time of the whole call (CUDA events) */
+  double kernel_ms;      /* device time of the main solver kernel alone */
+  int fallback_events;   /* sweeps re-run with exact per-row / per-column minima */
+  int kernel_launches;   /* engine kernels launched by the call */
+  int support_m;         /* rows kept after dropping zero-mass entries of a */
+  int support_n;         /* columns kept after dropping zero-mass entries of b */
+} rwig_report;
+
+/* ---- context ---------------------------------------------------------- */
+RWIG_API int rwig_init(int device);            /* optional; the first call initialises device 0 */
+RWIG_API void rwig_shutdown(void);             /* frees all device memory held by the engine */
+RWIG_API const char* rwig_last_error(void);    /* message of the last failure on this thread */
+RWIG_API int rwig_version(void);
+RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on this thread */
+
+/* ---- log-stabilised Sinkhorn ------------------------------------------
+ * Replaces the CPU-only Sinkhorn::compute_log (src/sinkhorn_impl_log.cpp:225)
+ * reached from sinkhorn_log_cpp (src/sinkhorn.cpp:142); the reference has no
+ * GPU entry for it (inst/include/cuda_interface.cuh:41, "TODO").
+ * a: M, b: N, C: M x N.  Outputs (any may be NULL): P (M x N), grad_a (M,
+ * needs withgrad), f (M), g (N; -inf off the support, as :267-270), loss.
+ */
+RWIG_API int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g, double* loss,
+                      int* iter, double* err, const double* a, const double* b,
+                      const double* C, int M, int N, double reg, int withgrad,
+                      int max_iter, double zero_tol);
+
+/* Same, with every array a device pointer (C with leading dimension M) and the
+ * work queued on `stream` (a cudaStream_t, NULL = the engine's stream).
+ * loss / iter / err are host pointers, written before the call returns. */
+RWIG_API int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, double* g, double* loss,
+                          int* iter, double* err, const double* a, const double* b,
+                          const double* C, int M, int N, double reg, int withgrad,
+                          int max_iter, double zero_tol, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RWIG_B200_H */

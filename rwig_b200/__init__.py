@@ -1,0 +1,11 @@
+"""rwig_b200 -- B200-native (sm_100a) engine for rwig's entropic optimal transport.
+
+Public Python surface (mirrors rwig's R API over the C ABI in include/rwig_b200.h):
+    sinkhorn(a, b, C, sinkhorn_control)
+The compute path is the CUDA library rwig_b200/librwig_b200.so; importing this
+package does not load it until the first call.
+"""
+from ._lib import RwigError, last_report, load  # noqa: F401
+from .api import check_sinkhorn_args, choose_sinkhorn_method, sinkhorn, sinkhorn_log_device  # noqa: F401
+
+__all__ = ["sinkhorn", "sinkhorn_log_device", "RwigError", "last_report", "load"]

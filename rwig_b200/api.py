@@ -1,0 +1,133 @@
+"""R-facing API of rwig, restated over the engine's C ABI.
+
+`sinkhorn()` mirrors rwig's R function of the same name (R/sinkhorn.R:85-181):
+same control list, defaults, validation messages, automatic method choice and
+result fields.  The compute goes through include/rwig_b200.h; there is no CPU
+path here.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import RwigError
+
+SINKHORN_ARGS = ("reg", "with_grad", "use_cuda", "n_threads", "method", "threshold", "max_iter",
+                 "zero_tol", "verbose")
+
+
+def check_sinkhorn_args(ctrl: dict | None) -> dict:
+    """Fill and validate a sinkhorn control list (R/check_args.R:108-189)."""
+    ctrl = dict(ctrl or {})
+    bad = [k for k in ctrl if k not in SINKHORN_ARGS]
+    if bad:
+        raise ValueError(", ".join(bad) + " not matching one of the sinkhorn arguments: " +
+                         ", ".join(f'"{a}"' for a in SINKHORN_ARGS))
+    defaults = dict(reg=0.1, with_grad=False, use_cuda=True, n_threads=0, method="auto",
+                    threshold=0.1, max_iter=1000, zero_tol=1e-6, verbose=10)
+    for k, v in defaults.items():
+        if ctrl.get(k) is None:
+            ctrl[k] = v
+    if ctrl["method"] not in ("auto", "vanilla", "log"):
+        raise ValueError('method must be from: "auto", "vanilla", or "log"')
+    return ctrl
+
+
+def choose_sinkhorn_method(C: np.ndarray, reg: float, threshold: float) -> str:
+    """The "auto" rule of R/sinkhorn.R:124-142."""
+    k1 = math.exp(-float(np.min(C)) / reg)
+    k2 = math.exp(-float(np.max(C)) / reg)
+    return "log" if min(k1, k2) < threshold else "vanilla"
+
+
+def _vec(x, name):
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim != 1:
+        raise ValueError(f"{name} must be a numeric vector!")
+    return np.ascontiguousarray(a)
+
+
+def _mat(x, name):
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError(f"{name} must be a numeric matrix!")
+    return np.asfortranarray(a)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def sinkhorn(a, b, C, sinkhorn_control: dict | None = None) -> dict:
+    """Entropic OT between histograms a and b under cost C (R/sinkhorn.R:85)."""
+    a = _vec(a, "a")
+    b = _vec(b, "b")
+    C = _mat(C, "C")
+    if a.shape[0] != C.shape[0] or b.shape[0] != C.shape[1]:
+        raise ValueError("a, b, C don't match in dimension!")
+    ctrl = check_sinkhorn_args(sinkhorn_control)
+    reg = ctrl["reg"]
+    if not isinstance(reg, (int, float)) or isinstance(reg, bool):
+        raise ValueError("reg must be a single value")
+    reg = float(reg)
+    method = ctrl["method"]
+    if method == "auto":
+        method = choose_sinkhorn_method(C, reg, ctrl["threshold"])
+    M, N = C.shape
+    with_grad = bool(ctrl["with_grad"])
+    P = np.zeros((M, N), order="F")
+    x, y = np.zeros(M), np.zeros(N)
+    ga = np.zeros(M) if with_grad else None
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    L = _lib.load()
+    if method == "log":
+        rc = L.rwig_sinkhorn_log(_dp(P), _dp(ga), _dp(x), _dp(y), ctypes.byref(loss), ctypes.byref(it),
+                                 ctypes.byref(err), _dp(a), _dp(b), _dp(C), M, N, reg, int(with_grad),
+                                 int(ctrl["max_iter"]), float(ctrl["zero_tol"]))
+        names = ("f", "g")
+    else:
+        fn = getattr(L, "rwig_sinkhorn_vanilla", None)
+        if fn is None:
+            raise RwigError(-6, "vanilla Sinkhorn is not available in this build")
+        rc = fn(_dp(P), _dp(ga), _dp(x), _dp(y), ctypes.byref(loss), ctypes.byref(it), ctypes.byref(err),
+                _dp(a), _dp(b), _dp(C), M, N, reg, int(with_grad), int(ctrl["max_iter"]),
+                float(ctrl["zero_tol"]))
+        names = ("u", "v")
+    _lib.check(rc)
+    out = {"P": P}
+    if with_grad:
+        out["grad_a"] = ga
+    out.update({names[0]: x, names[1]: y, "loss": loss.value, "iter": it.value, "err": err.value,
+                "return_status": rc, "method": method})
+    return out
+
+
+# ---------------------------------------------------------------------------
+# device-resident entry points (torch CUDA tensors as plain device buffers)
+# ---------------------------------------------------------------------------
+def _ptr(t):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()):
+        raise ValueError("device buffers must be contiguous float64 CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def sinkhorn_log_device(a, b, C_cm, reg, max_iter=1000, zero_tol=1e-6, P=None, f=None, g=None,
+                        stream=None) -> dict:
+    """Log-Sinkhorn on device buffers.  C_cm is the M x N cost in column-major
+    order, i.e. a contiguous (N, M) tensor holding C^T row-major; P likewise."""
+    M, N = a.shape[0], b.shape[0]
+    if C_cm.numel() != M * N:
+        raise ValueError("C must hold M*N entries")
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+    rc = _lib.load().rwig_sinkhorn_log_dev(_ptr(P), None, _ptr(f), _ptr(g), ctypes.byref(loss),
+                                           ctypes.byref(it), ctypes.byref(err), _ptr(a), _ptr(b),
+                                           _ptr(C_cm), M, N, float(reg), 0, int(max_iter), float(zero_tol),
+                                           st)
+    _lib.check(rc)
+    return {"loss": loss.value, "iter": it.value, "err": err.value, "return_status": rc}

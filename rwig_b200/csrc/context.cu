@@ -1,0 +1,140 @@
+// context.cu -- per-device context, scratch arena and the error / report
+// entry points of the C ABI.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "engine.h"
+
+namespace rwig {
+
+namespace {
+thread_local std::string t_last_error;
+thread_local rwig_report t_report;
+
+std::mutex g_ctx_mu;
+std::vector<std::unique_ptr<Context>> g_ctx;  // indexed by device
+
+int init_device(int dev, Context** out) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return set_error(RWIG_E_NODEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= ndev) return set_error(RWIG_E_INVALID, "device index out of range");
+  if ((int)g_ctx.size() < ndev) g_ctx.resize(ndev);
+  if (!g_ctx[dev]) {
+    auto c = std::make_unique<Context>();
+    c->device = dev;
+    RWIG_CUDA_TRY(cudaSetDevice(dev));
+    cudaDeviceProp prop;
+    RWIG_CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10)
+      return set_error(RWIG_E_NODEVICE, "device is not sm_100 class (this build targets sm_100a)");
+    c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    RWIG_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    RWIG_CUDA_TRY(cudaEventCreate(&c->ev0));
+    RWIG_CUDA_TRY(cudaEventCreate(&c->ev1));
+    RWIG_CUDA_TRY(cudaEventCreate(&c->evk));
+    g_ctx[dev] = std::move(c);
+  }
+  *out = g_ctx[dev].get();
+  return 0;
+}
+}  // namespace
+
+int set_error(int code, const std::string& msg) {
+  t_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s", (int)e, cudaGetErrorString(e), what);
+  t_last_error = buf;
+  return e == cudaErrorMemoryAllocation ? RWIG_E_NOMEM : RWIG_E_CUDA;
+}
+
+rwig_report& report() { return t_report; }
+
+void reset_report() {
+  std::memset(&t_report, 0, sizeof(t_report));
+}
+
+Context* get_context() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  Context* c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (dev < (int)g_ctx.size() && g_ctx[dev]) return g_ctx[dev].get();
+  }
+  if (init_device(dev, &c) != 0) return nullptr;
+  return c;
+}
+
+void* scratch(Context* ctx, int k, size_t bytes) {
+  if ((int)ctx->slots.size() <= k) {
+    ctx->slots.resize(k + 1, nullptr);
+    ctx->slot_bytes.resize(k + 1, 0);
+  }
+  if (ctx->slot_bytes[k] >= bytes && ctx->slots[k]) return ctx->slots[k];
+  if (ctx->slots[k]) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->slots[k]);
+    ctx->slots[k] = nullptr;
+    ctx->slot_bytes[k] = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cuda_fail(e, "cudaMalloc(scratch)");
+    return nullptr;
+  }
+  ctx->slots[k] = p;
+  ctx->slot_bytes[k] = want;
+  return p;
+}
+
+}  // namespace rwig
+
+using namespace rwig;
+
+extern "C" int rwig_init(int device) {
+  Context* c = nullptr;
+  int rc = init_device(device, &c);
+  if (rc != 0) return rc;
+  if (cudaSetDevice(device) != cudaSuccess) return set_error(RWIG_E_CUDA, "cudaSetDevice failed");
+  return 0;
+}
+
+extern "C" void rwig_shutdown(void) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  for (auto& c : g_ctx) {
+    if (!c) continue;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (void* p : c->slots)
+      if (p) cudaFree(p);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaEventDestroy(c->evk);
+    cudaStreamDestroy(c->stream);
+    c.reset();
+  }
+  g_ctx.clear();
+}
+
+extern "C" const char* rwig_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" int rwig_version(void) { return RWIG_B200_VERSION; }
+
+extern "C" int rwig_last_report(rwig_report* out) {
+  if (!out) return RWIG_E_INVALID;
+  *out = t_report;
+  return 0;
+}

@@ -1,0 +1,48 @@
+// engine.h -- host-side plumbing shared by the entry points: per-device
+// context (stream, events, scratch arena), error / report bookkeeping.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rwig_b200.h"
+
+namespace rwig {
+
+struct Context {
+  int device = -1;
+  int sm_count = 0;
+  int smem_optin = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk = nullptr;
+  std::mutex mu;
+  std::vector<void*> slots;
+  std::vector<size_t> slot_bytes;
+  void* pinned = nullptr;  // small pinned staging buffer for scalars
+  size_t pinned_bytes = 0;
+};
+
+// Returns the context of the current (or first) device, initialising it on
+// first use.  nullptr on failure (last error set).
+Context* get_context();
+
+// Grow-only scratch slot `k` of at least `bytes`; nullptr on failure.
+void* scratch(Context* ctx, int k, size_t bytes);
+
+// Error / report plumbing (thread-local).
+int set_error(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+rwig_report& report();
+void reset_report();
+
+#define RWIG_CUDA_TRY(expr)                              \
+  do {                                                   \
+    cudaError_t _e = (expr);                             \
+    if (_e != cudaSuccess) return ::rwig::cuda_fail(_e, #expr); \
+  } while (0)
+
+}  // namespace rwig

@@ -1,0 +1,64 @@
+"""Seeded synthetic inputs for the benchmark workloads (no public dataset is used).
+
+All arrays are FP64.  Each array has its own PCG64 stream:
+    1001 source points, 1002 target points, 1003 a / A, 1004 b,
+    1005 barycentric weights w, 1006 b_ext / document data.
+Histograms are Dirichlet(alpha) draws (normalised Gamma(alpha, 1)).  Costs are
+squared Euclidean distances summed over coordinates in ascending order, then
+divided by their maximum.  Matrices are returned column-major (Fortran order).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SEED_X, SEED_Y, SEED_A, SEED_B, SEED_W, SEED_DOC = 1001, 1002, 1003, 1004, 1005, 1006
+
+
+def rng(seed: int, salt: int = 0) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64([seed, salt]))
+
+
+def dirichlet(g: np.random.Generator, alpha: float, n: int, cols: int | None = None) -> np.ndarray:
+    shape = (n,) if cols is None else (n, cols)
+    x = g.gamma(alpha, 1.0, size=shape)
+    return np.asfortranarray(x / x.sum(axis=0, keepdims=True))
+
+
+def sq_euclid_cost(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """C_ij = sum_k (x_ik - y_jk)^2 accumulated in ascending k, divided by max C."""
+    C = np.zeros((x.shape[0], y.shape[0]), order="F")
+    for k in range(x.shape[1]):
+        d = x[:, k, None] - y[None, :, k]
+        C += d * d
+    C /= C.max()
+    return C
+
+
+def sinkhorn_problem(m: int, n: int, alpha: float, dim: int = 2, salt: int = 0):
+    """Histograms a (m), b (n) ~ Dirichlet(alpha); points uniform in [0,1]^dim."""
+    x = rng(SEED_X, salt).random((m, dim))
+    y = rng(SEED_Y, salt).random((n, dim))
+    a = dirichlet(rng(SEED_A, salt), alpha, m)
+    b = dirichlet(rng(SEED_B, salt), alpha, n)
+    return a, b, sq_euclid_cost(x, y)
+
+
+def vanilla_config(m=256, n=256):
+    """Plain vanilla Sinkhorn: Dirichlet(1) histograms, uniform points in [0,1]^2."""
+    return sinkhorn_problem(m, n, 1.0, 2)
+
+
+def log_config(m=4096, n=4096):
+    """Plain log Sinkhorn: Dirichlet(0.5) histograms, uniform points in [0,1]^2."""
+    return sinkhorn_problem(m, n, 0.5, 2)
+
+
+def barycenter_config(n=2048, S=32, dim=50, salt: int = 0):
+    """Log barycenter: n support points ~ N(0, I_dim), S Dirichlet(0.3) histograms,
+    w ~ Dirichlet(1), b_ext ~ Dirichlet(0.3)."""
+    x = rng(SEED_X, salt).standard_normal((n, dim))
+    C = sq_euclid_cost(x, x)
+    A = dirichlet(rng(SEED_A, salt), 0.3, n, S)
+    w = dirichlet(rng(SEED_W, salt), 1.0, S)
+    b_ext = dirichlet(rng(SEED_DOC, salt), 0.3, n)
+    return A, C, w, b_ext
