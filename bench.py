@@ -25,7 +25,6 @@ import re
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -48,6 +47,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling entry point: one warm-up and one measured solve of a chosen size
+    ap.add_argument("--single", action="store_true")
+    ap.add_argument("--m", type=int, default=M)
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--iters", type=int, default=20)
     return ap.parse_args()
 
 
@@ -67,13 +71,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per solver iteration from the committed ncu summary, if any."""
+def profiled_traffic(passes):
+    """DRAM bytes of one solver launch with `passes` sweeps over C, from the
+    committed ncu summary of a smaller launch of the same kernel (traffic grows
+    in proportion to the passes), or None."""
     p = os.path.join(ROOT, "profiles", "sinkhorn_log_kernel_4096.md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_iteration:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    txt = open(p).read()
+    a = re.search(r"dram_bytes_per_pass:\s*([0-9.eE+]+)", txt)
+    b = re.search(r"dram_bytes_final_plan:\s*([0-9.eE+]+)", txt)
+    if not (a and b):
+        return None
+    return float(a.group(1)) * passes + float(b.group(1))
 
 
 class ClockSampler:
@@ -89,27 +99,29 @@ class ClockSampler:
         self.lines = []
 
     def __enter__(self):
+        import tempfile
+        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)  # let the sampler start before the timed region
         except OSError:
             self.proc = None
         return self
 
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
-
     def __exit__(self, *exc):
         if self.proc is not None:
+            time.sleep(0.3)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        self.fh.close()
+        with open(self.fh.name) as fh:
+            self.lines = [ln.strip() for ln in fh if ln.strip()]
+        os.unlink(self.fh.name)
 
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
@@ -283,9 +295,9 @@ def run_engine(args):
         # final pass that reads C and writes P
         alg_bytes = (it_mean + 2) * M * N * 8
         achieved = alg_bytes / (kms / 1e3) / 1e9
-        tr = profiled_traffic()
+        tr = profiled_traffic(it_mean + 2)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (tr * (it_mean + 2) if tr else None), "peak_source": peak_kind,
+                "traffic": tr, "peak_source": peak_kind,
                 "kernel": "sinkhorn_log_kernel", "kernel_ms_per_launch": kms,
                 "alg_bytes_per_launch": alg_bytes}
         cpu = None
@@ -311,8 +323,31 @@ def run_engine(args):
     return 0
 
 
+def run_single(args):
+    """One warm-up plus one solve of an m x n problem with a fixed iteration
+    count (tol 0): the small case the kernel profiles are captured on."""
+    import torch
+
+    import rwig_b200 as rw
+    from rwig_b200 import synth
+    a, b, C = synth.log_config(args.m, args.n)
+    dev = torch.device("cuda", 0)
+    ta, tb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    tC = torch.from_numpy(C.T).to(dev)
+    P = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+    for _ in range(2):
+        r = rw.sinkhorn_log_device(ta, tb, tC, REG, args.iters, 0.0, P=P)
+    torch.cuda.synchronize()
+    rep = rw.last_report()
+    print(json.dumps({"m": args.m, "n": args.n, "iter": r["iter"], "kernel_ms": rep["kernel_ms"],
+                      "us_per_iter": rep["kernel_ms"] * 1e3 / max(1, r["iter"])}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.single:
+        return run_single(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

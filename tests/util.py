@@ -16,9 +16,11 @@ def mean_rel_diff(target, current):
     return float(np.abs(t - c).sum() / den) if den > 0 else float(np.abs(t - c).sum())
 
 
-def rel_err(x, ref):
+def rel_err(x, ref, scale=None):
     """Normwise relative error max|x - ref| / max|ref| over the finite entries;
-    non-finite entries must agree exactly."""
+    non-finite entries must agree exactly.  `scale` replaces max|ref| as the
+    denominator when given (for a dual pair (f, g), which is defined up to a
+    shared constant, both use max(|f|, |g|))."""
     x = np.asarray(x, dtype=float).ravel()
     ref = np.asarray(ref, dtype=float).ravel()
     assert x.shape == ref.shape, (x.shape, ref.shape)
@@ -27,6 +29,12 @@ def rel_err(x, ref):
     assert np.array_equal(x[~fin], ref[~fin], equal_nan=True), "non-finite values differ"
     if not fin.any():
         return 0.0
-    den = np.abs(ref[fin]).max()
+    den = np.abs(ref[fin]).max() if scale is None else scale
     num = np.abs(x[fin] - ref[fin]).max()
     return float(num / den) if den > 0 else float(num)
+
+
+def dual_scale(f, g):
+    v = np.concatenate([np.ravel(f), np.ravel(g)])
+    v = v[np.isfinite(v)]
+    return float(np.abs(v).max()) if v.size else 1.0
