@@ -81,6 +81,25 @@ RWIG_API int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, double*
                           const double* C, int M, int N, double reg, int withgrad,
                           int max_iter, double zero_tol, void* stream);
 
+/* Allocation-free log-Sinkhorn.  No counterpart in the reference: it exists for
+ * callers that cannot let a library allocate device memory (a host framework
+ * that owns the GPU's memory pool, a process under a hard device-memory quota,
+ * a serving loop that must not stall on cudaMalloc / cudaFree).  Same solver
+ * and results as rwig_sinkhorn_log_dev, but all scratch lives in a fixed
+ * ~10 MB block inside the library image, held by every GPU that loads the
+ * library until exit; the call makes no device allocation.
+ * Limits: M, N <= 4096, a and b strictly positive, M even, C 16-byte aligned
+ * (column-major, leading dimension M); anything else returns
+ * RWIG_E_UNSUPPORTED.  P, f, g are device outputs (any may be NULL); loss,
+ * iter, err are host pointers; `stream` is a cudaStream_t (NULL: legacy
+ * default stream).  All calls on a device share the block: calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the block's address; make it before any stream capture. */
+RWIG_API int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double* loss, int* iter,
+                                       double* err, const double* a, const double* b,
+                                       const double* C, int M, int N, double reg, int max_iter,
+                                       double zero_tol, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

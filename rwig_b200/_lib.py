@@ -67,6 +67,7 @@ SIGNATURES = {
     "rwig_sinkhorn_log": (_i, [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _i, _i, _d, _i, _i, _d]),
     "rwig_sinkhorn_log_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _i,
                                    _d, _vp]),
+    "rwig_sinkhorn_log_noalloc": (_i, [_vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _d, _vp]),
 }
 
 _lib = None

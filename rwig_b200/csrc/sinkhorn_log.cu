@@ -846,3 +846,224 @@ extern "C" int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   return rc;
 }
+
+// ===========================================================================
+// Allocation-free log-Sinkhorn (rwig_sinkhorn_log_noalloc).
+//
+// Some callers cannot let a library allocate device memory: a host framework
+// that has reserved the GPU's memory for its own pool, a process running under
+// a hard device-memory quota where a failed allocation in the middle of a
+// request is not acceptable, or a serving loop that must not pay for the
+// device-wide synchronisation that cudaMalloc / cudaFree can cause.  For them
+// this entry point runs the same solver kernel on a fixed scratch block that
+// lives in the library image itself: a file-scope __device__ array, created
+// when the library's device code is loaded and held by every GPU that loads
+// it until the process exits.  The caller passes all inputs and outputs.
+//
+// Limits: M <= 4096, N <= 4096, at most 148 CTAs, strictly positive a and b
+// (no support reduction, which would need a packed copy of C), M even and C
+// 16-byte aligned (the stage ring bulk-copies whole columns of C in place).
+// Larger or other inputs are rejected with RWIG_E_UNSUPPORTED.
+//
+// The scratch block is shared by every call on a device and keeps the last
+// call's contents; the control words, the potentials and the shifts are reset
+// at the start of each call by the preparation kernel.  Two calls whose work
+// overlaps on the GPU (different streams or host threads on the same device)
+// race on the block and give wrong results: callers must serialise them.
+// The first call on a device looks up the block's device address
+// (cudaGetSymbolAddress, with that device current) and caches it; make that
+// first call before any stream capture on the device.
+// ===========================================================================
+namespace rwig {
+namespace sklog_noalloc {
+
+constexpr int kMaxM = 4096;
+constexpr int kMaxN = 4096;
+constexpr int kMaxCtas = 148;
+// layout in doubles
+constexpr size_t kOffLogA = 0;
+constexpr size_t kOffELogA = kOffLogA + kMaxM;
+constexpr size_t kOffF0 = kOffELogA + kMaxM;
+constexpr size_t kOffF1 = kOffF0 + kMaxM;
+constexpr size_t kOffLogB = kOffF1 + kMaxM;
+constexpr size_t kOffELogB = kOffLogB + kMaxN;
+constexpr size_t kOffG = kOffELogB + kMaxN;
+constexpr size_t kOffMu = kOffG + kMaxN;
+constexpr size_t kOffRowP = kOffMu + kMaxN;
+constexpr size_t kOffRowPM = kOffRowP + (size_t)kMaxCtas * kMaxM;
+constexpr size_t kOffPart = kOffRowPM + (size_t)kMaxCtas * kMaxM;
+constexpr size_t kOffRes = kOffPart + (size_t)kMaxCtas * 8;
+constexpr size_t kOffCtrl = kOffRes + 8;  // 8 unsigned words = 4 doubles
+constexpr size_t kDoubles = kOffCtrl + 4;  // about 10.0 MB in total
+
+static __device__ __align__(256) double g_scratch[kDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+double* g_ptr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
+int g_smem_optin[kMaxDevices] = {};
+
+// Once per device, with that device current: device address of g_scratch.
+int setup(int dev, double** base, int* sms, int* smem_optin) {
+  if (dev < 0 || dev >= kMaxDevices) return set_error(RWIG_E_NODEVICE, "device index beyond 63");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    int major = 0;
+    RWIG_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major < 10) return set_error(RWIG_E_NODEVICE, "device is not sm_100 class (this build targets sm_100a)");
+    RWIG_CUDA_TRY(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    RWIG_CUDA_TRY(cudaDeviceGetAttribute(&g_smem_optin[dev], cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    g_ptr[dev] = static_cast<double*>(p);
+  }
+  *base = g_ptr[dev];
+  *sms = g_sms[dev];
+  *smem_optin = g_smem_optin[dev];
+  return 0;
+}
+
+// Counts zero entries of a and b into *out (one block).
+__global__ void count_zero_masses(const double* a, const double* b, int m, int n, unsigned* out) {
+  __shared__ unsigned s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0u;
+  __syncthreads();
+  unsigned c = 0u;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) c += (a[i] == 0.0);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) c += (b[j] == 0.0);
+  atomicAdd(&s_cnt, c);
+  __syncthreads();
+  if (threadIdx.x == 0) *out = s_cnt;
+}
+
+template <int RPT, int CW>
+int launch_noalloc(sklog::Params& p, int sms, int smem_optin, cudaStream_t st) {
+  using namespace sklog;
+  auto kern = sinkhorn_log_kernel<RPT, CW>;
+  const size_t smem = (size_t)STAGES * CW * p.ldc * 8 + STAGES * 8 + (2 * NW * CW + NW * 32) * 8;
+  if ((int)smem > smem_optin) return set_error(RWIG_E_UNSUPPORTED, "stage ring exceeds shared memory");
+  RWIG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem));
+  if (occ < 1) return set_error(RWIG_E_UNSUPPORTED, "kernel does not fit on an SM");
+  p.G = std::min(std::min(p.n, occ * sms), kMaxCtas);
+  void* args[] = {&p};
+  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(p.G), dim3(NT), args, smem, st));
+  return 0;
+}
+
+}  // namespace sklog_noalloc
+}  // namespace rwig
+
+extern "C" int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double* loss, int* iter,
+                                         double* err, const double* a, const double* b, const double* C,
+                                         int M, int N, double reg, int max_iter, double zero_tol,
+                                         void* stream) {
+  using namespace rwig;
+  using namespace rwig::sklog_noalloc;
+  reset_report();
+  if (!a || !b || !C) return set_error(RWIG_E_INVALID, "a, b and C must be non-null");
+  if (M < 1 || N < 1) return set_error(RWIG_E_INVALID, "M and N must be >= 1");
+  if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
+  if (M > kMaxM || N > kMaxN)
+    return set_error(RWIG_E_UNSUPPORTED,
+                     "problem exceeds the no-allocation limit of M <= 4096 and N <= 4096; "
+                     "use rwig_sinkhorn_log_dev");
+  if (M % 2 != 0 || (reinterpret_cast<uintptr_t>(C) % 16) != 0)
+    return set_error(RWIG_E_UNSUPPORTED,
+                     "the no-allocation entry needs an even M and a 16-byte aligned C; "
+                     "use rwig_sinkhorn_log_dev");
+  int dev = 0;
+  RWIG_CUDA_TRY(cudaGetDevice(&dev));
+  double* base = nullptr;
+  int sms = 0, smem_optin = 0;
+  int rc = setup(dev, &base, &sms, &smem_optin);
+  if (rc != 0) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  sklog::Params p{};
+  p.C = C;
+  p.ldc = M;
+  p.a = a;
+  p.b = b;
+  p.m = M;
+  p.n = N;
+  p.eps = reg;
+  p.inv_eps = 1.0 / reg;
+  p.max_iter = max_iter;
+  p.tol = zero_tol;
+  p.loga = base + kOffLogA;
+  p.eloga = base + kOffELogA;
+  p.logb = base + kOffLogB;
+  p.elogb = base + kOffELogB;
+  p.f0 = base + kOffF0;
+  p.f1 = base + kOffF1;
+  p.g = base + kOffG;
+  p.mu = base + kOffMu;
+  p.rowp = base + kOffRowP;
+  p.rowpm = base + kOffRowPM;
+  p.part = base + kOffPart;
+  p.res = base + kOffRes;
+  p.ctrl = reinterpret_cast<unsigned*>(base + kOffCtrl);
+  p.P = P;
+  p.ldp = M;
+  p.ridx = nullptr;
+  p.cidx = nullptr;
+  p.f_out = f;
+  p.g_out = g;
+
+  // every word the solver reads before writing is reset here: control words,
+  // f, g and the column shifts
+  sklog::prep_kernel<<<std::max(1, (std::max(M, N) + 255) / 256), 256, 0, st>>>(
+      a, b, M, N, reg, base + kOffLogA, base + kOffELogA, base + kOffLogB, base + kOffELogB,
+      base + kOffF0, base + kOffG, base + kOffMu, p.ctrl);
+  count_zero_masses<<<1, 256, 0, st>>>(a, b, M, N, p.ctrl + 4);
+  RWIG_CUDA_TRY(cudaGetLastError());
+  unsigned zeros = 0u;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(&zeros, p.ctrl + 4, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (zeros != 0u)
+    return set_error(RWIG_E_UNSUPPORTED,
+                     "the no-allocation entry needs strictly positive a and b (zero masses need the "
+                     "support-reducing rwig_sinkhorn_log_dev)");
+
+  const int rpt_need = (M + sklog::NT - 1) / sklog::NT;
+  if (rpt_need <= 1) rc = launch_noalloc<1, 16>(p, sms, smem_optin, st);
+  else if (rpt_need <= 2) rc = launch_noalloc<2, 8>(p, sms, smem_optin, st);
+  else if (rpt_need <= 4) rc = launch_noalloc<4, 4>(p, sms, smem_optin, st);
+  else rc = launch_noalloc<8, 2>(p, sms, smem_optin, st);
+  if (rc != 0) return rc;
+  RWIG_CUDA_TRY(cudaGetLastError());
+
+  double res[8];
+  unsigned ctrl[4];
+  RWIG_CUDA_TRY(cudaMemcpyAsync(res, p.res, sizeof(res), cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(ctrl, p.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (ctrl[2] != 0u) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "log-Sinkhorn kernel stopped by a bounded wait (error bits 0x%x)", ctrl[2]);
+    return set_error(RWIG_E_TIMEOUT, buf);
+  }
+  const int it = (int)res[0];
+  const double e = res[1];
+  if (loss) *loss = res[2];
+  if (iter) *iter = it;
+  if (err) *err = e;
+  const int status = (e <= zero_tol) ? 0 : (it == max_iter ? 1 : 2);
+  rwig_report& R = report();
+  R.iter = it;
+  R.status = status;
+  R.err = e;
+  R.marg_l1_row = res[3];
+  R.marg_l1_col = res[4];
+  R.marg_l2_row = res[5];
+  R.marg_l2_col = res[6];
+  R.fallback_events = (int)res[7];
+  R.kernel_launches = 3;
+  R.support_m = M;
+  R.support_n = N;
+  return status;
+}
