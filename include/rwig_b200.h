@@ -60,6 +60,12 @@ RWIG_API void rwig_shutdown(void);             /* frees all device memory held b
 RWIG_API const char* rwig_last_error(void);    /* message of the last failure on this thread */
 RWIG_API int rwig_version(void);
 RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on this thread */
+/* Engine options (process-wide):
+ *   "log_sinkhorn.scaled": 1 (default) runs the log-Sinkhorn iterations after
+ *       the first in stabilised scaling form, 0 keeps every iteration in the
+ *       log domain (same results within rounding; slower);
+ *   "log_sinkhorn.tau": absorption bound on |log u|, |log v| (default 100). */
+RWIG_API int rwig_set_option(const char* name, double value);
 
 /* ---- log-stabilised Sinkhorn ------------------------------------------
  * Replaces the CPU-only Sinkhorn::compute_log (src/sinkhorn_impl_log.cpp:225)
@@ -80,6 +86,11 @@ RWIG_API int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, double*
                           int* iter, double* err, const double* a, const double* b,
                           const double* C, int M, int N, double reg, int withgrad,
                           int max_iter, double zero_tol, void* stream);
+
+/* Self-check of the engine's internal exponential (no counterpart in the
+ * reference): evaluates it and CUDA's exp on n device doubles x, writing
+ * y_engine and y_cuda (device).  Used by the test suite to bound its error. */
+RWIG_API int rwig_selftest_exp(const double* x, double* y_engine, double* y_cuda, int n, void* stream);
 
 /* Allocation-free log-Sinkhorn.  No counterpart in the reference: it exists for
  * callers that cannot let a library allocate device memory (a host framework

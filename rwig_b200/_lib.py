@@ -64,9 +64,11 @@ SIGNATURES = {
     "rwig_last_error": (ctypes.c_char_p, []),
     "rwig_version": (_i, []),
     "rwig_last_report": (_i, [ctypes.POINTER(Report)]),
+    "rwig_set_option": (_i, [ctypes.c_char_p, _d]),
     "rwig_sinkhorn_log": (_i, [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _i, _i, _d, _i, _i, _d]),
     "rwig_sinkhorn_log_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _i,
                                    _d, _vp]),
+    "rwig_selftest_exp": (_i, [_vp, _vp, _vp, _i, _vp]),
     "rwig_sinkhorn_log_noalloc": (_i, [_vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _d, _vp]),
 }
 

@@ -103,38 +103,37 @@ __device__ __forceinline__ uint64_t l2_policy_evict_first() {
 }
 
 // ---- grid barrier -----------------------------------------------------------
-// Sense-free generation barrier for a cooperative launch (all CTAs resident).
-// ctrl[0] = arrival count, ctrl[1] = generation, *err = error bits.
-// Every thread of every CTA must call it.  Returns false when the error word
-// is (or becomes) non-zero; callers then leave their loops.
-__device__ __forceinline__ bool grid_barrier(unsigned* ctrl, unsigned* err, unsigned nblocks) {
-  __shared__ int s_ok;
+// Counting grid barrier for a cooperative launch: the CTAs add 1 to *count
+// at every barrier and wait until it reaches `target` = (barrier index + 1) *
+// nblocks, so no generation word and no last-arriver step are needed.  Thread 0
+// of each CTA fences (cumulative over the CTA's writes, ordered by the block
+// barrier), arrives with a relaxed reduction and polls with acquire loads.
+// The count must start at zero; the wait is bounded and sets *err on expiry.
+__device__ __forceinline__ bool grid_sync(unsigned* count, unsigned* err, unsigned target) {
+  __shared__ int s_ok2;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = ctrl + 1;
-    const unsigned gen = *vgen;
     __threadfence();
-    const unsigned arrived = atomicAdd(ctrl, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(ctrl, 0u);
-      __threadfence();
-      atomicAdd(ctrl + 1, 1u);
-    } else {
-      const unsigned long long t0 = globaltimer_ns();
-      while (*vgen == gen) {
+    asm volatile("red.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+    unsigned long long t0 = 0;
+    for (unsigned spin = 0;; ++spin) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+      if ((int)(v - target) >= 0) break;
+      if ((spin & 255u) == 0u) {
         if (*(volatile unsigned*)err != 0u) break;
-        __nanosleep(64);
-        if (globaltimer_ns() - t0 > kWaitLimitNs) {
+        const unsigned long long now = globaltimer_ns();
+        if (t0 == 0) t0 = now;
+        else if (now - t0 > kWaitLimitNs) {
           atomicOr(err, KERR_BARRIER_TIMEOUT);
           break;
         }
       }
     }
-    __threadfence();
-    s_ok = (*(volatile unsigned*)err == 0u);
+    s_ok2 = (*(volatile unsigned*)err == 0u);
   }
   __syncthreads();
-  return s_ok != 0;
+  return s_ok2 != 0;
 }
 
 // ---- warp reductions ------------------------------------------------------------

@@ -2,7 +2,9 @@
 // entry points of the C ABI.
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <string>
 
 #include "engine.h"
 
@@ -43,6 +45,18 @@ int init_device(int dev, Context** out) {
   return 0;
 }
 }  // namespace
+
+namespace {
+std::mutex g_opt_mu;
+std::map<std::string, double> g_opts;
+const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau"};
+}  // namespace
+
+double option(const char* name, double dflt) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  auto it = g_opts.find(name);
+  return it == g_opts.end() ? dflt : it->second;
+}
 
 int set_error(int code, const std::string& msg) {
   t_last_error = msg;
@@ -130,6 +144,17 @@ extern "C" void rwig_shutdown(void) {
 }
 
 extern "C" const char* rwig_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" int rwig_set_option(const char* name, double value) {
+  if (!name) return set_error(RWIG_E_INVALID, "option name is null");
+  for (const char* known : kOptionNames)
+    if (std::strcmp(known, name) == 0) {
+      std::lock_guard<std::mutex> lk(g_opt_mu);
+      g_opts[name] = value;
+      return 0;
+    }
+  return set_error(RWIG_E_INVALID, std::string("unknown option: ") + name);
+}
 
 extern "C" int rwig_version(void) { return RWIG_B200_VERSION; }
 

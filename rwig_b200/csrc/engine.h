@@ -33,6 +33,9 @@ Context* get_context();
 // Grow-only scratch slot `k` of at least `bytes`; nullptr on failure.
 void* scratch(Context* ctx, int k, size_t bytes);
 
+// Engine options (rwig_set_option); unknown names return `dflt`.
+double option(const char* name, double dflt);
+
 // Error / report plumbing (thread-local).
 int set_error(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);

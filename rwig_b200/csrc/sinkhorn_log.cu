@@ -30,13 +30,19 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "fastexp.cuh"
+#include "sk_common.cuh"
+#include "sk_host.h"
 
 namespace rwig {
 namespace sklog {
 
-constexpr int NT = 512;
-constexpr int NW = NT / 32;
-constexpr int STAGES = 3;
+using sk::STAGES;
+using sk::Ring;
+using sk::flag_error;
+using sk::block_sum_cols;
+using sk::block_min_cols;
+using sk::sum_partials;
 
 struct Params {
   const double* C;
@@ -65,68 +71,36 @@ struct Params {
   const int* cidx;
   double* f_out;  // optional, full size
   double* g_out;
-  double* res;    // [8] iter, err, loss, l1row, l1col, l2row, l2col, robust events
+  double* res;    // [9] iter, err, loss, l1row, l1col, l2row, l2col, robust events, finished
+  int ncol_max;   // upper bound of columns per CTA (sizes the shared column arrays)
+  // Resumable runs.  resume = 1 starts from f = f0 (reduced, set by the host)
+  // and g = g_state after iter0 iterations with error err0, skipping the
+  // initial row sweep.  iter_cap > 0 stops after that many iterations of this
+  // launch.  At exit f_state / g_state hold the state to resume from (the f
+  // of the next iteration and the current g) or, once the solve is finished
+  // (err < tol or max_iter), the final f and g; res[8] = 1 when finished.
+  // do_final = 0 skips the plan / loss / marginal pass.
+  int resume, iter0, iter_cap, do_final;
+  double err0;
+  double* f_state;
+  double* g_state;
 };
 
-// Stage ring over this CTA's column groups; the q-th consumed stage holds
-// column group (q mod nst) and lives in buffer q mod STAGES.
-template <int CW>
-struct Ring {
-  double* buf;
-  uint64_t* bar;
-  const double* C;
-  long long ldc;
-  int c0, c1, nst;
-  unsigned q;  // next stage to consume (identical in every thread)
-
-  __device__ int group_begin(unsigned seq) const { return c0 + (int)(seq % (unsigned)nst) * CW; }
-  __device__ int group_cols(unsigned seq) const { return min(CW, c1 - group_begin(seq)); }
-  __device__ double* slot(unsigned seq) const { return buf + (size_t)(seq % STAGES) * CW * ldc; }
-
-  // thread 0 only
-  __device__ void issue(unsigned seq) const {
-    const int jb = group_begin(seq);
-    const unsigned bytes = (unsigned)(group_cols(seq) * ldc * 8);
-    uint64_t* b = bar + (seq % STAGES);
-    mbar_arrive_expect_tx(b, bytes);
-    bulk_g2s(slot(seq), C + (size_t)jb * ldc, bytes, b);
-  }
-  __device__ bool wait(unsigned seq) const { return mbar_wait_bounded(bar + (seq % STAGES), (seq / STAGES) & 1u); }
-};
-
-__device__ __forceinline__ void flag_error(unsigned* ctrl, unsigned bits) { atomicOr(ctrl + 2, bits); }
-
-// Per-column block reduction: every warp ends with the same total per column.
-template <int CW>
-__device__ __forceinline__ void block_sum_cols(double (&v)[CW], double* red, int& par) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < CW; ++c) {
-    double t = warp_sum(v[c]);
-    if (lane == 0) red[(par * NW + w) * CW + c] = t;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < CW; ++c) v[c] = warp_sum(lane < NW ? red[(par * NW + lane) * CW + c] : 0.0);
-  par ^= 1;
+// Dynamic shared memory of one CTA: stage ring, mbarriers, reduction scratch,
+// exp table and the per-column state of the CTA's strip (b, log b, eps log b, g, shift).
+template <int CW, int NWARPS>
+__host__ __device__ constexpr size_t smem_bytes(long long ldc, int ncol_max) {
+  return (size_t)STAGES * CW * ldc * 8 + STAGES * 8 +
+         (size_t)(2 * NWARPS * CW + NWARPS * 32 + 64 * kExpTableSpread) * 8 +
+         (size_t)6 * ncol_max * 8;
 }
 
-template <int CW>
-__device__ __forceinline__ void block_min_cols(double (&v)[CW], double* red, int& par) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < CW; ++c) {
-    double t = warp_min(v[c]);
-    if (lane == 0) red[(par * NW + w) * CW + c] = t;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < CW; ++c) v[c] = warp_min(lane < NW ? red[(par * NW + lane) * CW + c] : INFINITY);
-  par ^= 1;
-}
-
-template <int RPT, int CW>
-__global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
+// RPT rows per thread, CW columns per stage, NTT threads per CTA; FULL when
+// every thread row is a real row (m == RPT * NTT), which drops the row masks.
+template <int RPT, int CW, int NTT, bool FULL>
+__global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
+  constexpr int NT = NTT;
+  constexpr int NW = NTT / 32;
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int cta = blockIdx.x, G = p.G;
@@ -138,6 +112,15 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
   ring.bar = reinterpret_cast<uint64_t*>(smem + (size_t)STAGES * CW * p.ldc * 8);
   double* red = reinterpret_cast<double*>(ring.bar + STAGES);  // [2][NW][CW]
   double* red3 = red + 2 * NW * CW;                            // [NW][32]
+  double* tbl = red3 + NW * 32;                                // [64 x 16] 2^(j/64), bank-spread
+  const double* tbl_l = tbl + (tid & (kExpTableSpread - 1));  // this lane's replica
+  const int NCM = p.ncol_max;
+  double* cb = tbl + 64 * kExpTableSpread;  // b_j of this CTA's columns
+  double* clogb = cb + NCM;     // log b_j
+  double* celogb = clogb + NCM; // eps log b_j
+  double* cg = celogb + NCM;    // g_j
+  double* cmu = cg + NCM;       // column shift (previous column soft-min / eps)
+  double* csum = cmu + NCM;     // column sums of the current sweep
   __shared__ double s_scalar[4];
   ring.C = p.C;
   ring.ldc = p.ldc;
@@ -148,6 +131,15 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
   const int r0 = (int)(((long long)cta * m) / G), r1 = (int)(((long long)(cta + 1) * m) / G);
   int par = 0;
 
+  load_exp_table_spread(tbl);
+  for (int c = tid; c < ring.c1 - ring.c0; c += NT) {
+    const int j = ring.c0 + c;
+    cb[c] = p.b[j];
+    clogb[c] = p.logb[j];
+    celogb[c] = p.elogb[j];
+    cg[c] = p.resume ? p.g_state[j] : 0.0;
+    cmu[c] = 0.0;
+  }
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(ring.bar + s, 1);
     fence_mbar_init();
@@ -157,22 +149,25 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
     for (int s = 0; s < STAGES; ++s) ring.issue(s);
 
   bool ok = true;
-  double f[RPT];
+  unsigned nbar = 0;  // grid barriers passed so far (same in every CTA)
+  auto gsync = [&]() -> bool { ++nbar; return grid_sync(p.ctrl, p.ctrl + 2, nbar * (unsigned)G); };
+  // fr[k]: this thread's rows of f, scaled by 1/eps during the iterations
+  double fr[RPT];
+  bool valid[RPT];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) valid[k] = FULL || (tid + k * NT) < m;
   double* fcur = p.f0;
   double* fnext = p.f1;
   unsigned robust_seen = 0;
 
   // ---------------------------------------------------------------- helpers
-  auto load_f = [&](const double* src) {
+  auto load_f = [&](const double* src, double scale) {
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-      const int i = tid + k * NT;
-      f[k] = (i < m) ? __ldcg(src + i) : 0.0;
-    }
+    for (int k = 0; k < RPT; ++k) fr[k] = valid[k] ? __ldcg(src + tid + k * NT) * scale : 0.0;
   };
 
-  // Robust row soft-min partials of R = (C - f) - g over this CTA's columns:
-  // running (min, sum) per row, one exponential per element.
+  // Robust row soft-min partials of R/eps = (C - f - g)/eps over this CTA's
+  // columns: running (min, sum) per row, one exponential per element; fr holds f/eps.
   auto robust_row_sweep = [&]() -> bool {
     double rm[RPT], rs[RPT];
 #pragma unroll
@@ -189,14 +184,14 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
       const double* buf = ring.slot(seq);
       const int jb = ring.group_begin(seq), nc = ring.group_cols(seq);
       for (int c = 0; c < nc; ++c) {
-        const double gj = p.g[jb + c];
+        const double gj = cg[jb - ring.c0 + c] * inv_eps;
+        const double* col = buf + (size_t)c * p.ldc + tid;
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
-          const int i = tid + k * NT;
-          if (i < m) {
-            const double x = (buf[(size_t)c * p.ldc + i] - f[k]) - gj;
+          if (valid[k]) {
+            const double x = fma(col[k * NT], inv_eps, -(fr[k] + gj));
             const double d = x - rm[k];
-            const double e = exp(-fabs(d) * inv_eps);
+            const double e = exp_tbl<kExpTableSpread>(-fabs(d), tbl_l);
             if (d < 0.0) {
               rs[k] = rs[k] * e + 1.0;
               rm[k] = x;
@@ -212,8 +207,8 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
     }
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
-      const int i = tid + k * NT;
-      if (i < m) {
+      if (valid[k]) {
+        const int i = tid + k * NT;
         p.rowpm[(size_t)cta * m + i] = rm[k];
         p.rowp[(size_t)cta * m + i] = rs[k];
       }
@@ -222,49 +217,56 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
   };
 
   // Row merge over all CTAs for rows [r0, r1).  robust: partials are
-  // (min, sum) pairs; otherwise plain sums of the plan.  Writes fnext and the
-  // CTA's squared row error into part[cta][0].
+  // (min, sum) pairs of R/eps; otherwise plain sums of the plan.  Writes
+  // fnext and the CTA's squared row error into part[cta][0].
   auto row_merge = [&](bool robust) {
     double errr = 0.0;
     for (int rb = r0; rb < r1; rb += 32) {
       const int i = rb + lane;
-      const bool valid = i < r1;
+      const bool vi = i < r1;
       double Rrow = 0.0;
       if (robust) {
         double mn = INFINITY;
-        if (valid)
-          for (int q2 = w; q2 < G; q2 += NW) mn = fmin(mn, __ldcg(p.rowpm + (size_t)q2 * m + i));
+        if (vi)
+          for (int q2 = w; q2 < G; q2 += 4 * NW) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              v[u] = (q2 + u * NW < G) ? __ldcg(p.rowpm + (size_t)(q2 + u * NW) * m + i) : INFINITY;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) mn = fmin(mn, v[u]);
+          }
         red3[w * 32 + lane] = mn;
         __syncthreads();
         mn = INFINITY;
         for (int ww = 0; ww < NW; ++ww) mn = fmin(mn, red3[ww * 32 + lane]);
         __syncthreads();
         double acc = 0.0;
-        if (valid)
+        if (vi)
           for (int q2 = w; q2 < G; q2 += NW) {
             const double mp = __ldcg(p.rowpm + (size_t)q2 * m + i);
-            if (mp < INFINITY) acc += __ldcg(p.rowp + (size_t)q2 * m + i) * exp(-(mp - mn) * inv_eps);
+            if (mp < INFINITY) acc += __ldcg(p.rowp + (size_t)q2 * m + i) * exp(-(mp - mn));
           }
         red3[w * 32 + lane] = acc;
         __syncthreads();
         double tot = 0.0;
         for (int ww = 0; ww < NW; ++ww) tot += red3[ww * 32 + lane];
-        Rrow = mn - eps * log(tot);
+        Rrow = eps * (mn - log(tot));
       } else {
         double acc = 0.0;
-        if (valid)
-          for (int q2 = w; q2 < G; q2 += NW) acc += __ldcg(p.rowp + (size_t)q2 * m + i);
+        if (vi) acc = sum_partials<NW>(p.rowp, i, m, G, w);
         red3[w * 32 + lane] = acc;
         __syncthreads();
         double tot = 0.0;
         for (int ww = 0; ww < NW; ++ww) tot += red3[ww * 32 + lane];
-        if (w == 0 && valid && !(tot >= 1e-290 && tot <= 1e290)) atomicAdd(p.ctrl + 3, 1u);
+        if (w == 0 && vi && !(tot >= 1e-250 && tot <= 1e250)) atomicAdd(p.ctrl + 3, 1u);
         Rrow = -eps * log(tot);
       }
-      if (w == 0 && valid) {
-        const double d = -Rrow * inv_eps - p.loga[i];
+      if (w == 0 && vi) {
+        const double la = p.loga[i], ela = p.eloga[i], fc = __ldcg(fcur + i);
+        const double d = -Rrow * inv_eps - la;
         errr += d * d;
-        fnext[i] = __ldcg(fcur + i) + (p.eloga[i] + Rrow);
+        fnext[i] = fc + (ela + Rrow);
       }
       __syncthreads();
     }
@@ -274,43 +276,57 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
     }
   };
 
-  // Deterministic sum of part[*][k] over CTAs (same order in every CTA).
-  auto total = [&](int k) -> double {
+  // Deterministic sums of part[*][k0] and part[*][k1] over CTAs (same order
+  // in every CTA).
+  auto total2 = [&](int k0, int k1, double& t0, double& t1) {
     if (w == 0) {
-      double acc = 0.0;
-      for (int q2 = lane; q2 < G; q2 += 32) acc += __ldcg(p.part + (size_t)q2 * 8 + k);
-      acc = warp_sum(acc);
-      if (lane == 0) s_scalar[0] = acc;
+      double a0 = 0.0, a1 = 0.0;
+      for (int q2 = lane; q2 < G; q2 += 64) {
+        const bool h = q2 + 32 < G;
+        const double x0 = __ldcg(p.part + (size_t)q2 * 8 + k0), x1 = __ldcg(p.part + (size_t)q2 * 8 + k1);
+        const double y0 = h ? __ldcg(p.part + (size_t)(q2 + 32) * 8 + k0) : 0.0;
+        const double y1 = h ? __ldcg(p.part + (size_t)(q2 + 32) * 8 + k1) : 0.0;
+        a0 += x0 + y0;
+        a1 += x1 + y1;
+      }
+      a0 = warp_sum(a0);
+      a1 = warp_sum(a1);
+      if (lane == 0) {
+        s_scalar[0] = a0;
+        s_scalar[1] = a1;
+      }
     }
     __syncthreads();
-    const double v = s_scalar[0];
+    t0 = s_scalar[0];
+    t1 = s_scalar[1];
     __syncthreads();
-    return v;
   };
 
   // -------------------------------------------------------------- init
-  int iter = 0;
-  double err = 1000.0;
-  if (p.max_iter > 0) {
-    load_f(fcur);  // zeros
+  int iter = p.resume ? p.iter0 : 0;
+  double err = p.resume ? p.err0 : 1000.0;
+  if (!p.resume && p.max_iter > 0) {
+    load_f(fcur, inv_eps);  // zeros
     ok = robust_row_sweep();
-    ok = grid_barrier(p.ctrl, p.ctrl + 2, G) && ok;
+    ok = gsync() && ok;
     if (ok) {
       row_merge(true);
-      ok = grid_barrier(p.ctrl, p.ctrl + 2, G);
+      ok = gsync();
     }
     { double* t = fcur; fcur = fnext; fnext = t; }
   }
 
   // -------------------------------------------------------------- iterations
+  // Column pass in units of 1/eps: y_ij = C_ij/eps - f_i/eps, shift mu_j,
+  // e_ij = exp(mu_j - y_ij), s_j = sum_i e_ij, softmin_i(C_ij - f_i) = eps (mu_j - log s_j).
   while (ok && iter < p.max_iter && err >= p.tol) {
     ++iter;
-    load_f(fcur);
+    load_f(fcur, inv_eps);
     double r[RPT];
 #pragma unroll
     for (int k = 0; k < RPT; ++k) r[k] = 0.0;
     double errc = 0.0;
-    const bool first = (iter == 1);
+    const bool first = (iter == (p.resume ? p.iter0 : 0) + 1);
 
     for (int s = 0; s < ring.nst && ok; ++s) {
       const unsigned seq = ring.q;
@@ -319,7 +335,7 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
         ok = false;
         break;
       }
-      const double* buf = ring.slot(seq);
+      const double* buf = ring.slot(seq) + tid;
       const int jb = ring.group_begin(seq), nc = ring.group_cols(seq);
       double mu[CW], sum[CW], e[RPT][CW];
       bool exact = first;
@@ -330,31 +346,34 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
             double lm = INFINITY;
             if (c < nc) {
 #pragma unroll
-              for (int k = 0; k < RPT; ++k) {
-                const int i = tid + k * NT;
-                if (i < m) lm = fmin(lm, buf[(size_t)c * p.ldc + i] - f[k]);
-              }
+              for (int k = 0; k < RPT; ++k)
+                if (valid[k]) lm = fmin(lm, fma(buf[(size_t)c * p.ldc + k * NT], inv_eps, -fr[k]));
             }
             mu[c] = lm;
           }
-          block_min_cols<CW>(mu, red, par);
+          block_min_cols<CW, NW>(mu, red, par);
         } else {
 #pragma unroll
-          for (int c = 0; c < CW; ++c) mu[c] = (c < nc) ? p.mu[jb + c] : 0.0;
+          for (int c = 0; c < CW; ++c) mu[c] = (c < nc) ? cmu[jb - ring.c0 + c] : 0.0;
         }
 #pragma unroll
         for (int c = 0; c < CW; ++c) {
           sum[c] = 0.0;
+          if (c < nc) {
+            const double* col = buf + (size_t)c * p.ldc;
 #pragma unroll
-          for (int k = 0; k < RPT; ++k) {
-            const int i = tid + k * NT;
-            double ev = 0.0;
-            if (c < nc && i < m) ev = exp((mu[c] - (buf[(size_t)c * p.ldc + i] - f[k])) * inv_eps);
-            e[k][c] = ev;
-            sum[c] += ev;
+            for (int k = 0; k < RPT; ++k) {
+              double ev = 0.0;
+              if (valid[k]) ev = exp_tbl<kExpTableSpread>(fma(col[k * NT], -inv_eps, mu[c] + fr[k]), tbl_l);
+              e[k][c] = ev;
+              sum[c] += ev;
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) e[k][c] = 0.0;
           }
         }
-        block_sum_cols<CW>(sum, red, par);
+        block_sum_cols<CW, NW>(sum, red, par);
         bool bad = false;
 #pragma unroll
         for (int c = 0; c < CW; ++c)
@@ -366,71 +385,94 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
       if (tid == 0) ring.issue(seq + STAGES);
       ring.q = seq + 1;
 
+      // lane c of every warp owns column jb + c: b_j / s_j, and (warp 0) the
+      // column update; the ratio is shared across the warp by shuffles
+      double mine_s = 0.0, mine_mu = 0.0;
+#pragma unroll
+      for (int c = 0; c < CW; ++c)
+        if (c == lane) {
+          mine_s = sum[c];
+          mine_mu = mu[c];
+        }
+      const bool owner = lane < nc;
+      const int jl = jb - ring.c0 + lane;  // local column index
+      const double beta_l = owner ? cb[jl] * rcp_nr(mine_s) : 0.0;
       double beta[CW];
 #pragma unroll
-      for (int c = 0; c < CW; ++c) beta[c] = (c < nc) ? p.b[jb + c] / sum[c] : 0.0;
-      if (w == 0 && lane < nc) {
-        // column finalisation for column jb + lane (lane < nc <= CW)
-        double sml = 0.0, mul = 0.0;
-#pragma unroll
-        for (int c = 0; c < CW; ++c)
-          if (c == lane) {
-            sml = sum[c];
-            mul = mu[c];
-          }
-        const int j = jb + lane;
-        const double sm = mul - eps * log(sml);   // softmin_i(C_ij - f_i)
-        const double gj = p.g[j];
-        const double rmin = sm - gj;              // mincol(R(f, g))_j
-        const double gn = gj + (p.elogb[j] + rmin);
-        p.g[j] = gn;
-        p.mu[j] = sm;
-        const double d = -(sm - gn) * inv_eps - p.logb[j];
-        errc += d * d;
+      for (int c = 0; c < CW; ++c) beta[c] = __shfl_sync(0xffffffffu, beta_l, c);
+      if (w == 0 && owner) {
+        cmu[jl] = mine_mu;  // shift used by this sweep
+        csum[jl] = mine_s;
       }
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
         double acc = 0.0;
 #pragma unroll
-        for (int c = 0; c < CW; ++c) acc += e[k][c] * beta[c];
+        for (int c = 0; c < CW; ++c) acc = fma(e[k][c], beta[c], acc);
         r[k] += acc;
       }
     }
     if (!ok) break;
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-      const int i = tid + k * NT;
-      if (i < m) p.rowp[(size_t)cta * m + i] = r[k];
+    for (int k = 0; k < RPT; ++k)
+      if (valid[k]) p.rowp[(size_t)cta * m + tid + k * NT] = r[k];
+    // column updates of the whole strip, off the per-stage critical path
+    __syncthreads();
+    if (w == 0) {
+      for (int c = lane; c < ring.c1 - ring.c0; c += 32) {
+        const double sm = cmu[c] - log(csum[c]);  // softmin_i(C_ij - f_i) / eps
+        const double gj = cg[c];
+        const double rmin = eps * sm - gj;        // mincol(R(f, g))_j
+        const double gn = gj + (celogb[c] + rmin);
+        cg[c] = gn;
+        cmu[c] = sm;
+        const double d = -(eps * sm - gn) * inv_eps - clogb[c];
+        errc += d * d;
+      }
     }
     if (w == 0) {
       errc = warp_sum(errc);
       if (lane == 0) p.part[(size_t)cta * 8 + 1] = errc;
     }
-    if (!grid_barrier(p.ctrl, p.ctrl + 2, G)) { ok = false; break; }
+    if (!gsync()) { ok = false; break; }
     row_merge(false);
-    if (!grid_barrier(p.ctrl, p.ctrl + 2, G)) { ok = false; break; }
+    if (!gsync()) { ok = false; break; }
     const unsigned rob = *(volatile unsigned*)(p.ctrl + 3);
     if (rob != robust_seen) {
       // some merged row sum left the safe range: redo the row soft-min with
       // the reference's per-row minimum shift, with g already updated
       robust_seen = rob;
       if (!robust_row_sweep()) { ok = false; break; }
-      if (!grid_barrier(p.ctrl, p.ctrl + 2, G)) { ok = false; break; }
+      if (!gsync()) { ok = false; break; }
       row_merge(true);
-      if (!grid_barrier(p.ctrl, p.ctrl + 2, G)) { ok = false; break; }
+      if (!gsync()) { ok = false; break; }
     }
-    const double er = total(0), ec = total(1);
+    double er, ec;
+    total2(0, 1, er, ec);
     err = sqrt(er) + sqrt(ec);
     if (iter < p.max_iter && err >= p.tol) {
       double* t = fcur;
       fcur = fnext;
       fnext = t;
+      if (p.iter_cap > 0 && iter - (p.resume ? p.iter0 : 0) >= p.iter_cap) break;  // hand-off
+    }
+  }
+  const bool finished = !(iter < p.max_iter && err >= p.tol);
+
+  // state for a resumed run: fcur and this CTA's columns of g
+  if (ok && p.f_state) {
+    for (int c = tid; c < ring.c1 - ring.c0; c += NT) p.g_state[ring.c0 + c] = cg[c];
+    for (int i = r0 + tid; i < r1; i += NT) p.f_state[i] = __ldcg(fcur + i);
+    if (cta == 0 && tid == 0) {
+      p.res[0] = iter;
+      p.res[1] = err;
+      p.res[8] = finished ? 1.0 : 0.0;
     }
   }
 
   // -------------------------------------------------------------- final plan, loss, report
-  if (ok) {
-    load_f(fcur);
+  if (ok && finished && p.do_final) {
+    load_f(fcur, 1.0);
     double rr[RPT];
 #pragma unroll
     for (int k = 0; k < RPT; ++k) rr[k] = 0.0;
@@ -450,14 +492,14 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
         cs[c] = 0.0;
         if (c < nc) {
           const int j = jb + c;
-          const double gj = p.g[j];
+          const double gj = cg[j - ring.c0];
           const long long jf = p.cidx ? p.cidx[j] : j;
 #pragma unroll
           for (int k = 0; k < RPT; ++k) {
-            const int i = tid + k * NT;
-            if (i < m) {
+            if (valid[k]) {
+              const int i = tid + k * NT;
               const double cij = buf[(size_t)c * p.ldc + i];
-              const double R = (cij - f[k]) - gj;
+              const double R = (cij - fr[k]) - gj;
               const double Pv = exp(-R * inv_eps);
               if (p.P) {
                 const long long ifull = p.ridx ? p.ridx[i] : i;
@@ -471,7 +513,7 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
           }
         }
       }
-      block_sum_cols<CW>(cs, red, par);
+      block_sum_cols<CW, NW>(cs, red, par);
       if (tid == 0) ring.issue(seq + STAGES);
       ring.q = seq + 1;
       if (w == 0 && lane < nc) {
@@ -480,18 +522,17 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
         for (int c = 0; c < CW; ++c)
           if (c == lane) csl = cs[c];
         const int j = jb + lane;
-        const double d = csl - p.b[j];
+        const double d = csl - cb[j - ring.c0];
         c1 += fabs(d);
         c2 += d * d;
-        if (p.g_out) p.g_out[p.cidx ? p.cidx[j] : j] = p.g[j];
+        p.g[j] = cg[j - ring.c0];
+        if (p.g_out) p.g_out[p.cidx ? p.cidx[j] : j] = cg[j - ring.c0];
       }
     }
     if (ok) {
 #pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int i = tid + k * NT;
-        if (i < m) p.rowp[(size_t)cta * m + i] = rr[k];
-      }
+      for (int k = 0; k < RPT; ++k)
+        if (valid[k]) p.rowp[(size_t)cta * m + tid + k * NT] = rr[k];
       // block-reduce the loss and column-violation partials
       double v[4] = {l1, l2, c1, c2};
 #pragma unroll
@@ -506,19 +547,18 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
         p.part[(size_t)cta * 8 + 2 + tid] = acc;
       }
       __syncthreads();
-      ok = grid_barrier(p.ctrl, p.ctrl + 2, G);
+      ok = gsync();
     }
     if (ok) {
       double a1 = 0.0, a2 = 0.0;
       for (int rb = r0; rb < r1; rb += 32) {
         const int i = rb + lane;
-        const bool valid = i < r1;
+        const bool vi = i < r1;
         double acc = 0.0;
-        if (valid)
-          for (int q2 = w; q2 < G; q2 += NW) acc += __ldcg(p.rowp + (size_t)q2 * m + i);
+        if (vi) acc = sum_partials<NW>(p.rowp, i, m, G, w);
         red3[w * 32 + lane] = acc;
         __syncthreads();
-        if (w == 0 && valid) {
+        if (w == 0 && vi) {
           double tot = 0.0;
           for (int ww = 0; ww < NW; ++ww) tot += red3[ww * 32 + lane];
           const double d = tot - p.a[i];
@@ -536,11 +576,13 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
           p.part[(size_t)cta * 8 + 7] = a2;
         }
       }
-      ok = grid_barrier(p.ctrl, p.ctrl + 2, G);
+      ok = gsync();
     }
     if (ok && cta == 0) {
-      const double tl1 = total(2), tl2 = total(3), tc1 = total(4), tc2 = total(5), tr1 = total(6),
-                   tr2 = total(7);
+      double tl1, tl2, tc1, tc2, tr1, tr2;
+      total2(2, 3, tl1, tl2);
+      total2(4, 5, tc1, tc2);
+      total2(6, 7, tr1, tr2);
       if (tid == 0) {
         p.res[0] = iter;
         p.res[1] = err;
@@ -550,6 +592,7 @@ __global__ void __launch_bounds__(NT, 1) sinkhorn_log_kernel(Params p) {
         p.res[5] = sqrt(tr2);
         p.res[6] = sqrt(tc2);
         p.res[7] = *(volatile unsigned*)(p.ctrl + 3);
+        p.res[8] = 1.0;
       }
     }
   }
@@ -609,21 +652,34 @@ __global__ void fill_kernel(double* x, long long n, double v) {
     x[k] = v;
 }
 
-template <int RPT, int CW>
+template <int RPT, int CW, int NTT>
 int launch(Context* ctx, Params& p, cudaStream_t st, int* launches) {
-  auto kern = sinkhorn_log_kernel<RPT, CW>;
-  const size_t smem = (size_t)STAGES * CW * p.ldc * 8 + STAGES * 8 + (2 * NW * CW + NW * 32) * 8;
-  if ((int)smem > ctx->smem_optin) return set_error(RWIG_E_UNSUPPORTED, "stage ring exceeds shared memory");
+  auto kern = (p.m == RPT * NTT) ? sinkhorn_log_kernel<RPT, CW, NTT, true> : sinkhorn_log_kernel<RPT, CW, NTT, false>;
+  p.ncol_max = (p.n + ctx->sm_count - 1) / ctx->sm_count;
+  const size_t smem = smem_bytes<CW, NTT / 32>(p.ldc, p.ncol_max);
+  if ((int)smem > ctx->smem_optin)
+    return set_error(RWIG_E_UNSUPPORTED, "stage ring and column state exceed shared memory");
   RWIG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem));
+  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTT, smem));
   if (occ < 1) return set_error(RWIG_E_UNSUPPORTED, "kernel does not fit on an SM");
   const int maxG = occ * ctx->sm_count;
   p.G = std::min(p.G, maxG);  // p.G arrives as the scratch-sized cap
   void* args[] = {&p};
-  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(p.G), dim3(NT), args, smem, st));
+  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(p.G), dim3(NTT), args, smem, st));
   ++*launches;
   return 0;
+}
+
+// Shape choice by rows m: 512 threads, 1, 2, 4, 8 or 16 rows per thread and
+// 16, 8, 4, 2 or 1 columns per stage (64 KB stages at the largest m of each).
+inline int dispatch_launch(Context* ctx, Params& p, cudaStream_t st, int* launches) {
+  const int m = p.m;
+  if (m <= 512) return launch<1, 16, 512>(ctx, p, st, launches);
+  if (m <= 1024) return launch<2, 8, 512>(ctx, p, st, launches);
+  if (m <= 2048) return launch<4, 4, 512>(ctx, p, st, launches);
+  if (m <= 4096) return launch<8, 2, 512>(ctx, p, st, launches);
+  return launch<16, 1, 512>(ctx, p, st, launches);
 }
 
 }  // namespace sklog
@@ -632,7 +688,7 @@ int launch(Context* ctx, Params& p, cudaStream_t st, int* launches) {
 enum {
   SL_LOGA = 0, SL_ELOGA, SL_LOGB, SL_ELOGB, SL_F0, SL_F1, SL_G, SL_MU, SL_ROWP, SL_ROWPM, SL_PART,
   SL_CTRL, SL_RES, SL_CRED, SL_AR, SL_BR, SL_RIDX, SL_CIDX, SL_HOST_C, SL_HOST_A, SL_HOST_B,
-  SL_HOST_P, SL_HOST_F, SL_HOST_G
+  SL_HOST_P, SL_HOST_F, SL_HOST_G, SL_FST, SL_GST, SL_FT, SL_GT, SL_KT, SL_U0, SL_U1
 };
 
 // Core of both log-Sinkhorn entry points: inputs on the device.
@@ -662,7 +718,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   const int m = (int)ri.size(), n = (int)ci.size();
   if (m == 0 || n == 0)
     return set_error(RWIG_E_INVALID, "a and b must each have at least one non-zero entry");
-  if (m > 16 * NT) return set_error(RWIG_E_UNSUPPORTED, "more than 8192 supported rows");
+  if (m > 8192) return set_error(RWIG_E_UNSUPPORTED, "more than 8192 supported rows");
   const bool reduced = (m != M) || (n != N);
   // the stage ring bulk-copies whole columns: C must start on 16 bytes and
   // have an even leading dimension, otherwise it is repacked first
@@ -707,7 +763,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   p.inv_eps = 1.0 / reg;
   p.max_iter = max_iter;
   p.tol = zero_tol;
-  const int Gmax = std::min(n, 2 * ctx->sm_count);
+  const int Gmax = std::min(std::min(n, 2 * ctx->sm_count), 320);  // merge loads assume G <= 20 warps' worth
   double* loga = (double*)scratch(ctx, SL_LOGA, sizeof(double) * m);
   double* eloga = (double*)scratch(ctx, SL_ELOGA, sizeof(double) * m);
   double* logb = (double*)scratch(ctx, SL_LOGB, sizeof(double) * n);
@@ -720,7 +776,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   p.rowpm = (double*)scratch(ctx, SL_ROWPM, sizeof(double) * (size_t)Gmax * m);
   p.part = (double*)scratch(ctx, SL_PART, sizeof(double) * (size_t)Gmax * 8);
   p.ctrl = (unsigned*)scratch(ctx, SL_CTRL, sizeof(unsigned) * 4);
-  p.res = (double*)scratch(ctx, SL_RES, sizeof(double) * 8);
+  p.res = (double*)scratch(ctx, SL_RES, sizeof(double) * 16);
   if (!loga || !eloga || !logb || !elogb || !p.f0 || !p.f1 || !p.g || !p.mu || !p.rowp || !p.rowpm ||
       !p.part || !p.ctrl || !p.res)
     return RWIG_E_NOMEM;
@@ -735,6 +791,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   p.f_out = f;
   p.g_out = g;
   p.G = Gmax;
+  p.do_final = 1;
 
   prep_kernel<<<std::max(1, (std::max(m, n) + 255) / 256), 256, 0, st>>>(
       ar, br, m, n, reg, loga, eloga, logb, elogb, p.f0, p.g, p.mu, p.ctrl);
@@ -753,28 +810,126 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
     }
   }
 
-  const int rpt_need = (m + NT - 1) / NT;
-  RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
-  int rc;
-  if (rpt_need <= 1) rc = launch<1, 16>(ctx, p, st, &launches);
-  else if (rpt_need <= 2) rc = launch<2, 8>(ctx, p, st, &launches);
-  else if (rpt_need <= 4) rc = launch<4, 4>(ctx, p, st, &launches);
-  else if (rpt_need <= 8) rc = launch<8, 2>(ctx, p, st, &launches);
-  else rc = launch<16, 1>(ctx, p, st, &launches);
-  if (rc != 0) return rc;
-  RWIG_CUDA_TRY(cudaGetLastError());
-  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
-
-  double res[8];
+  double res[16];
   unsigned ctrl[4];
-  RWIG_CUDA_TRY(cudaMemcpyAsync(res, p.res, sizeof(res), cudaMemcpyDeviceToHost, st));
-  RWIG_CUDA_TRY(cudaMemcpyAsync(ctrl, p.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
-  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
-  if (ctrl[2] != 0u) {
-    char buf[160];
-    std::snprintf(buf, sizeof(buf), "log-Sinkhorn kernel stopped by a bounded wait (error bits 0x%x)", ctrl[2]);
-    return set_error(RWIG_E_TIMEOUT, buf);
+  int fallbacks = 0;
+  // Runs one cooperative launch of `launch_fn` and reads back its results.
+  auto run = [&](auto&& launch_fn) -> int {
+    RWIG_CUDA_TRY(cudaMemsetAsync(p.ctrl, 0, sizeof(unsigned) * 4, st));
+    int r = launch_fn();
+    if (r != 0) return r;
+    RWIG_CUDA_TRY(cudaGetLastError());
+    ++launches;
+    RWIG_CUDA_TRY(cudaMemcpyAsync(res, p.res, sizeof(res), cudaMemcpyDeviceToHost, st));
+    RWIG_CUDA_TRY(cudaMemcpyAsync(ctrl, p.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
+    RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ctrl[2] != 0u) {
+      char buf[160];
+      std::snprintf(buf, sizeof(buf), "log-Sinkhorn kernel stopped by a bounded wait (error bits 0x%x)", ctrl[2]);
+      return set_error(RWIG_E_TIMEOUT, buf);
+    }
+    fallbacks += (int)ctrl[3];
+    return 0;
+  };
+  auto log_launch = [&]() { int dummy = 0; return dispatch_launch(ctx, p, st, &dummy); };
+
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
+  int rc = 0;
+  const bool scaled = option("log_sinkhorn.scaled", 1.0) != 0.0 && max_iter > 1;
+  if (!scaled) {
+    // every iteration in the log domain, one launch
+    rc = run(log_launch);
+    if (rc != 0) return rc;
+  } else {
+    // first iteration in the log domain (robust start), then the scaled form
+    // with absorptions; the plan / loss pass reads C with the final f, g
+    double* fst = (double*)scratch(ctx, SL_FST, sizeof(double) * m);
+    double* gst = (double*)scratch(ctx, SL_GST, sizeof(double) * n);
+    double* ft = (double*)scratch(ctx, SL_FT, sizeof(double) * m);
+    double* gt = (double*)scratch(ctx, SL_GT, sizeof(double) * n);
+    double* Kt = (double*)scratch(ctx, SL_KT, sizeof(double) * ldc * n);
+    double* u0 = (double*)scratch(ctx, SL_U0, sizeof(double) * m);
+    double* u1 = (double*)scratch(ctx, SL_U1, sizeof(double) * m);
+    if (!fst || !gst || !ft || !gt || !Kt || !u0 || !u1) return RWIG_E_NOMEM;
+    p.f_state = fst;
+    p.g_state = gst;
+    p.iter_cap = 1;
+    rc = run(log_launch);
+    if (rc != 0) return rc;
+    int it_now = (int)res[0];
+    double err_now = res[1];
+    bool finished = res[8] != 0.0;
+    bool final_done = finished;
+    const double tau = option("log_sinkhorn.tau", 100.0);
+    while (!finished) {
+      RWIG_CUDA_TRY(cudaMemcpyAsync(ft, fst, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+      RWIG_CUDA_TRY(cudaMemcpyAsync(gt, gst, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      rc = launch_absorb(ctx, Cr, ldc, ft, gt, m, n, 1.0 / reg, Kt, st);
+      if (rc != 0) return rc;
+      rc = launch_fill_ones(ctx, u0, m, st);
+      if (rc != 0) return rc;
+      launches += 2;
+      ScaledParams sp{};
+      sp.K = Kt;
+      sp.ldk = ldc;
+      sp.a = ar;
+      sp.b = br;
+      sp.loga = loga;
+      sp.logb = logb;
+      sp.m = m;
+      sp.n = n;
+      sp.G = Gmax;
+      sp.eps = reg;
+      sp.inv_eps = 1.0 / reg;
+      sp.tol = zero_tol;
+      sp.tau = tau;
+      sp.iter0 = it_now;
+      sp.max_iter = max_iter;
+      sp.err0 = err_now;
+      sp.u0 = u0;
+      sp.u1 = u1;
+      sp.ft = ft;
+      sp.gt = gt;
+      sp.rowp = p.rowp;
+      sp.part = p.part;
+      sp.ctrl = p.ctrl;
+      sp.res = p.res;
+      sp.f_state = fst;
+      sp.g_state = gst;
+      rc = run([&]() { return launch_scaled(ctx, sp, st); });
+      if (rc != 0) return rc;
+      it_now = (int)res[0];
+      err_now = res[1];
+      const int stt = (int)res[2];
+      if (stt == kScaledFinished) {
+        finished = true;
+      } else if (stt == kScaledUnsafe) {
+        // the rest of the solve in the log domain, from the state handed back
+        ++fallbacks;
+        RWIG_CUDA_TRY(cudaMemcpyAsync(p.f0, fst, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+        p.resume = 1;
+        p.iter0 = it_now;
+        p.err0 = err_now;
+        p.iter_cap = 0;
+        rc = run(log_launch);
+        if (rc != 0) return rc;
+        finished = final_done = true;
+      }
+    }
+    if (!final_done) {
+      // plan, loss and marginals from C with the final f, g (no iterations)
+      RWIG_CUDA_TRY(cudaMemcpyAsync(p.f0, fst, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+      p.resume = 1;
+      p.iter0 = it_now;
+      p.err0 = err_now;
+      p.max_iter = it_now;
+      p.iter_cap = 0;
+      rc = run(log_launch);
+      if (rc != 0) return rc;
+    }
   }
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
+  RWIG_CUDA_TRY(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f, kms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   cudaEventElapsedTime(&kms, ctx->evk, ctx->ev1);
@@ -794,7 +949,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   R.marg_l2_col = res[6];
   R.device_ms = ms;
   R.kernel_ms = kms;
-  R.fallback_events = (int)res[7];
+  R.fallback_events = fallbacks;
   R.kernel_launches = launches;
   R.support_m = m;
   R.support_n = n;
@@ -893,7 +1048,7 @@ constexpr size_t kOffRowP = kOffMu + kMaxN;
 constexpr size_t kOffRowPM = kOffRowP + (size_t)kMaxCtas * kMaxM;
 constexpr size_t kOffPart = kOffRowPM + (size_t)kMaxCtas * kMaxM;
 constexpr size_t kOffRes = kOffPart + (size_t)kMaxCtas * 8;
-constexpr size_t kOffCtrl = kOffRes + 8;  // 8 unsigned words = 4 doubles
+constexpr size_t kOffCtrl = kOffRes + 16;  // 8 unsigned words = 4 doubles
 constexpr size_t kDoubles = kOffCtrl + 4;  // about 10.0 MB in total
 
 static __device__ __align__(256) double g_scratch[kDoubles];
@@ -938,19 +1093,21 @@ __global__ void count_zero_masses(const double* a, const double* b, int m, int n
   if (threadIdx.x == 0) *out = s_cnt;
 }
 
-template <int RPT, int CW>
+template <int RPT, int CW, int NTT>
 int launch_noalloc(sklog::Params& p, int sms, int smem_optin, cudaStream_t st) {
   using namespace sklog;
-  auto kern = sinkhorn_log_kernel<RPT, CW>;
-  const size_t smem = (size_t)STAGES * CW * p.ldc * 8 + STAGES * 8 + (2 * NW * CW + NW * 32) * 8;
-  if ((int)smem > smem_optin) return set_error(RWIG_E_UNSUPPORTED, "stage ring exceeds shared memory");
+  auto kern = (p.m == RPT * NTT) ? sinkhorn_log_kernel<RPT, CW, NTT, true> : sinkhorn_log_kernel<RPT, CW, NTT, false>;
+  p.ncol_max = (p.n + std::min(sms, kMaxCtas) - 1) / std::min(sms, kMaxCtas);
+  const size_t smem = smem_bytes<CW, NTT / 32>(p.ldc, p.ncol_max);
+  if ((int)smem > smem_optin)
+    return set_error(RWIG_E_UNSUPPORTED, "stage ring and column state exceed shared memory");
   RWIG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem));
+  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTT, smem));
   if (occ < 1) return set_error(RWIG_E_UNSUPPORTED, "kernel does not fit on an SM");
   p.G = std::min(std::min(p.n, occ * sms), kMaxCtas);
   void* args[] = {&p};
-  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(p.G), dim3(NT), args, smem, st));
+  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(p.G), dim3(NTT), args, smem, st));
   return 0;
 }
 
@@ -1013,6 +1170,7 @@ extern "C" int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double
   p.cidx = nullptr;
   p.f_out = f;
   p.g_out = g;
+  p.do_final = 1;
 
   // every word the solver reads before writing is reset here: control words,
   // f, g and the column shifts
@@ -1029,11 +1187,10 @@ extern "C" int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double
                      "the no-allocation entry needs strictly positive a and b (zero masses need the "
                      "support-reducing rwig_sinkhorn_log_dev)");
 
-  const int rpt_need = (M + sklog::NT - 1) / sklog::NT;
-  if (rpt_need <= 1) rc = launch_noalloc<1, 16>(p, sms, smem_optin, st);
-  else if (rpt_need <= 2) rc = launch_noalloc<2, 8>(p, sms, smem_optin, st);
-  else if (rpt_need <= 4) rc = launch_noalloc<4, 4>(p, sms, smem_optin, st);
-  else rc = launch_noalloc<8, 2>(p, sms, smem_optin, st);
+  if (M <= 512) rc = launch_noalloc<1, 16, 512>(p, sms, smem_optin, st);
+  else if (M <= 1024) rc = launch_noalloc<2, 8, 512>(p, sms, smem_optin, st);
+  else if (M <= 2048) rc = launch_noalloc<4, 4, 512>(p, sms, smem_optin, st);
+  else rc = launch_noalloc<8, 2, 512>(p, sms, smem_optin, st);
   if (rc != 0) return rc;
   RWIG_CUDA_TRY(cudaGetLastError());
 

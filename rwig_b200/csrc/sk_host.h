@@ -1,0 +1,42 @@
+// sk_host.h -- host-side interface of the scaled-form log-Sinkhorn iterations
+// (sinkhorn_scaled.cu), used by the log-Sinkhorn driver (sinkhorn_log.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace rwig {
+
+enum { kScaledRunning = 0, kScaledFinished = 1, kScaledAbsorb = 2, kScaledUnsafe = 3 };
+
+struct ScaledParams {
+  const double* K;  // absorbed kernel, reduced m x n, leading dimension ldk
+  long long ldk;
+  const double* a;
+  const double* b;
+  const double* loga;
+  const double* logb;
+  int m, n, G;
+  double eps, inv_eps, tol, tau;
+  int iter0, max_iter;
+  double err0;
+  double* u0;  // current u (all ones after an absorption); ping-pong with u1
+  double* u1;
+  const double* ft;  // absorbed potentials f~, g~
+  const double* gt;
+  double* rowp;  // [G][m]
+  double* part;  // [G][8]
+  unsigned* ctrl;
+  double* res;       // iter, err, status
+  double* f_state;   // exit state (reduced)
+  double* g_state;
+  int ncol_max;
+};
+
+int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st);
+int launch_absorb(Context* ctx, const double* C, long long ldc, const double* ft, const double* gt, int m,
+                  int n, double inv_eps, double* K, cudaStream_t st);
+int launch_fill_ones(Context* ctx, double* x, int n, cudaStream_t st);
+
+}  // namespace rwig

@@ -138,3 +138,41 @@ def test_repeatable_bitwise():
     for k in ("P", "f", "g"):
         assert np.array_equal(r1[k], r2[k])
     assert r1["loss"] == r2["loss"] and r1["iter"] == r2["iter"]
+
+
+@pytest.fixture
+def engine_option():
+    """Sets engine options for one test and restores the defaults."""
+    L = rw.load()
+    set_opts = []
+
+    def _set(name, value):
+        assert L.rwig_set_option(name.encode(), float(value)) == 0
+        set_opts.append(name)
+
+    yield _set
+    L.rwig_set_option(b"log_sinkhorn.scaled", 1.0)
+    L.rwig_set_option(b"log_sinkhorn.tau", 100.0)
+
+
+@pytest.mark.parametrize("m,n,reg", [(700, 500, 0.02), (4096, 300, 0.01), (129, 1000, 0.05)])
+def test_log_domain_only_mode(engine_option, m, n, reg):
+    """Every iteration in the log domain (no scaled form): same parity bar."""
+    engine_option("log_sinkhorn.scaled", 0)
+    a, b, C = synth.sinkhorn_problem(m, n, 0.5, salt=m + 3 * n)
+    _compare(a, b, C, reg)
+
+
+@pytest.mark.parametrize("tau", [0.5, 5.0])
+def test_frequent_absorption(engine_option, tau):
+    """A small absorption bound rebuilds the scaled kernel many times; the
+    results must not move."""
+    engine_option("log_sinkhorn.tau", tau)
+    a, b, C = synth.sinkhorn_problem(900, 700, 0.5, salt=17)
+    got, ref = _compare(a, b, C, 0.01)
+    if tau < 1.0:
+        assert rw.last_report()["kernel_launches"] > 6  # more than one absorption
+
+
+def test_unknown_option_rejected():
+    assert rw.load().rwig_set_option(b"no.such.option", 1.0) == -1
