@@ -47,7 +47,9 @@ typedef struct rwig_report {
   double marg_l2_row;    /* || P 1 - a ||_2 */
   double marg_l2_col;    /* || P^T 1 - b ||_2 */
   double device_ms;      /* device time of the whole call (CUDA events) */
-  double kernel_ms;      /* device time of the main solver kernel alone */
+  double kernel_ms;      /* device time of the solver kernels (first launch to last) */
+  double sweep_ms;       /* device time of the launches that ran scaled-form iterations */
+  int sweep_iters;       /* iterations run by those launches */
   int fallback_events;   /* sweeps re-run with exact per-row / per-column minima */
   int kernel_launches;   /* engine kernels launched by the call */
   int support_m;         /* rows kept after dropping zero-mass entries of a */
@@ -64,7 +66,10 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "log_sinkhorn.scaled": 1 (default) runs the log-Sinkhorn iterations after
  *       the first in stabilised scaling form, 0 keeps every iteration in the
  *       log domain (same results within rounding; slower);
- *   "log_sinkhorn.tau": absorption bound on |log u|, |log v| (default 100). */
+ *   "log_sinkhorn.tau": absorption bound on |log u|, |log v| (default 100);
+ *   "log_sinkhorn.l2_hot": share of each CTA's column groups of the scaled
+ *       kernel copied with an L2 evict_last hint, the rest evict_first
+ *       (default 0: all evict_first; negative: no hint). */
 RWIG_API int rwig_set_option(const char* name, double value);
 
 /* ---- log-stabilised Sinkhorn ------------------------------------------

@@ -47,6 +47,8 @@ class Report(ctypes.Structure):
         ("marg_l2_col", _d),
         ("device_ms", _d),
         ("kernel_ms", _d),
+        ("sweep_ms", _d),
+        ("sweep_iters", _i),
         ("fallback_events", _i),
         ("kernel_launches", _i),
         ("support_m", _i),

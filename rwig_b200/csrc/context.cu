@@ -39,6 +39,8 @@ int init_device(int dev, Context** out) {
     RWIG_CUDA_TRY(cudaEventCreate(&c->ev0));
     RWIG_CUDA_TRY(cudaEventCreate(&c->ev1));
     RWIG_CUDA_TRY(cudaEventCreate(&c->evk));
+    RWIG_CUDA_TRY(cudaEventCreate(&c->evs0));
+    RWIG_CUDA_TRY(cudaEventCreate(&c->evs1));
     g_ctx[dev] = std::move(c);
   }
   *out = g_ctx[dev].get();
@@ -49,7 +51,7 @@ int init_device(int dev, Context** out) {
 namespace {
 std::mutex g_opt_mu;
 std::map<std::string, double> g_opts;
-const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau"};
+const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "log_sinkhorn.l2_hot"};
 }  // namespace
 
 double option(const char* name, double dflt) {
@@ -137,6 +139,8 @@ extern "C" void rwig_shutdown(void) {
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     cudaEventDestroy(c->evk);
+    cudaEventDestroy(c->evs0);
+    cudaEventDestroy(c->evs1);
     cudaStreamDestroy(c->stream);
     c.reset();
   }

@@ -18,7 +18,7 @@ struct Context {
   int sm_count = 0;
   int smem_optin = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk = nullptr, evs0 = nullptr, evs1 = nullptr;
   std::mutex mu;
   std::vector<void*> slots;
   std::vector<size_t> slot_bytes;

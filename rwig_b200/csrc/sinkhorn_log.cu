@@ -128,6 +128,10 @@ __global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
   ring.c1 = (int)(((long long)(cta + 1) * p.n) / G);
   ring.nst = (ring.c1 - ring.c0 + CW - 1) / CW;
   ring.q = 0;
+  // C streams through L2 once per sweep: mark it first to evict, which keeps
+  // the small per-iteration vectors and partials resident
+  ring.hot_groups = 0;
+  ring.pol_cold = l2_policy_evict_first();
   const int r0 = (int)(((long long)cta * m) / G), r1 = (int)(((long long)(cta + 1) * m) / G);
   int par = 0;
 
@@ -813,6 +817,8 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   double res[16];
   unsigned ctrl[4];
   int fallbacks = 0;
+  double sweep_ms = 0.0;
+  int sweep_iters = 0;
   // Runs one cooperative launch of `launch_fn` and reads back its results.
   auto run = [&](auto&& launch_fn) -> int {
     RWIG_CUDA_TRY(cudaMemsetAsync(p.ctrl, 0, sizeof(unsigned) * 4, st));
@@ -896,8 +902,20 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
       sp.res = p.res;
       sp.f_state = fst;
       sp.g_state = gst;
-      rc = run([&]() { return launch_scaled(ctx, sp, st); });
+      sp.l2_hot_fraction = option("log_sinkhorn.l2_hot", 0.0);
+      RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
+      rc = run([&]() {
+        int r = launch_scaled(ctx, sp, st);
+        if (r == 0) r = cudaEventRecord(ctx->evs1, st) == cudaSuccess ? 0 : RWIG_E_CUDA;
+        return r;
+      });
       if (rc != 0) return rc;
+      {
+        float sms = 0.f;
+        cudaEventElapsedTime(&sms, ctx->evs0, ctx->evs1);
+        sweep_ms += sms;
+        sweep_iters += (int)res[0] - sp.iter0;
+      }
       it_now = (int)res[0];
       err_now = res[1];
       const int stt = (int)res[2];
@@ -949,6 +967,8 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   R.marg_l2_col = res[6];
   R.device_ms = ms;
   R.kernel_ms = kms;
+  R.sweep_ms = sweep_ms;
+  R.sweep_iters = sweep_iters;
   R.fallback_events = fallbacks;
   R.kernel_launches = launches;
   R.support_m = m;

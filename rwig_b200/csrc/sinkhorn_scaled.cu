@@ -70,6 +70,11 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
   ring.c1 = (int)(((long long)(cta + 1) * p.n) / G);
   ring.nst = (ring.c1 - ring.c0 + CW - 1) / CW;
   ring.q = 0;
+  if (p.l2_hot_fraction >= 0.0) {
+    ring.hot_groups = (int)(p.l2_hot_fraction * ring.nst + 0.5);
+    ring.pol_hot = l2_policy_evict_last();
+    ring.pol_cold = l2_policy_evict_first();
+  }
   const int ncols = ring.c1 - ring.c0;
   const int r0 = (int)(((long long)cta * m) / G), r1 = (int)(((long long)(cta + 1) * m) / G);
   int par = 0;

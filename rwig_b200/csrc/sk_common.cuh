@@ -25,13 +25,23 @@ struct Ring {
   __device__ int group_cols(unsigned seq) const { return min(CW, c1 - group_begin(seq)); }
   __device__ double* slot(unsigned seq) const { return buf + (size_t)(seq % STAGES) * CW * ldc; }
 
+  // L2 priority: column groups below hot_groups are copied with an
+  // evict_last hint (they stay resident between sweeps), the rest with
+  // evict_first; hot_groups < 0 copies without a hint.
+  int hot_groups = -1;
+  uint64_t pol_hot = 0, pol_cold = 0;
+
   // thread 0 only
   __device__ void issue(unsigned seq) const {
-    const int jb = group_begin(seq);
-    const unsigned bytes = (unsigned)(group_cols(seq) * ldc * 8);
+    const int grp = (int)(seq % (unsigned)nst);
+    const int jb = c0 + grp * CW;
+    const unsigned bytes = (unsigned)(min(CW, c1 - jb) * ldc * 8);
     uint64_t* b = bar + (seq % STAGES);
     mbar_arrive_expect_tx(b, bytes);
-    bulk_g2s(slot(seq), C + (size_t)jb * ldc, bytes, b);
+    if (hot_groups < 0)
+      bulk_g2s(slot(seq), C + (size_t)jb * ldc, bytes, b);
+    else
+      bulk_g2s_hint(slot(seq), C + (size_t)jb * ldc, bytes, b, grp < hot_groups ? pol_hot : pol_cold);
   }
   __device__ bool wait(unsigned seq) const { return mbar_wait_bounded(bar + (seq % STAGES), (seq / STAGES) & 1u); }
 };

@@ -32,6 +32,7 @@ struct ScaledParams {
   double* f_state;   // exit state (reduced)
   double* g_state;
   int ncol_max;
+  double l2_hot_fraction;  // share of each CTA's column groups kept in L2 (evict_last); < 0: no hint
 };
 
 int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st);
