@@ -72,6 +72,25 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       (default 0: all evict_first; negative: no hint). */
 RWIG_API int rwig_set_option(const char* name, double value);
 
+/* ---- vanilla Sinkhorn --------------------------------------------------
+ * Replaces cuda_sinkhorn_vanilla (inst/include/cuda_interface.cuh:13-18,
+ * src/cuda_sinkhorn.cu:181) called from sinkhorn_vanilla_cuda (src/sinkhorn.cpp:51),
+ * with the semantics of the CPU path Sinkhorn::compute_vanilla
+ * (src/sinkhorn_impl_vanilla.cpp:18): zero masses dropped, `err >= zero_tol`
+ * continues, u, v zero off the support.  a: M, b: N, C: M x N.  Outputs (any
+ * may be NULL): P (M x N), grad_a (M, needs withgrad), u (M), v (N), loss.
+ */
+RWIG_API int rwig_sinkhorn_vanilla(double* P, double* grad_a, double* u, double* v, double* loss,
+                                   int* iter, double* err, const double* a, const double* b,
+                                   const double* C, int M, int N, double reg, int withgrad,
+                                   int max_iter, double zero_tol);
+
+/* Same on device pointers (see rwig_sinkhorn_log_dev). */
+RWIG_API int rwig_sinkhorn_vanilla_dev(double* P, double* grad_a, double* u, double* v, double* loss,
+                                       int* iter, double* err, const double* a, const double* b,
+                                       const double* C, int M, int N, double reg, int withgrad,
+                                       int max_iter, double zero_tol, void* stream);
+
 /* ---- log-stabilised Sinkhorn ------------------------------------------
  * Replaces the CPU-only Sinkhorn::compute_log (src/sinkhorn_impl_log.cpp:225)
  * reached from sinkhorn_log_cpp (src/sinkhorn.cpp:142); the reference has no

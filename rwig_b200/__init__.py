@@ -6,6 +6,7 @@ The compute path is the CUDA library rwig_b200/librwig_b200.so; importing this
 package does not load it until the first call.
 """
 from ._lib import RwigError, last_report, load  # noqa: F401
-from .api import check_sinkhorn_args, choose_sinkhorn_method, sinkhorn, sinkhorn_log_device  # noqa: F401
+from .api import (check_sinkhorn_args, choose_sinkhorn_method, sinkhorn, sinkhorn_log_device,  # noqa: F401
+                  sinkhorn_vanilla_device)
 
-__all__ = ["sinkhorn", "sinkhorn_log_device", "RwigError", "last_report", "load"]
+__all__ = ["sinkhorn", "sinkhorn_log_device", "sinkhorn_vanilla_device", "RwigError", "last_report", "load"]

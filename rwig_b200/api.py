@@ -116,6 +116,22 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def sinkhorn_vanilla_device(a, b, C_cm, reg, max_iter=1000, zero_tol=1e-6, P=None, u=None, v=None,
+                            stream=None) -> dict:
+    """Vanilla Sinkhorn on device buffers (layout as sinkhorn_log_device)."""
+    M, N = a.shape[0], b.shape[0]
+    if C_cm.numel() != M * N:
+        raise ValueError("C must hold M*N entries")
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+    rc = _lib.load().rwig_sinkhorn_vanilla_dev(_ptr(P), None, _ptr(u), _ptr(v), ctypes.byref(loss),
+                                               ctypes.byref(it), ctypes.byref(err), _ptr(a), _ptr(b),
+                                               _ptr(C_cm), M, N, float(reg), 0, int(max_iter),
+                                               float(zero_tol), st)
+    _lib.check(rc)
+    return {"loss": loss.value, "iter": it.value, "err": err.value, "return_status": rc}
+
+
 def sinkhorn_log_device(a, b, C_cm, reg, max_iter=1000, zero_tol=1e-6, P=None, f=None, g=None,
                         stream=None) -> dict:
     """Log-Sinkhorn on device buffers.  C_cm is the M x N cost in column-major

@@ -696,17 +696,25 @@ enum {
 };
 
 // Core of both log-Sinkhorn entry points: inputs on the device.
-static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double* grad_a, double* f,
-                               double* g, double* loss, int* iter, double* err, const double* a,
-                               const double* b, const double* C, int M, int N, double reg,
-                               int withgrad, int max_iter, double zero_tol) {
+__global__ void scatter_kernel(const double* x, const int* idx, int n, double* out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[idx ? idx[k] : k] = x[k];
+}
+
+// Shared driver of the vanilla and log-stabilised Sinkhorn entry points; inputs
+// on the device.  Log: f, g are the dual potentials (-inf off the support).
+// Vanilla: f, g receive the scalings u, v (0 off the support).
+static int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, double* grad_a, double* f,
+                           double* g, double* loss, int* iter, double* err, const double* a,
+                           const double* b, const double* C, int M, int N, double reg,
+                           int withgrad, int max_iter, double zero_tol) {
   using namespace sklog;
   reset_report();
   if (!a || !b || !C) return set_error(RWIG_E_INVALID, "a, b and C must be non-null");
   if (M < 1 || N < 1) return set_error(RWIG_E_INVALID, "M and N must be >= 1");
   if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
   if (withgrad && grad_a)
-    return set_error(RWIG_E_UNSUPPORTED, "log-Sinkhorn gradient is not available in this build");
+    return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient is not available in this build");
   int launches = 0;
 
   // support reduction (src/sinkhorn_impl_log.cpp:238-249): drop zero masses
@@ -792,8 +800,8 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   p.ldp = M;
   p.ridx = d_ridx;
   p.cidx = d_cidx;
-  p.f_out = f;
-  p.g_out = g;
+  p.f_out = vanilla ? nullptr : f;
+  p.g_out = vanilla ? nullptr : g;
   p.G = Gmax;
   p.do_final = 1;
 
@@ -804,12 +812,13 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
     if (P) {
       RWIG_CUDA_TRY(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)M * N, st));
     }
+    const double off = vanilla ? 0.0 : -INFINITY;  // sinkhorn_impl_vanilla.cpp:59-62, _log.cpp:267-268
     if (f && m < M) {
-      fill_kernel<<<(M + 255) / 256, 256, 0, st>>>(f, M, -INFINITY);
+      fill_kernel<<<(M + 255) / 256, 256, 0, st>>>(f, M, off);
       ++launches;
     }
     if (g && n < N) {
-      fill_kernel<<<(N + 255) / 256, 256, 0, st>>>(g, N, -INFINITY);
+      fill_kernel<<<(N + 255) / 256, 256, 0, st>>>(g, N, off);
       ++launches;
     }
   }
@@ -842,7 +851,97 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
   RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
   int rc = 0;
   const bool scaled = option("log_sinkhorn.scaled", 1.0) != 0.0 && max_iter > 1;
-  if (!scaled) {
+  if (vanilla) {
+    // K = exp(-C/eps) (sinkhorn_impl_vanilla.cpp:41); u = a / (K 1), then the
+    // scaled sweeps; P, loss and marginals from C with f = eps log u, g = eps log v
+    double* fst = (double*)scratch(ctx, SL_FST, sizeof(double) * m);
+    double* gst = (double*)scratch(ctx, SL_GST, sizeof(double) * n);
+    double* Kt = (double*)scratch(ctx, SL_KT, sizeof(double) * ldc * n);
+    double* u0 = (double*)scratch(ctx, SL_U0, sizeof(double) * m);
+    double* u1 = (double*)scratch(ctx, SL_U1, sizeof(double) * m);
+    if (!fst || !gst || !Kt || !u0 || !u1) return RWIG_E_NOMEM;
+    rc = launch_absorb(ctx, Cr, ldc, p.f0, p.g, m, n, 1.0 / reg, Kt, st);  // f0, g are zero here
+    if (rc != 0) return rc;
+    ++launches;
+    int it_now = 0;
+    double err_now = 1000.0;
+    if (max_iter > 0) {
+      rc = launch_fill_ones(ctx, u0, m, st);
+      if (rc != 0) return rc;
+      ++launches;
+      ScaledParams sp{};
+      sp.K = Kt;
+      sp.ldk = ldc;
+      sp.a = ar;
+      sp.b = br;
+      sp.loga = loga;
+      sp.logb = logb;
+      sp.m = m;
+      sp.n = n;
+      sp.G = Gmax;
+      sp.eps = reg;
+      sp.inv_eps = 1.0 / reg;
+      sp.tol = zero_tol;
+      sp.tau = INFINITY;
+      sp.iter0 = 0;
+      sp.max_iter = max_iter;
+      sp.err0 = 1000.0;
+      sp.u0 = u0;
+      sp.u1 = u1;
+      sp.ft = p.f0;
+      sp.gt = p.g;
+      sp.rowp = p.rowp;
+      sp.part = p.part;
+      sp.ctrl = p.ctrl;
+      sp.res = p.res;
+      sp.f_state = fst;
+      sp.g_state = gst;
+      sp.l2_hot_fraction = option("log_sinkhorn.l2_hot", 0.0);
+      sp.vanilla_init = 1;
+      RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
+      rc = run([&]() {
+        int r = launch_scaled(ctx, sp, st, true);
+        if (r == 0) r = cudaEventRecord(ctx->evs1, st) == cudaSuccess ? 0 : RWIG_E_CUDA;
+        return r;
+      });
+      if (rc != 0) return rc;
+      float sms = 0.f;
+      cudaEventElapsedTime(&sms, ctx->evs0, ctx->evs1);
+      sweep_ms += sms;
+      sweep_iters += (int)res[0];
+      it_now = (int)res[0];
+      err_now = res[1];
+    } else {
+      // no iteration: u = v = 1 (sinkhorn_impl_vanilla.cpp:96-97)
+      rc = launch_fill_ones(ctx, fst, m, st);
+      if (rc == 0) rc = launch_fill_ones(ctx, gst, n, st);
+      if (rc != 0) return rc;
+      launches += 2;
+    }
+    if (f) {
+      scatter_kernel<<<std::max(1, (m + 255) / 256), 256, 0, st>>>(fst, d_ridx, m, f);
+      ++launches;
+    }
+    if (g) {
+      scatter_kernel<<<std::max(1, (n + 255) / 256), 256, 0, st>>>(gst, d_cidx, n, g);
+      ++launches;
+    }
+    rc = launch_uv_to_potentials(ctx, fst, gst, m, n, reg, fst, gst, st);
+    if (rc != 0) return rc;
+    ++launches;
+    RWIG_CUDA_TRY(cudaMemcpyAsync(p.f0, fst, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+    p.f_state = fst;
+    p.g_state = gst;
+    p.resume = 1;
+    p.iter0 = it_now;
+    p.err0 = err_now;
+    p.max_iter = it_now;
+    p.iter_cap = 0;
+    rc = run(log_launch);
+    if (rc != 0) return rc;
+    res[0] = it_now;
+    res[1] = err_now;
+  } else if (!scaled) {
     // every iteration in the log domain, one launch
     rc = run(log_launch);
     if (rc != 0) return rc;
@@ -905,7 +1004,7 @@ static int sinkhorn_log_device(Context* ctx, cudaStream_t st, double* P, double*
       sp.l2_hot_fraction = option("log_sinkhorn.l2_hot", 0.0);
       RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
       rc = run([&]() {
-        int r = launch_scaled(ctx, sp, st);
+        int r = launch_scaled(ctx, sp, st, false);
         if (r == 0) r = cudaEventRecord(ctx->evs1, st) == cudaSuccess ? 0 : RWIG_E_CUDA;
         return r;
       });
@@ -988,14 +1087,25 @@ extern "C" int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, doubl
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  return sinkhorn_log_device(ctx, st, P, grad_a, f, g, loss, iter, err, a, b, C, M, N, reg, withgrad,
-                             max_iter, zero_tol);
+  return sinkhorn_device(ctx, st, false, P, grad_a, f, g, loss, iter, err, a, b, C, M, N, reg, withgrad,
+                         max_iter, zero_tol);
 }
 
-extern "C" int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g, double* loss,
-                                 int* iter, double* err, const double* a, const double* b,
-                                 const double* C, int M, int N, double reg, int withgrad,
-                                 int max_iter, double zero_tol) {
+extern "C" int rwig_sinkhorn_vanilla_dev(double* P, double* grad_a, double* u, double* v, double* loss,
+                                         int* iter, double* err, const double* a, const double* b,
+                                         const double* C, int M, int N, double reg, int withgrad,
+                                         int max_iter, double zero_tol, void* stream) {
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  return sinkhorn_device(ctx, st, true, P, grad_a, u, v, loss, iter, err, a, b, C, M, N, reg, withgrad,
+                         max_iter, zero_tol);
+}
+
+static int sinkhorn_host(bool vanilla, double* P, double* grad_a, double* f, double* g, double* loss,
+                         int* iter, double* err, const double* a, const double* b, const double* C, int M,
+                         int N, double reg, int withgrad, int max_iter, double zero_tol) {
   if (!a || !b || !C || M < 1 || N < 1) return set_error(RWIG_E_INVALID, "bad arguments");
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
@@ -1012,14 +1122,30 @@ extern "C" int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g
   RWIG_CUDA_TRY(cudaMemcpyAsync(dC, C, sizeof(double) * MN, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(da, a, sizeof(double) * M, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-  int rc = sinkhorn_log_device(ctx, st, dP, grad_a, df, dg, loss, iter, err, da, db, dC, M, N, reg,
-                               withgrad, max_iter, zero_tol);
+  int rc = sinkhorn_device(ctx, st, vanilla, dP, grad_a, df, dg, loss, iter, err, da, db, dC, M, N, reg,
+                           withgrad, max_iter, zero_tol);
   if (rc < 0) return rc;
   if (P) RWIG_CUDA_TRY(cudaMemcpyAsync(P, dP, sizeof(double) * MN, cudaMemcpyDeviceToHost, st));
   if (f) RWIG_CUDA_TRY(cudaMemcpyAsync(f, df, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
   if (g) RWIG_CUDA_TRY(cudaMemcpyAsync(g, dg, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   return rc;
+}
+
+extern "C" int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g, double* loss,
+                                 int* iter, double* err, const double* a, const double* b,
+                                 const double* C, int M, int N, double reg, int withgrad,
+                                 int max_iter, double zero_tol) {
+  return sinkhorn_host(false, P, grad_a, f, g, loss, iter, err, a, b, C, M, N, reg, withgrad, max_iter,
+                       zero_tol);
+}
+
+extern "C" int rwig_sinkhorn_vanilla(double* P, double* grad_a, double* u, double* v, double* loss,
+                                     int* iter, double* err, const double* a, const double* b,
+                                     const double* C, int M, int N, double reg, int withgrad,
+                                     int max_iter, double zero_tol) {
+  return sinkhorn_host(true, P, grad_a, u, v, loss, iter, err, a, b, C, M, N, reg, withgrad, max_iter,
+                       zero_tol);
 }
 
 // ===========================================================================

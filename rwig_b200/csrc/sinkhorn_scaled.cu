@@ -42,7 +42,11 @@ __host__ __device__ constexpr size_t smem_bytes(long long ldk, int ncol_max) {
          (size_t)6 * ncol_max * 8;
 }
 
-template <int RPT, int CW, int NTT, bool FULL>
+// VAN: vanilla Sinkhorn (Sinkhorn::_fwd_vanilla, src/sinkhorn_impl_vanilla.cpp:93-166)
+// on K = exp(-C/eps): the same sweeps, an initial pass u = a / (K 1) (:117),
+// the stopping error ||u o Kv - a||_2 + ||v o K^T u - b||_2 (:139), no
+// absorption; the exit state is u, v themselves.
+template <int RPT, int CW, int NTT, bool FULL, bool VAN>
 __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
   constexpr int NT = NTT;
   constexpr int NW = NTT / 32;
@@ -107,9 +111,10 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
   int iter = p.iter0;
   double err = p.err0, err_prev = p.err0;
   int status = kScaledRunning;
+  bool init = VAN && p.vanilla_init;  // the K 1 pass before the first iteration
 
-  while (ok && iter < p.max_iter && err >= p.tol) {
-    ++iter;
+  while (ok && (init || (iter < p.max_iter && err >= p.tol))) {
+    if (!init) ++iter;
     double u[RPT], r[RPT];
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
@@ -146,7 +151,7 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
         if (c == lane) mine_s = sum[c];
       const bool owner = lane < nc;
       const int jl = jb - ring.c0 + lane;
-      const double v_l = owner ? cb[jl] * rcp_nr(mine_s) : 0.0;
+      const double v_l = owner ? (init ? 1.0 : cb[jl] * rcp_nr(mine_s)) : 0.0;
       double v[CW];
 #pragma unroll
       for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);
@@ -172,10 +177,15 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
     if (w == 0) {
       double errc = 0.0, vmax = 0.0;
       for (int c = lane; c < ncols; c += 32) {
-        const double d = log(cv[c] * csum[c]) - clogb[c];
-        errc += d * d;
-        vmax = fmax(vmax, fabs(log(cv[c])));
-        if (!(csum[c] >= 1e-250 && csum[c] <= 1e250)) vmax = INFINITY;
+        if (VAN) {
+          const double d = cv[c] * csum[c] - cb[c];
+          errc += d * d;
+        } else {
+          const double d = log(cv[c] * csum[c]) - clogb[c];
+          errc += d * d;
+          vmax = fmax(vmax, fabs(log(cv[c])));
+          if (!(csum[c] >= 1e-250 && csum[c] <= 1e250)) vmax = INFINITY;
+        }
       }
       errc = warp_sum(errc);
 #pragma unroll
@@ -200,12 +210,17 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
           double tot = 0.0;
           for (int ww = 0; ww < NW; ++ww) tot += red3[ww * 32 + lane];
           const double ui = __ldcg(ucur + i);
-          const double d = log(ui * tot) - p.loga[i];
-          errr += d * d;
           const double un = p.a[i] / tot;
           unext[i] = un;
-          umax = fmax(umax, fabs(log(un)));
-          if (!(tot >= 1e-250 && tot <= 1e250)) unsafe = 1.0;
+          if (VAN) {
+            const double d = ui * tot - p.a[i];
+            errr += d * d;
+          } else {
+            const double d = log(ui * tot) - p.loga[i];
+            errr += d * d;
+            umax = fmax(umax, fabs(log(un)));
+            if (!(tot >= 1e-250 && tot <= 1e250)) unsafe = 1.0;
+          }
         }
         __syncthreads();
       }
@@ -252,7 +267,15 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
     __syncthreads();
     const double err_t = s_tot[0], drift = s_tot[1], unsafe = s_tot[2];
     __syncthreads();
-    if (unsafe != 0.0 || !(drift <= 1e300)) {
+    if (init) {
+      // u = a / (K 1); no iteration counted, no error
+      double* t = ucur;
+      ucur = unext;
+      unext = t;
+      init = false;
+      continue;
+    }
+    if (!VAN && (unsafe != 0.0 || !(drift <= 1e300))) {
       // hand back to the log domain from the state before this iteration
       status = kScaledUnsafe;
       --iter;
@@ -267,18 +290,19 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
     double* t = ucur;
     ucur = unext;
     unext = t;
-    if (drift > p.tau) {
+    if (!VAN && drift > p.tau) {
       status = kScaledAbsorb;
       break;
     }
   }
   if (ok && status == kScaledRunning) status = kScaledFinished;
 
-  // ---- exit state: f = f~ + eps log u, g = g~ + eps log v
+  // ---- exit state: f = f~ + eps log u, g = g~ + eps log v (vanilla: u, v)
   if (ok) {
-    for (int i = r0 + tid; i < r1; i += NT) p.f_state[i] = p.ft[i] + eps * log(__ldcg(ucur + i));
+    for (int i = r0 + tid; i < r1; i += NT)
+      p.f_state[i] = VAN ? __ldcg(ucur + i) : p.ft[i] + eps * log(__ldcg(ucur + i));
     for (int c = tid; c < ncols; c += NT)
-      p.g_state[ring.c0 + c] = cgt[c] + eps * log(status == kScaledUnsafe ? cvp[c] : cv[c]);
+      p.g_state[ring.c0 + c] = VAN ? cv[c] : cgt[c] + eps * log(status == kScaledUnsafe ? cvp[c] : cv[c]);
     if (cta == 0 && tid == 0) {
       p.res[0] = iter;
       p.res[1] = err;
@@ -307,9 +331,9 @@ __global__ void fill_ones(double* x, int n) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 1.0;
 }
 
-template <int RPT, int CW, int NTT>
+template <int RPT, int CW, int NTT, bool VAN>
 int launch_one(Context* ctx, ScaledParams& p, cudaStream_t st) {
-  auto kern = (p.m == RPT * NTT) ? scaled_kernel<RPT, CW, NTT, true> : scaled_kernel<RPT, CW, NTT, false>;
+  auto kern = (p.m == RPT * NTT) ? scaled_kernel<RPT, CW, NTT, true, VAN> : scaled_kernel<RPT, CW, NTT, false, VAN>;
   p.ncol_max = (p.n + ctx->sm_count - 1) / ctx->sm_count;
   const size_t smem = smem_bytes<CW, NTT / 32>(p.ldk, p.ncol_max);
   if ((int)smem > ctx->smem_optin)
@@ -326,14 +350,33 @@ int launch_one(Context* ctx, ScaledParams& p, cudaStream_t st) {
 
 }  // namespace skscaled
 
-int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st) {
+template <bool VAN>
+static int launch_by_rows(Context* ctx, ScaledParams& p, cudaStream_t st) {
   using namespace skscaled;
   const int m = p.m;
-  if (m <= 512) return launch_one<1, 16, 512>(ctx, p, st);
-  if (m <= 1024) return launch_one<2, 8, 512>(ctx, p, st);
-  if (m <= 2048) return launch_one<4, 4, 512>(ctx, p, st);
-  if (m <= 4096) return launch_one<8, 2, 512>(ctx, p, st);
-  return launch_one<16, 1, 512>(ctx, p, st);
+  if (m <= 512) return launch_one<1, 16, 512, VAN>(ctx, p, st);
+  if (m <= 1024) return launch_one<2, 8, 512, VAN>(ctx, p, st);
+  if (m <= 2048) return launch_one<4, 4, 512, VAN>(ctx, p, st);
+  if (m <= 4096) return launch_one<8, 2, 512, VAN>(ctx, p, st);
+  return launch_one<16, 1, 512, VAN>(ctx, p, st);
+}
+
+int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st, bool vanilla) {
+  return vanilla ? launch_by_rows<true>(ctx, p, st) : launch_by_rows<false>(ctx, p, st);
+}
+
+__global__ void uv_to_potentials(const double* u, const double* v, int m, int n, double eps, double* f,
+                                 double* g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = t; i < m; i += stride) f[i] = eps * log(u[i]);
+  for (int j = t; j < n; j += stride) g[j] = eps * log(v[j]);
+}
+
+int launch_uv_to_potentials(Context* ctx, const double* u, const double* v, int m, int n, double eps,
+                            double* f, double* g, cudaStream_t st) {
+  uv_to_potentials<<<std::max(1, (std::max(m, n) + 255) / 256), 256, 0, st>>>(u, v, m, n, eps, f, g);
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
 }
 
 int launch_absorb(Context* ctx, const double* C, long long ldc, const double* ft, const double* gt, int m,

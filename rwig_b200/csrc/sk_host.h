@@ -33,9 +33,12 @@ struct ScaledParams {
   double* g_state;
   int ncol_max;
   double l2_hot_fraction;  // share of each CTA's column groups kept in L2 (evict_last); < 0: no hint
+  int vanilla_init;         // vanilla mode: start with the pass u = a / (K 1)
 };
 
-int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st);
+int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st, bool vanilla);
+int launch_uv_to_potentials(Context* ctx, const double* u, const double* v, int m, int n, double eps,
+                            double* f, double* g, cudaStream_t st);
 int launch_absorb(Context* ctx, const double* C, long long ldc, const double* ft, const double* gt, int m,
                   int n, double inv_eps, double* K, cudaStream_t st);
 int launch_fill_ones(Context* ctx, double* x, int n, cudaStream_t st);
