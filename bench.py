@@ -1,11 +1,13 @@
-"""Benchmark: log-stabilised Sinkhorn, one 4096 x 4096 FP64 problem per solve.
+"""Benchmark of the rwig_b200 engine.
 
-Workload: a, b ~ Dirichlet(0.5) (n = m = 4096), support points uniform in
-[0,1]^2, squared-Euclidean cost normalised by its max, eps = 0.01,
-max_iter = 2000, zero_tol = 1e-9; outputs plan P, potentials f, g, loss.
+Default workload (the headline): log-stabilised Sinkhorn, one 4096 x 4096 FP64
+problem per solve, a, b ~ Dirichlet(0.5), support points uniform in [0,1]^2,
+squared-Euclidean cost normalised by its max, eps = 0.01, max_iter = 2000,
+zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
+--workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
 
 One step = one full solve.  `value` = solves/s over all ranks with inputs
 already resident in HBM (CUDA events on the launching stream, L2 flushed
@@ -30,27 +32,19 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-M = N = 4096
-REG = 0.01
-MAX_ITER = 2000
-TOL = 1e-9
-WORKLOAD = (f"log-Sinkhorn {M}x{N} FP64, Dirichlet(0.5) marginals, uniform points in [0,1]^2, "
-            f"squared-Euclidean cost / max, eps={REG}, max_iter={MAX_ITER}, tol={TOL:g}, outputs P,f,g,loss")
-METRIC = "log-Sinkhorn solves/s (4096x4096, FP64)"
-UNIT = "solves/s"
-
-
+DEFAULT_WORKLOAD = "log4096"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling entry point: one warm-up and one measured solve of a chosen size
     ap.add_argument("--single", action="store_true")
-    ap.add_argument("--m", type=int, default=M)
-    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--m", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--l2-hot", type=float, default=None, help="engine option log_sinkhorn.l2_hot")
     return ap.parse_args()
@@ -139,59 +133,224 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_solve_estimate(a, b, C, threads, iters_full, lo=2, hi=8):
-    """Time the oracle at two iteration counts and extrapolate one full solve.
-    Returns (seconds per solve, description of the sample)."""
-    import oracle
-    t = {}
-    for it in (lo, hi):
-        t0 = time.perf_counter()
-        oracle.sinkhorn_log(a, b, C, REG, max_iter=it, zero_tol=0.0, n_threads=threads)
-        t[it] = time.perf_counter() - t0
-    per_iter = max((t[hi] - t[lo]) / (hi - lo), 1e-9)
-    fixed = max(t[lo] - lo * per_iter, 0.0)
-    secs = fixed + iters_full * per_iter
-    sample = (f"{lo}- and {hi}-iteration runs of the same {M}x{N} problem ({threads} threads), "
-              f"extrapolated to a {iters_full}-iteration solve: {per_iter * 1e3:.1f} ms/iteration, "
-              f"{fixed * 1e3:.0f} ms fixed")
-    return secs, sample
+class SinkhornWorkload:
+    """One full solve of a single Sinkhorn problem per step."""
+
+    higher_is_better = True
+
+    def __init__(self, method, m, n, reg, alpha, max_iter, tol):
+        self.method, self.m, self.n, self.reg = method, m, n, reg
+        self.alpha, self.max_iter, self.tol = alpha, max_iter, tol
+        self.unit = "solves/s"
+        kind = "log-Sinkhorn" if method == "log" else "vanilla Sinkhorn"
+        self.metric = f"{kind} solves/s ({m}x{n}, FP64)"
+        self.desc = (f"{kind} {m}x{n} FP64, Dirichlet({alpha:g}) marginals, uniform points in [0,1]^2, "
+                     f"squared-Euclidean cost / max, eps={reg:g}, max_iter={max_iter}, tol={tol:g}, "
+                     f"outputs P, {'f, g' if method == 'log' else 'u, v'}, loss")
+
+    def inputs(self):
+        from rwig_b200 import synth
+        return synth.sinkhorn_problem(self.m, self.n, self.alpha, 2)
+
+    def cpu_seconds(self, threads, iters_full):
+        """CPU port time of one solve: bounded runs at two iteration counts,
+        extrapolated to the solve's iteration count."""
+        import oracle
+        a, b, C = self.inputs()
+        if self.method == "vanilla":
+            threads = 1  # the reference's vanilla path runs on one BLAS thread
+            t0 = time.perf_counter()
+            k = 0
+            while True:
+                oracle.sinkhorn_vanilla(a, b, C, self.reg, max_iter=self.max_iter, zero_tol=self.tol)
+                k += 1
+                if time.perf_counter() - t0 > 2.0:
+                    break
+            secs = (time.perf_counter() - t0) / k
+            return secs, threads, f"{k} full solves of the same problem, 1 thread"
+        lo, hi = 2, 8
+        t = {}
+        for it in (lo, hi):
+            t0 = time.perf_counter()
+            oracle.sinkhorn_log(a, b, C, self.reg, max_iter=it, zero_tol=0.0, n_threads=threads, want_P=True)
+            t[it] = time.perf_counter() - t0
+        per_iter = max((t[hi] - t[lo]) / (hi - lo), 1e-9)
+        fixed = max(t[lo] - lo * per_iter, 0.0)
+        secs = fixed + iters_full * per_iter
+        sample = (f"{lo}- and {hi}-iteration runs of the same {self.m}x{self.n} problem ({threads} threads), "
+                  f"extrapolated to a {iters_full}-iteration solve: {per_iter * 1e3:.1f} ms/iteration, "
+                  f"{fixed * 1e3:.0f} ms fixed")
+        return secs, threads, sample
+
+    def reference_iters(self):
+        """Iteration count of the full solve (run by the CPU port once, cached)."""
+        import oracle
+        if self.method == "vanilla":
+            a, b, C = self.inputs()
+            return oracle.sinkhorn_vanilla(a, b, C, self.reg, max_iter=self.max_iter, zero_tol=self.tol)["iter"]
+        # the 4096^2 log solve takes ~30 s on the CPU port: its count is recorded
+        # here and re-checked by tests/test_gpu_sinkhorn_log.py::test_benchmark_workload_iterations
+        return {("log", 4096, 4096, 0.01): 221}.get((self.method, self.m, self.n, self.reg), self.max_iter)
+
+    def run(self, args, dev, world, rank, clocks_cls):
+        import numpy as np
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        m, n = self.m, self.n
+        a, b, C = self.inputs()
+        ta, tb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        tC = torch.from_numpy(C.T).to(dev)  # column-major m x n as a contiguous (n, m) block
+        P = torch.empty((n, m), dtype=torch.float64, device=dev)
+        x = torch.empty(m, dtype=torch.float64, device=dev)
+        y = torch.empty(n, dtype=torch.float64, device=dev)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+        stream = torch.cuda.current_stream()
+        dev_fn = rw.sinkhorn_log_device if self.method == "log" else rw.sinkhorn_vanilla_device
+
+        def solve():
+            if self.method == "log":
+                return dev_fn(ta, tb, tC, self.reg, self.max_iter, self.tol, P=P, f=x, g=y, stream=stream)
+            return dev_fn(ta, tb, tC, self.reg, self.max_iter, self.tol, P=P, u=x, v=y, stream=stream)
+
+        for _ in range(args.warmup):
+            flush.zero_()
+            solve()
+        torch.cuda.synchronize()
+
+        def barrier():
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            torch.cuda.synchronize()
+
+        times, reps, iters = [], [], []
+        with clocks_cls(dev.index) as clocks:
+            barrier()
+            for _ in range(args.steps):
+                flush.zero_()  # L2 flush between timed steps (outside the timed region)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = solve()
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                reps.append(rw.last_report())
+                iters.append(r["iter"])
+            barrier()
+        tot_ms = max_over_ranks(sum(times), world, dev)
+        value = args.steps * world / (tot_ms / 1e3)
+
+        # end to end through the host-pointer C ABI, pinned host buffers
+        hC = torch.from_numpy(C.T.copy()).pin_memory()
+        ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+        hP = torch.empty((n, m), dtype=torch.float64).pin_memory()
+        hx = torch.empty(m, dtype=torch.float64).pin_memory()
+        hy = torch.empty(n, dtype=torch.float64).pin_memory()
+        L = _lib.load()
+        fn = L.rwig_sinkhorn_log if self.method == "log" else L.rwig_sinkhorn_vanilla
+        dp = ctypes.POINTER(ctypes.c_double)
+
+        def cp(t):
+            return ctypes.cast(ctypes.c_void_p(t.data_ptr()), dp)
+
+        def host_solve():
+            loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+            rc = fn(cp(hP), None, cp(hx), cp(hy), ctypes.byref(loss), ctypes.byref(it), ctypes.byref(err),
+                    cp(ha), cp(hb), cp(hC), m, n, self.reg, 0, self.max_iter, self.tol)
+            _lib.check(rc)
+
+        host_solve()
+        barrier()
+        e2e_s = 0.0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            host_solve()
+            e2e_s += time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, world, dev)
+        assert np.array_equal(hP.numpy(), P.cpu().numpy()), "host and device entry points disagree"
+        if rank != 0:
+            return None
+
+        peak, peak_kind = measured_peaks()
+        it_mean = sum(iters) / len(iters)
+        kms = sum(r["kernel_ms"] for r in reps) / len(reps)
+        s_ms = sum(r["sweep_ms"] for r in reps) / len(reps)
+        s_it = sum(r["sweep_iters"] for r in reps) / len(reps)
+        # dominant kernel: the scaled sweep kernel; algorithmic bytes = one read
+        # of the m x n kernel matrix per iteration it runs
+        alg_bytes = s_it * m * n * 8
+        achieved = alg_bytes / (s_ms / 1e3) / 1e9 if s_ms > 0 else None
+        tr = profiled_traffic(s_it) if (self.method, m, n) == ("log", 4096, 4096) else None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": tr, "peak_source": peak_kind,
+                "kernel": "scaled_kernel (Sinkhorn sweep)", "kernel_ms_per_solve": s_ms,
+                "kernel_iters_per_solve": s_it, "alg_bytes_per_solve": alg_bytes,
+                "all_kernels_ms_per_solve": kms}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1, int(round(it_mean)))
+            cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
+        return {"value": value, "ms_per_step": tot_ms / args.steps,
+                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
+                           "iterations_per_solve": it_mean, "l2": "flushed between steps (256 MB write)"},
+                "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
+                        "h2d_bytes_per_step": (m * n + m + n) * 8, "d2h_bytes_per_step": (m * n + m + n) * 8 + 8},
+                "gpu_launches": sum(r["kernel_launches"] for r in reps), "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clocks.summary()}
+
+    def reference(self, args):
+        threads = os.cpu_count() or 1
+        iters = self.reference_iters()
+        for _ in range(args.warmup):
+            self.cpu_seconds(threads, iters)
+        secs, cores, sample = [], 1, ""
+        for _ in range(args.steps):
+            s_, cores, sample = self.cpu_seconds(threads, iters)
+            secs.append(s_)
+        return sum(secs), cores, sample
+
+
+WORKLOADS = {
+    "log4096": SinkhornWorkload("log", 4096, 4096, 0.01, 0.5, 2000, 1e-9),
+    "vanilla256": SinkhornWorkload("vanilla", 256, 256, 0.1, 1.0, 1000, 1e-9),
+}
+
+
+def max_over_ranks(x, world, dev):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def base_line(wl, args, world):
+    return {"metric": wl.metric, "unit": wl.unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": wl.higher_is_better, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic"}
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    import numpy as np  # noqa: F401
-    from rwig_b200 import synth
-    a, b, C = synth.log_config(M, N)
-    threads = os.cpu_count() or 1
-    # one step = one estimated full solve, timed as two bounded oracle runs
-    for _ in range(args.warmup):
-        cpu_solve_estimate(a, b, C, threads, MAX_ITER, lo=1, hi=2)
-    secs = []
-    sample = ""
-    for _ in range(args.steps):
-        s, sample = cpu_solve_estimate(a, b, C, threads, MAX_ITER)
-        secs.append(s)
-    tot = sum(secs)
+    wl = WORKLOADS[args.workload]
+    tot, cores, sample = wl.reference(args)
     value = args.steps / tot
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "cpu"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line = {"impl": "reference", **base_line(wl, args, args.gpus), "value": value,
+            "ms_per_step": tot / args.steps * 1e3, "config": {"workload": wl.desc, "parallelism": "cpu"},
+            "cpu_baseline": {"value": value, "unit": wl.unit, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_engine(args):
-    import numpy as np
     import torch
-
-    import rwig_b200 as rw
-    from rwig_b200 import _lib, synth
-
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -199,127 +358,10 @@ def run_engine(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
-    a, b, C = synth.log_config(M, N)
-    ta = torch.from_numpy(a).to(dev)
-    tb = torch.from_numpy(b).to(dev)
-    tC = torch.from_numpy(C.T).to(dev)  # column-major M x N as a contiguous (N, M) block
-    P = torch.empty((N, M), dtype=torch.float64, device=dev)
-    f = torch.empty(M, dtype=torch.float64, device=dev)
-    g = torch.empty(N, dtype=torch.float64, device=dev)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
-    stream = torch.cuda.current_stream()
-
-    def solve():
-        return rw.sinkhorn_log_device(ta, tb, tC, REG, MAX_ITER, TOL, P=P, f=f, g=g, stream=stream)
-
-    for _ in range(args.warmup):
-        flush.zero_()
-        solve()
-    torch.cuda.synchronize()
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    times, kern, iters, launches, sweep_ms, sweep_it = [], [], [], 0, [], []
-    with ClockSampler(local) as clocks:
-        barrier()
-        for _ in range(args.steps):
-            flush.zero_()  # L2 flush between timed steps (outside the timed region)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            r = solve()
-            e1.record(stream)
-            e1.synchronize()
-            rep = rw.last_report()
-            times.append(e0.elapsed_time(e1))
-            kern.append(rep["kernel_ms"])
-            sweep_ms.append(rep["sweep_ms"])
-            sweep_it.append(rep["sweep_iters"])
-            iters.append(r["iter"])
-            launches += rep["kernel_launches"]
-        barrier()
-    tot_ms = sum(times)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = args.steps * world / (tot_ms / 1e3)
-
-    # end to end through the host-pointer C ABI, pinned host buffers
-    hC = torch.from_numpy(C.T.copy()).pin_memory()
-    ha = torch.from_numpy(a).pin_memory()
-    hb = torch.from_numpy(b).pin_memory()
-    hP = torch.empty((N, M), dtype=torch.float64).pin_memory()
-    hf = torch.empty(M, dtype=torch.float64).pin_memory()
-    hg = torch.empty(N, dtype=torch.float64).pin_memory()
-    L = _lib.load()
-    dp = ctypes.POINTER(ctypes.c_double)
-
-    def cp(t):
-        return ctypes.cast(ctypes.c_void_p(t.data_ptr()), dp)
-
-    def host_solve():
-        loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
-        rc = L.rwig_sinkhorn_log(cp(hP), None, cp(hf), cp(hg), ctypes.byref(loss), ctypes.byref(it),
-                                 ctypes.byref(err), cp(ha), cp(hb), cp(hC), M, N, REG, 0, MAX_ITER, TOL)
-        _lib.check(rc)
-        return loss.value
-
-    host_solve()
-    barrier()
-    e2e_s = 0.0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        host_solve()
-        e2e_s += time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = args.steps * world / e2e_s
-    assert np.array_equal(hP.numpy(), P.cpu().numpy()), "host and device entry points disagree"
-
-    line = None
+    wl = WORKLOADS[args.workload]
+    out = wl.run(args, dev, world, rank, ClockSampler)
     if rank == 0:
-        peak, peak_kind = measured_peaks()
-        it_mean = sum(iters) / len(iters)
-        kms = sum(kern) / len(kern)
-        # dominant kernel: the scaled-form sweep kernel; algorithmic bytes = one
-        # read of the M x N kernel matrix per iteration it runs
-        s_ms = sum(sweep_ms) / len(sweep_ms)
-        s_it = sum(sweep_it) / len(sweep_it)
-        alg_bytes = s_it * M * N * 8
-        achieved = alg_bytes / (s_ms / 1e3) / 1e9 if s_ms > 0 else None
-        tr = profiled_traffic(s_it)
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None,
-                "traffic": tr, "peak_source": peak_kind,
-                "kernel": "scaled_kernel (scaled-form log-Sinkhorn sweep)", "kernel_ms_per_solve": s_ms,
-                "kernel_iters_per_solve": s_it, "alg_bytes_per_solve": alg_bytes,
-                "all_kernels_ms_per_solve": kms,
-                "all_kernels_alg_GBps": (it_mean + 2) * M * N * 8 / (kms / 1e3) / 1e9}
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            secs, sample = cpu_solve_estimate(a, b, C, threads, int(round(it_mean)))
-            cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
-                           "iterations_per_solve": it_mean, "l2": "flushed between steps (256 MB write)"},
-                "e2e": {"value": e2e_value, "unit": UNIT,
-                        "h2d_bytes_per_step": (M * N + M + N) * 8,
-                        "d2h_bytes_per_step": (M * N + M + N) * 8 + 8},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clocks.summary()}
-        print(json.dumps(line), flush=True)
+        print(json.dumps({**base_line(wl, args, world), **out}), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -328,7 +370,7 @@ def run_engine(args):
 
 
 def run_single(args):
-    """One warm-up plus one solve of an m x n problem with a fixed iteration
+    """One warm-up plus one solve of an m x n log problem with a fixed iteration
     count (tol 0): the small case the kernel profiles are captured on."""
     import torch
 
@@ -342,7 +384,7 @@ def run_single(args):
     tC = torch.from_numpy(C.T).to(dev)
     P = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
     for _ in range(2):
-        r = rw.sinkhorn_log_device(ta, tb, tC, REG, args.iters, 0.0, P=P)
+        r = rw.sinkhorn_log_device(ta, tb, tC, 0.01, args.iters, 0.0, P=P)
     torch.cuda.synchronize()
     rep = rw.last_report()
     print(json.dumps({"m": args.m, "n": args.n, "iter": r["iter"], "kernel_ms": rep["kernel_ms"],

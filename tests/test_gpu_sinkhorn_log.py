@@ -176,3 +176,28 @@ def test_frequent_absorption(engine_option, tau):
 
 def test_unknown_option_rejected():
     assert rw.load().rwig_set_option(b"no.such.option", 1.0) == -1
+
+
+def test_benchmark_workload_iterations():
+    """The 4096 x 4096 log workload converges in the iteration count the CPU
+    reference arm of bench.py extrapolates to (the CPU port's own full solve of
+    it takes ~30 s, so the count is recorded there)."""
+    import bench
+    wl = bench.WORKLOADS["log4096"]
+    a, b, C = wl.inputs()
+    r = rw.sinkhorn(a, b, C, {"reg": wl.reg, "method": "log", "max_iter": wl.max_iter, "zero_tol": wl.tol})
+    assert r["iter"] == wl.reference_iters()
+
+
+def test_full_size_against_oracle_fixture():
+    """The 4096 x 4096 benchmark solve against the CPU oracle's full solve
+    (tests/golden/log4096_oracle.npz, made by tests/golden/make_log4096.py)."""
+    import os
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "log4096_oracle.npz"))
+    a, b, C = synth.log_config(4096, 4096)
+    got = rw.sinkhorn(a, b, C, {"reg": 0.01, "method": "log", "max_iter": 2000, "zero_tol": 1e-9})
+    assert got["iter"] == int(ref["iter"]) and got["return_status"] == int(ref["return_status"])
+    sc = dual_scale(ref["f"], ref["g"])
+    assert rel_err(got["f"], ref["f"], sc) <= PARITY_TOL
+    assert rel_err(got["g"], ref["g"], sc) <= PARITY_TOL
+    assert abs(got["loss"] - float(ref["loss"])) <= PARITY_TOL * abs(float(ref["loss"]))
