@@ -116,6 +116,14 @@ RWIG_API int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, double*
  * y_engine and y_cuda (device).  Used by the test suite to bound its error. */
 RWIG_API int rwig_selftest_exp(const double* x, double* y_engine, double* y_cuda, int n, void* stream);
 
+/* Self-check of the engine's FP64 tensor-core GEMM (no counterpart in the
+ * reference): Y (Mo x S, ldy) = op(K) X with op(K) = K (trans = 0) or K^T
+ * (trans = 1), K column-major with even ldk, X (Kd x S, ldx); all device
+ * pointers.  splits <= 0 picks the split-K count.  Returns the split count. */
+RWIG_API int rwig_selftest_dgemm(const double* K, long long ldk, int trans, int Mo, int Kd, int S,
+                                 const double* X, long long ldx, double* Y, long long ldy, int splits,
+                                 void* stream);
+
 /* Allocation-free log-Sinkhorn.  No counterpart in the reference: it exists for
  * callers that cannot let a library allocate device memory (a host framework
  * that owns the GPU's memory pool, a process under a hard device-memory quota,

@@ -74,6 +74,8 @@ SIGNATURES = {
     "rwig_sinkhorn_log_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _i,
                                    _d, _vp]),
     "rwig_selftest_exp": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "rwig_selftest_dgemm": (_i, [_vp, ctypes.c_longlong, _i, _i, _i, _i, _vp, ctypes.c_longlong, _vp,
+                                 ctypes.c_longlong, _i, _vp]),
     "rwig_sinkhorn_log_noalloc": (_i, [_vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _d, _vp]),
 }
 
