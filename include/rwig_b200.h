@@ -54,6 +54,7 @@ typedef struct rwig_report {
   int kernel_launches;   /* engine kernels launched by the call */
   int support_m;         /* rows kept after dropping zero-mass entries of a */
   int support_n;         /* columns kept after dropping zero-mass entries of b */
+  double bary_norm;      /* barycenters: sum of the un-normalised barycenter b */
 } rwig_report;
 
 /* ---- context ---------------------------------------------------------- */
@@ -110,6 +111,39 @@ RWIG_API int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, double*
                           int* iter, double* err, const double* a, const double* b,
                           const double* C, int M, int N, double reg, int withgrad,
                           int max_iter, double zero_tol, void* stream);
+
+/* ---- Wasserstein barycenters -------------------------------------------
+ * rwig_barycenter_parallel replaces cuda_barycenter_parallel
+ * (inst/include/cuda_interface.cuh:20-26, src/cuda_barycenter.cu:268) called
+ * from barycenter_parallel_cuda (src/barycenter.cpp:67), with the semantics of
+ * Barycenter::compute_parallel (src/barycenter_impl_parallel.cpp:19);
+ * rwig_barycenter_log is the GPU form of the CPU-only Barycenter::compute_log
+ * (src/barycenter_impl_log.cpp:23, reached from src/barycenter.cpp:168).
+ * A: M x S histograms, w: S weights, C: M x N cost, b_ext: N (only read when
+ * withgrad).  Outputs (any may be NULL): parallel U (M x S), V (N x S); log
+ * F (M x S), G (N x S); b (N, normalised); grad_A (M x S), grad_w (S), loss
+ * (need withgrad).  S <= 64.
+ */
+RWIG_API int rwig_barycenter_parallel(double* U, double* V, double* b, double* grad_A, double* grad_w,
+                                      double* loss, int* iter, double* err, const double* A,
+                                      const double* w, const double* C, const double* b_ext, int M,
+                                      int N, int S, double reg, int withgrad, int max_iter,
+                                      double zero_tol);
+RWIG_API int rwig_barycenter_log(double* F, double* G, double* b, double* grad_A, double* grad_w,
+                                 double* loss, int* iter, double* err, const double* A, const double* w,
+                                 const double* C, const double* b_ext, int M, int N, int S, double reg,
+                                 int withgrad, int max_iter, double zero_tol);
+/* Same on device pointers, work queued on `stream`; loss / iter / err are host pointers. */
+RWIG_API int rwig_barycenter_parallel_dev(double* U, double* V, double* b, double* grad_A,
+                                          double* grad_w, double* loss, int* iter, double* err,
+                                          const double* A, const double* w, const double* C,
+                                          const double* b_ext, int M, int N, int S, double reg,
+                                          int withgrad, int max_iter, double zero_tol, void* stream);
+RWIG_API int rwig_barycenter_log_dev(double* F, double* G, double* b, double* grad_A, double* grad_w,
+                                     double* loss, int* iter, double* err, const double* A,
+                                     const double* w, const double* C, const double* b_ext, int M,
+                                     int N, int S, double reg, int withgrad, int max_iter,
+                                     double zero_tol, void* stream);
 
 /* Self-check of the engine's internal exponential (no counterpart in the
  * reference): evaluates it and CUDA's exp on n device doubles x, writing

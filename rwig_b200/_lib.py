@@ -53,6 +53,7 @@ class Report(ctypes.Structure):
         ("kernel_launches", _i),
         ("support_m", _i),
         ("support_n", _i),
+        ("bary_norm", _d),
     ]
 
     def as_dict(self):
@@ -73,6 +74,14 @@ SIGNATURES = {
     "rwig_sinkhorn_log": (_i, [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _i, _i, _d, _i, _i, _d]),
     "rwig_sinkhorn_log_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _i,
                                    _d, _vp]),
+    "rwig_barycenter_parallel": (_i, [_dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp, _i, _i, _i,
+                                      _d, _i, _i, _d]),
+    "rwig_barycenter_log": (_i, [_dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp, _i, _i, _i, _d, _i,
+                                 _i, _d]),
+    "rwig_barycenter_parallel_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _vp, _i, _i,
+                                          _i, _d, _i, _i, _d, _vp]),
+    "rwig_barycenter_log_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _vp, _i, _i, _i, _d,
+                                     _i, _i, _d, _vp]),
     "rwig_selftest_exp": (_i, [_vp, _vp, _vp, _i, _vp]),
     "rwig_selftest_dgemm": (_i, [_vp, ctypes.c_longlong, _i, _i, _i, _i, _vp, ctypes.c_longlong, _vp,
                                  ctypes.c_longlong, _i, _vp]),

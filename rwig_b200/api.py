@@ -105,6 +105,78 @@ def sinkhorn(a, b, C, sinkhorn_control: dict | None = None) -> dict:
     return out
 
 
+BARYCENTER_ARGS = SINKHORN_ARGS
+
+
+def check_barycenter_args(ctrl: dict | None) -> dict:
+    """Fill and validate a barycenter control list (R/check_args.R:193-271)."""
+    ctrl = dict(ctrl or {})
+    bad = [k for k in ctrl if k not in BARYCENTER_ARGS]
+    if bad:
+        raise ValueError(", ".join(bad) + " not matching one of the barycenter arguments: " +
+                         ", ".join(f'"{a}"' for a in BARYCENTER_ARGS))
+    defaults = dict(reg=0.1, with_grad=False, use_cuda=True, n_threads=0, method="auto", threshold=0.1,
+                    max_iter=1000, zero_tol=1e-6, verbose=0)
+    for k, v in defaults.items():
+        if ctrl.get(k) is None:
+            ctrl[k] = v
+    if ctrl["method"] not in ("auto", "parallel", "log"):
+        raise ValueError('method must be from: "auto", "parallel", or "log"')
+    return ctrl
+
+
+def barycenter(A, C, w, b_ext=None, barycenter_control: dict | None = None) -> dict:
+    """Wasserstein barycenter of the columns of A (R/barycenter.R:90)."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    C = np.asfortranarray(np.asarray(C, dtype=np.float64))
+    if A.ndim != 2:
+        raise ValueError("A must be a numeric matrix!")
+    if C.ndim != 2:
+        raise ValueError("C must be a numeric matrix!")
+    w = np.asarray(w, dtype=np.float64)
+    if w.ndim != 1:
+        raise ValueError("w must be a numeric vector!")
+    if A.shape[0] != C.shape[0]:
+        raise ValueError("number of rows of A and C must equal!")
+    ctrl = check_barycenter_args(barycenter_control)
+    reg = ctrl["reg"]
+    if not isinstance(reg, (int, float)) or isinstance(reg, bool):
+        raise ValueError("reg must be a single value")
+    reg = float(reg)
+    with_grad = bool(ctrl["with_grad"])
+    if with_grad and b_ext is None:
+        raise ValueError("you must supply the `b_ext` with `with_grad = TRUE`!")
+    method = ctrl["method"]
+    if method == "auto":  # R/barycenter.R:168-182
+        method = "log" if choose_sinkhorn_method(C, reg, ctrl["threshold"]) == "log" else "parallel"
+    M, S = A.shape
+    N = C.shape[1]
+    if w.shape[0] != S:
+        raise ValueError("w must have one weight per column of A")
+    be = np.ascontiguousarray(np.asarray(b_ext, dtype=np.float64).ravel()) if with_grad else None
+    if with_grad and be.shape[0] != N:
+        raise ValueError("b_ext must have one entry per column of C")
+    X1 = np.zeros((M, S), order="F")
+    X2 = np.zeros((N, S), order="F")
+    b = np.zeros(N)
+    gA = np.zeros((M, S), order="F") if with_grad else None
+    gw = np.zeros(S) if with_grad else None
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    L = _lib.load()
+    fn = L.rwig_barycenter_log if method == "log" else L.rwig_barycenter_parallel
+    rc = fn(_dp(X1), _dp(X2), _dp(b), _dp(gA), _dp(gw), ctypes.byref(loss), ctypes.byref(it), ctypes.byref(err),
+            _dp(A), _dp(np.ascontiguousarray(w)), _dp(C), _dp(be), M, N, S, reg, int(with_grad),
+            int(ctrl["max_iter"]), float(ctrl["zero_tol"]))
+    _lib.check(rc)
+    names = ("F", "G") if method == "log" else ("U", "V")
+    out = {"b": b}
+    if with_grad:
+        out.update(grad_A=gA, grad_w=gw, loss=loss.value)
+    out.update({names[0]: X1, names[1]: X2, "iter": it.value, "err": err.value, "return_status": rc,
+                "method": method})
+    return out
+
+
 # ---------------------------------------------------------------------------
 # device-resident entry points (torch CUDA tensors as plain device buffers)
 # ---------------------------------------------------------------------------

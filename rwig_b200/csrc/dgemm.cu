@@ -2,6 +2,7 @@
 // self-check entry point.
 #include <algorithm>
 
+#define RWIG_DGEMM_DEFINE_KERNEL
 #include "dgemm.cuh"
 #include "engine.h"
 

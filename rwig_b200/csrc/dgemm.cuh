@@ -104,6 +104,7 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, Smem& sm, int st, 
   }
 }
 
+#ifdef RWIG_DGEMM_DEFINE_KERNEL  // defined in dgemm.cu only
 __global__ void __launch_bounds__(NTH) dgemm_splitk_kernel(GemmArgs g) {
   __shared__ __align__(16) Smem sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -153,6 +154,8 @@ __global__ void __launch_bounds__(NTH) dgemm_splitk_kernel(GemmArgs g) {
     }
   }
 }
+
+#endif  // RWIG_DGEMM_DEFINE_KERNEL
 
 // Fixed-order sum of the split partials of entry (r, c).
 __device__ __forceinline__ double reduce_splits(const double* part, int splits, int Mo, int S, int r, int c) {

@@ -1,0 +1,111 @@
+"""Parity of the CUDA barycenters (rwig_barycenter_parallel / _log) with the CPU
+oracle (Barycenter::compute_parallel / compute_log restated), rwig's
+known-answer vectors, and central finite differences of the engine's own
+gradients."""
+import numpy as np
+import pytest
+
+import oracle
+import rwig_b200 as rw
+from rwig_b200 import synth
+from tests.util import GOLDEN_TOL, PARITY_TOL, dual_scale, mean_rel_diff, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare(method, A, C, w, be, reg, with_grad=True, max_iter=1000, zero_tol=1e-6):
+    f = oracle.barycenter_log if method == "log" else oracle.barycenter_parallel
+    ref = f(A, C, w, be, reg, with_grad=with_grad, max_iter=max_iter, zero_tol=zero_tol)
+    got = rw.barycenter(A, C, w, be if with_grad else None,
+                        {"reg": reg, "method": method, "with_grad": with_grad, "max_iter": max_iter,
+                         "zero_tol": zero_tol})
+    assert got["iter"] == ref["iter"] and got["return_status"] == ref["return_status"]
+    assert rel_err(got["b"], ref["b"]) <= PARITY_TOL, rel_err(got["b"], ref["b"])
+    if method == "log":
+        sc = dual_scale(ref["F"], ref["G"])
+        for k in ("F", "G"):
+            assert rel_err(got[k], ref[k], sc) <= PARITY_TOL, (k, rel_err(got[k], ref[k], sc))
+    else:
+        for k in ("U", "V"):
+            assert rel_err(got[k], ref[k]) <= PARITY_TOL, (k, rel_err(got[k], ref[k]))
+    if with_grad:
+        for k in ("grad_A", "grad_w"):
+            assert rel_err(got[k], ref[k]) <= PARITY_TOL, (k, rel_err(got[k], ref[k]))
+        assert abs(got["loss"] - ref["loss"]) <= PARITY_TOL * abs(ref["loss"])
+    assert abs(got["err"] - ref["err"]) <= 1e-8 * abs(ref["err"]) + 1e-13
+    return got, ref
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+def test_golden_vectors(golden, method):
+    g = golden["barycenter"]
+    A, C = np.array(g["inputs"]["A"]), np.array(g["inputs"]["C"])
+    w, be, reg = np.array(g["inputs"]["w"]), np.array(g["inputs"]["b"]), g["inputs"]["reg"]
+    r = rw.barycenter(A, C, w, be, {"reg": reg, "method": method, "with_grad": True})
+    keys = ("loss", "grad_A", "grad_w", "b") + (("U", "V") if method == "parallel" else ("F", "G"))
+    for k in keys:
+        assert mean_rel_diff(g[method][k], r[k]) <= GOLDEN_TOL, k
+    _compare(method, A, C, w, be, reg)
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+@pytest.mark.parametrize("n,S,dim,reg,L,tol", [
+    (64, 4, 3, 0.1, 1000, 1e-9), (200, 7, 5, 0.1, 30, 0.0), (256, 32, 50, 0.05, 50, 0.0),
+    (513, 3, 2, 0.2, 1000, 1e-10), (2, 2, 2, 0.1, 5, 0.0),
+])
+def test_parity_shapes(method, n, S, dim, reg, L, tol):
+    A, C, w, be = synth.barycenter_config(n=n, S=S, dim=dim, salt=n + S)
+    _compare(method, A, C, w, be, reg, max_iter=L, zero_tol=tol)
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+def test_rectangular_cost(method):
+    """M != N: histograms on M points, barycenter on N."""
+    g = synth.rng(31)
+    x, y = g.random((150, 3)), g.random((90, 3))
+    C = synth.sq_euclid_cost(x, y)
+    A = synth.dirichlet(g, 0.5, 150, 5)
+    w = synth.dirichlet(g, 1.0, 5)
+    be = synth.dirichlet(g, 1.0, 90)
+    _compare(method, A, C, w, be, 0.1, max_iter=40, zero_tol=0.0)
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+def test_without_gradient(method):
+    A, C, w, be = synth.barycenter_config(n=300, S=6, dim=4, salt=9)
+    _compare(method, A, C, w, be, 0.1, with_grad=False, max_iter=1000, zero_tol=1e-8)
+
+
+def _fd(fun, x, idx, h=1e-6):
+    out = []
+    for k in idx:
+        xp, xm = x.copy(), x.copy()
+        xp.flat[k] += h
+        xm.flat[k] -= h
+        out.append((fun(xp) - fun(xm)) / (2 * h))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+def test_gradient_finite_differences(method):
+    """Central differences (h = 1e-6) of the engine's objective: ||b - b_ext||^2
+    with the un-normalised b (parallel), or with the normaliser held at its
+    value (log), which is what the reference's backward differentiates."""
+    A, C, w, be = synth.barycenter_config(n=256, S=8, dim=10, salt=3)
+    L, reg = 30, 0.05
+    ctrl = {"reg": reg, "method": method, "with_grad": True, "max_iter": L, "zero_tol": 0.0}
+    r = rw.barycenter(A, C, w, be, ctrl)
+    Z0 = rw.last_report()["bary_norm"]
+
+    def obj(A_, w_):
+        q = rw.barycenter(A_, C, w_, be, ctrl)
+        z = rw.last_report()["bary_norm"]
+        braw = q["b"] * z
+        return float((((braw / Z0) if method == "log" else braw) - be) @ (((braw / Z0) if method == "log" else braw) - be))
+
+    gw = _fd(lambda x: obj(A, x), w, range(w.size))
+    assert np.abs(gw - r["grad_w"]).max() <= 1e-6 * max(1.0, np.abs(gw).max())
+    g = np.random.default_rng(0)
+    idx = [k for k in g.choice(A.size, 40, replace=False) if A.flat[k] > 1e-3]
+    gA = _fd(lambda X: obj(X, w), A, idx)
+    assert np.abs(gA - r["grad_A"].flat[idx]).max() <= 1e-6 * max(1.0, np.abs(gA).max())
