@@ -4,7 +4,8 @@ Default workload (the headline): log-stabilised Sinkhorn, one 4096 x 4096 FP64
 problem per solve, a, b ~ Dirichlet(0.5), support points uniform in [0,1]^2,
 squared-Euclidean cost normalised by its max, eps = 0.01, max_iter = 2000,
 zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
---workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)).
+--workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)),
+--workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
@@ -29,6 +30,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -46,6 +49,7 @@ def parse():
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--s", type=int, default=32, help="histograms (barycenter --single)")
     ap.add_argument("--l2-hot", type=float, default=None, help="engine option log_sinkhorn.l2_hot")
     return ap.parse_args()
 
@@ -312,9 +316,178 @@ class SinkhornWorkload:
         return sum(secs), cores, sample
 
 
+def measured_dgemm_tflops(dev):
+    """cuBLAS FP64 GEMM throughput on this GPU (torch.matmul float64, 8192^3,
+    best of 5): the denominator for the FP64 tensor-core kernels, since the
+    peak file records bf16 and HBM only."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+class BarycenterWorkload:
+    """One log-barycenter solve with its gradient per step (fixed L iterations)."""
+
+    higher_is_better = True
+
+    def __init__(self, n=2048, S=32, dim=50, reg=0.05, L=50):
+        self.n, self.S, self.dim, self.reg, self.L = n, S, dim, reg, L
+        self.unit = "solves/s"
+        self.metric = f"log-barycenter + gradient solves/s (N={n}, S={S}, L={L}, FP64)"
+        self.desc = (f"log-domain Wasserstein barycenter of S={S} Dirichlet(0.3) histograms on N={n} points "
+                     f"~ N(0, I_{dim}), squared-Euclidean cost / max, w ~ Dirichlet(1), b_ext ~ Dirichlet(0.3), "
+                     f"eps={reg:g}, L={L} unrolled iterations (max_iter={L}, zero_tol=0), outputs b, F, G, "
+                     f"grad_A, grad_w, loss")
+
+    def inputs(self):
+        from rwig_b200 import synth
+        return synth.barycenter_config(n=self.n, S=self.S, dim=self.dim)
+
+    def gemm_flops(self):
+        # forward: K 1, then K^T U and K V per iteration, plus the residual
+        # Gram matrix; backward: K T2 at the seed step, K^T T and K T2 at the others
+        n, S, L = self.n, self.S, self.L
+        products = 1 + 2 * L + (2 * L - 1)
+        return products * 2.0 * n * n * S + 2.0 * n * S * S
+
+    def cpu_seconds(self, threads):
+        import oracle
+        A, C, w, be = self.inputs()
+        t = {}
+        for it in (1, 2):
+            t0 = time.perf_counter()
+            oracle.barycenter_log(A, C, w, be, self.reg, with_grad=True, n_threads=threads, max_iter=it,
+                                  zero_tol=0.0)
+            t[it] = time.perf_counter() - t0
+        per = max(t[2] - t[1], 1e-9)
+        fixed = max(t[1] - per, 0.0)
+        secs = fixed + self.L * per
+        sample = (f"1- and 2-iteration runs (forward + backward, {threads} threads) of the same problem, "
+                  f"extrapolated to L={self.L}: {per:.2f} s per iteration, {fixed:.2f} s fixed")
+        return secs, threads, sample
+
+    def run(self, args, dev, world, rank, clocks_cls):
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        n, S = self.n, self.S
+        A, C, w, be = self.inputs()
+        tA = torch.from_numpy(np.ascontiguousarray(A.T)).to(dev)
+        tC = torch.from_numpy(np.ascontiguousarray(C.T)).to(dev)
+        tw, tbe = torch.from_numpy(w).to(dev), torch.from_numpy(be).to(dev)
+        F = torch.empty((S, n), dtype=torch.float64, device=dev)
+        G = torch.empty((S, n), dtype=torch.float64, device=dev)
+        b = torch.empty(n, dtype=torch.float64, device=dev)
+        gA = torch.empty((S, n), dtype=torch.float64, device=dev)
+        gw = torch.empty(S, dtype=torch.float64, device=dev)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+        stream = torch.cuda.current_stream()
+        L = _lib.load()
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+        def solve():
+            loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+            rc = L.rwig_barycenter_log_dev(vp(F), vp(G), vp(b), vp(gA), vp(gw), ctypes.byref(loss), ctypes.byref(it),
+                                           ctypes.byref(err), vp(tA), vp(tw), vp(tC), vp(tbe), n, n, S, self.reg, 1,
+                                           self.L, 0.0, ctypes.c_void_p(stream.cuda_stream))
+            _lib.check(rc)
+            return rw.last_report()
+
+        for _ in range(args.warmup):
+            flush.zero_()
+            solve()
+        torch.cuda.synchronize()
+        times, reps = [], []
+        with clocks_cls(dev.index) as clocks:
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                reps.append(solve())
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            torch.cuda.synchronize()
+        tot_ms = max_over_ranks(sum(times), world, dev)
+
+        # end to end through the host-pointer entry
+        hA = np.asfortranarray(A)
+        hC = np.asfortranarray(C)
+        hF, hG = np.zeros((n, S), order="F"), np.zeros((n, S), order="F")
+        hb, hgA, hgw = np.zeros(n), np.zeros((n, S), order="F"), np.zeros(S)
+        dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+
+        def host_solve():
+            loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+            _lib.check(L.rwig_barycenter_log(dp(hF), dp(hG), dp(hb), dp(hgA), dp(hgw), ctypes.byref(loss),
+                                             ctypes.byref(it), ctypes.byref(err), dp(hA), dp(w), dp(hC), dp(be), n, n,
+                                             S, self.reg, 1, self.L, 0.0))
+
+        for _ in range(2):
+            host_solve()
+        e2e_s = 0.0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            host_solve()
+            e2e_s += time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, world, dev)
+        assert np.array_equal(hgw, gw.cpu().numpy()), "host and device entry points disagree"
+        if rank != 0:
+            return None
+        tf_peak = measured_dgemm_tflops(dev)
+        kms = sum(r["kernel_ms"] for r in reps) / len(reps)
+        achieved = self.gemm_flops() / (kms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
+                "frac": achieved / tf_peak, "traffic": None,
+                "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
+                "kernel": "dgemm_kernel with fused epilogues (whole solve, device time)",
+                "flops_per_solve": self.gemm_flops(), "ms_per_solve": kms}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1)
+            cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
+        MS, NN = n * S * 8, n * n * 8
+        return {"value": args.steps * world / (tot_ms / 1e3), "ms_per_step": tot_ms / args.steps,
+                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
+                           "l2": "flushed between steps (256 MB write)"},
+                "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
+                        "h2d_bytes_per_step": MS + NN + (S + n) * 8, "d2h_bytes_per_step": 3 * MS + (n + S) * 8},
+                "gpu_launches": sum(r["kernel_launches"] for r in reps), "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clocks.summary()}
+
+    def reference(self, args):
+        threads = os.cpu_count() or 1
+        secs, sample = [], ""
+        for _ in range(args.steps):
+            s_, cores, sample = self.cpu_seconds(threads)
+            secs.append(s_)
+        return sum(secs), threads, sample
+
+
 WORKLOADS = {
     "log4096": SinkhornWorkload("log", 4096, 4096, 0.01, 0.5, 2000, 1e-9),
     "vanilla256": SinkhornWorkload("vanilla", 256, 256, 0.1, 1.0, 1000, 1e-9),
+    "barycenter2048": BarycenterWorkload(),
 }
 
 
@@ -371,11 +544,23 @@ def run_engine(args):
 
 def run_single(args):
     """One warm-up plus one solve of an m x n log problem with a fixed iteration
-    count (tol 0): the small case the kernel profiles are captured on."""
+    count (tol 0): the small case the kernel profiles are captured on.  With
+    --workload barycenter2048: two log-barycenter solves with gradient on n
+    points, --s histograms, --iters iterations (the second one is captured
+    into a CUDA graph)."""
     import torch
 
     import rwig_b200 as rw
     from rwig_b200 import synth
+    if args.workload.startswith("barycenter"):
+        A, C, w, be = synth.barycenter_config(n=args.n, S=args.s, dim=50)
+        for _ in range(2):
+            r = rw.barycenter(A, C, w, be, {"reg": 0.05, "with_grad": True, "method": "log",
+                                            "max_iter": args.iters, "zero_tol": 0.0})
+        rep = rw.last_report()
+        print(json.dumps({"n": args.n, "S": args.s, "iter": r["iter"], "device_ms": rep["device_ms"],
+                          "launches": rep["kernel_launches"]}))
+        return 0
     a, b, C = synth.log_config(args.m, args.n)
     if args.l2_hot is not None:
         rw.load().rwig_set_option(b"log_sinkhorn.l2_hot", float(args.l2_hot))

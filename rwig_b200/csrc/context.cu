@@ -133,6 +133,8 @@ extern "C" void rwig_shutdown(void) {
     if (!c) continue;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    for (auto& ge : c->graphs)
+      if (ge.exec) cudaGraphExecDestroy(ge.exec);
     for (void* p : c->slots)
       if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);

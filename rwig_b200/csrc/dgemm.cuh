@@ -1,42 +1,83 @@
 // dgemm.cuh -- FP64 tensor-core (DMMA, mma.sync m16n8k4 .f64) GEMM for the
 // skinny products of the barycenter and WDL paths:
-//     Y (Mo x S) = op(K) * X (Kd x S),   op(K) = K or K^T,
-// K column-major (ldk), X and Y column-major.  Split-K: each CTA computes a
-// 64 x 32 tile of Y over one slice of the contraction and writes it to a
-// partial buffer [split][S][Mo]; callers reduce the splits in a fixed order
-// (deterministic) inside their own epilogue kernels.
+//     Y (Mo x W) = op(K) * X (Kd x W),   op(K) = K or K^T,
+// K column-major (ldk even, 16-byte aligned), X column-major.
 //
-// Tiles: 4 warps per CTA, each 16 rows x 32 columns (four m16n8k4 n-tiles);
-// BK = 16 contraction steps per stage, two stages through cp.async (16-byte
-// copies, zero-filled at the edges).
+// One CTA (8 warps) computes a BM x BN tile of Y over one slice of the
+// contraction; each warp owns 16 rows x BN columns (NT m16n8k4 n-tiles) and
+// one half of every BK step (warps 0-3 the first 16 k, warps 4-7 the second),
+// the two halves being added in a fixed order at the end.  Operands stream
+// through a STAGES-deep cp.async ring in their natural global layout (K^T
+// tiles m-major, K tiles k-major, X tiles column-major), padded so the
+// fragment reads are free of bank conflicts.
+//
+// Split-K runs inside a thread-block cluster of `splits` CTAs stacked along
+// z: every CTA parks its partial tile in shared memory, and after a cluster
+// barrier CTA z sums rows [z*BM/splits, (z+1)*BM/splits) of all partials
+// through distributed shared memory, in the fixed order 0..splits-1 (the
+// result is bitwise repeatable and independent of scheduling).  The summed
+// rows then go to an epilogue functor, so the elementwise work that follows
+// each product never makes a separate pass over HBM.
+//
+// Epilogue interface (called by all NTH threads of the CTA; may use
+// __syncthreads):
+//     epi(r0, nr, c0, nc, t, ldt, ws)
+// rows r0 .. r0+nr-1 of Y (nr <= 0: nothing to do), columns c0 .. c0+nc-1
+// (nc = BN), value (r0 + r, c0 + c) at t[c * ldt + r]; ws: (BN + 1) * ldt
+// doubles of shared scratch.  Columns at or beyond W hold zeros.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
+
+#include "engine.h"
 
 namespace rwig {
 namespace dg {
 
-constexpr int BM = 64, BN = 32, BK = 16, NTH = 128;
+constexpr int BM = 64, BK = 32, NTH = 256, STAGES = 4;
 constexpr int PAD = 4;  // doubles of padding per shared row
+constexpr int kMaxSplits = 8;
 
 struct GemmArgs {
   const double* K;
   long long ldk;
-  int trans;         // 0: Y = K X (Mo = rows of K), 1: Y = K^T X (Mo = cols of K)
-  int Mo, Kd, S;     // output rows, contraction length, output columns
-  const double* X;   // Kd x S, column-major
+  int Mo, Kd, W;     // output rows, contraction length, output columns
+  const double* X;   // Kd x W, column-major
   long long ldx;
-  double* part;      // [splits][S][Mo]
-  int splits;        // contraction slices (gridDim.z)
+  int splits;        // cluster size along z: 1, 2, 4 or 8
 };
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+template <int TRANS>
+__host__ __device__ constexpr int a_stage_doubles() {
+  return TRANS ? BM * (BK + PAD) : BK * (BM + PAD);
+}
+template <int NT>
+__host__ __device__ constexpr int b_stage_doubles() {
+  return NT * 8 * (BK + PAD);
+}
+template <int TRANS, int NT>
+__host__ __device__ constexpr int smem_doubles() {
+  // pipeline ring, or (after the main loop) partial tile + summed rows + epilogue scratch
+  return (STAGES * (a_stage_doubles<TRANS>() + b_stage_doubles<NT>()) > NT * 8 * (3 * BM + 1) + BM)
+             ? STAGES * (a_stage_doubles<TRANS>() + b_stage_doubles<NT>())
+             : NT * 8 * (3 * BM + 1) + BM;
+}
+
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem, int src_bytes) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
 }
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ void mma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
   asm volatile(
@@ -45,21 +86,37 @@ __device__ __forceinline__ void mma_16x8x4(double (&d)[4], double a0, double a1,
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// Shared tiles: A as [BK][BM + PAD] (k-major), B as [BK][BN + PAD].
-struct Smem {
-  double A[2][BK][BM + PAD];
-  double B[2][BK][BN + PAD];
-};
+__device__ __forceinline__ unsigned cluster_nctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+// Load a double from the same shared-memory offset in cluster CTA `rank`.
+__device__ __forceinline__ double ld_cluster(const double* p, unsigned rank) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  unsigned ra;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(ra) : "memory");
+  return v;
+}
 
-// Loads the A and B tiles of contraction step k0 into stage `st`.
-__device__ __forceinline__ void load_stage(const GemmArgs& g, Smem& sm, int st, int m0, int n0, int k0, int kend) {
+// Issues the copies of contraction step [k0, k0 + BK) into one ring stage.
+// XV = 2: X columns copied as 16-byte pairs (ldx even, X 16-byte aligned);
+// XV = 1: 8-byte copies.  Out-of-range elements are zero-filled.
+template <int TRANS, int NT, int XV>
+__device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double* Bs, int m0, int n0, int k0,
+                                           int kend) {
   const int tid = threadIdx.x;
-  // A tile: BK x BM doubles = 512 16-byte chunks, 4 per thread
-  if (!g.trans) {
-    // A[m][k] = K[m + k*ldk]: chunk = (k, pair of m)
+  if (!TRANS) {
+    // A[k][m] = K[m + k*ldk]: 32 k x 32 m-pairs
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int idx = tid + c * NTH;  // 0..511
+    for (int c = 0; c < (BK * BM / 2) / NTH; ++c) {
+      const int idx = tid + c * NTH;
       const int kk = idx >> 5, mp = (idx & 31) * 2;
       const int gk = k0 + kk, gm = m0 + mp;
       int bytes = 0;
@@ -68,101 +125,234 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, Smem& sm, int st, 
         bytes = (gm + 1 < g.Mo) ? 16 : 8;
         src = g.K + gm + (long long)gk * g.ldk;
       }
-      cp_async16(&sm.A[st][kk][mp], src, bytes);
+      cp_async16(As + kk * (BM + PAD) + mp, src, bytes);
     }
   } else {
-    // A[m][k] = K[k + m*ldk]: chunk = (m, pair of k), stored transposed
+    // A[m][k] = K[k + m*ldk]: 64 m x 16 k-pairs
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < (BM * BK / 2) / NTH; ++c) {
       const int idx = tid + c * NTH;
-      const int mm = idx >> 3, kp = (idx & 7) * 2;
+      const int mm = idx >> 4, kp = (idx & 15) * 2;
       const int gk = k0 + kp, gm = m0 + mm;
-      double v0 = 0.0, v1 = 0.0;
-      if (gm < g.Mo) {
-        const double* src = g.K + gk + (long long)gm * g.ldk;
-        if (gk < kend) v0 = __ldg(src);
-        if (gk + 1 < kend) v1 = __ldg(src + 1);
+      int bytes = 0;
+      const double* src = g.K;
+      if (gk < kend && gm < g.Mo) {
+        bytes = (gk + 1 < kend) ? 16 : 8;
+        src = g.K + gk + (long long)gm * g.ldk;
       }
-      sm.A[st][kp][mm] = v0;
-      sm.A[st][kp + 1][mm] = v1;
+      cp_async16(As + mm * (BK + PAD) + kp, src, bytes);
     }
   }
-  // B tile: BK x BN doubles = 256 chunks, 2 per thread; B[k][n] = X[k + n*ldx]
+  // B[n][k] = X[k + n*ldx]
+  if (XV == 2) {
 #pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    const int idx = tid + c * NTH;  // 0..255
-    const int nn = idx >> 3, kp = (idx & 7) * 2;
-    const int gk = k0 + kp, gn = n0 + nn;
-    double v0 = 0.0, v1 = 0.0;
-    if (gn < g.S) {
-      const double* src = g.X + gk + (long long)gn * g.ldx;
-      if (gk < kend) v0 = __ldg(src);
-      if (gk + 1 < kend) v1 = __ldg(src + 1);
+    for (int c = 0; c < NT * 8 * 16 / NTH; ++c) {  // NT*8 columns x 16 k-pairs
+      const int idx = tid + c * NTH;
+      const int nn = idx >> 4, kp = (idx & 15) * 2;
+      const int gk = k0 + kp, gn = n0 + nn;
+      int bytes = 0;
+      const double* src = g.X;
+      if (gk < kend && gn < g.W) {
+        bytes = (gk + 1 < kend) ? 16 : 8;
+        src = g.X + gk + (long long)gn * g.ldx;
+      }
+      cp_async16(Bs + nn * (BK + PAD) + kp, src, bytes);
     }
-    sm.B[st][kp][nn] = v0;
-    sm.B[st][kp + 1][nn] = v1;
+  } else {
+#pragma unroll
+    for (int c = 0; c < NT * 8 * 32 / NTH; ++c) {  // NT*8 columns x 32 k
+      const int idx = tid + c * NTH;
+      const int nn = idx >> 5, kk = idx & 31;
+      const int gk = k0 + kk, gn = n0 + nn;
+      int bytes = 0;
+      const double* src = g.X;
+      if (gk < kend && gn < g.W) {
+        bytes = 8;
+        src = g.X + gk + (long long)gn * g.ldx;
+      }
+      cp_async8(Bs + nn * (BK + PAD) + kk, src, bytes);
+    }
   }
 }
 
-#ifdef RWIG_DGEMM_DEFINE_KERNEL  // defined in dgemm.cu only
-__global__ void __launch_bounds__(NTH) dgemm_splitk_kernel(GemmArgs g) {
-  __shared__ __align__(16) Smem sm;
+template <int TRANS, int NT, int XV, class Epi>
+__global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
+  extern __shared__ __align__(16) double smem[];
+  constexpr int BN = NT * 8;
+  constexpr int ASZ = a_stage_doubles<TRANS>(), BSZ = b_stage_doubles<NT>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int slice = (g.Kd + g.splits - 1) / g.splits;
-  const int kbeg = blockIdx.z * slice;
+  const int splits = g.splits;
+  // the launch must form one cluster of `splits` CTAs along z
+  if (splits > 1 && (int)cluster_nctarank() != splits) return;
+  const int z = blockIdx.z;
+  int slice = (g.Kd + splits - 1) / splits;
+  slice = ((slice + BK - 1) / BK) * BK;
+  const int kbeg = z * slice;
   const int kend = min(g.Kd, kbeg + slice);
-  double acc[4][4];
+  const int nsteps = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+
+  double acc[NT][4];
 #pragma unroll
-  for (int t = 0; t < 4; ++t)
+  for (int t = 0; t < NT; ++t)
 #pragma unroll
     for (int e = 0; e < 4; ++e) acc[t][e] = 0.0;
 
-  const int nsteps = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
-  if (nsteps > 0) load_stage(g, sm, 0, m0, n0, kbeg, kend);
-  cp_async_commit();
-  const int wm = warp * 16;
-  for (int s = 0; s < nsteps; ++s) {
-    const int st = s & 1;
-    if (s + 1 < nsteps) load_stage(g, sm, st ^ 1, m0, n0, kbeg + (s + 1) * BK, kend);
+  double* As = smem;
+  double* Bs = smem + STAGES * ASZ;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nsteps) load_stage<TRANS, NT, XV>(g, As + s * ASZ, Bs + s * BSZ, m0, n0, kbeg + s * BK, kend);
     cp_async_commit();
-    cp_async_wait_one();
-    __syncthreads();
+  }
+  const int wm = (warp & 3) * 16, kh = (warp >> 2) * (BK / 2);
+  for (int s = 0; s < nsteps; ++s) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();  // stage s visible; stage s-1 no longer read
+    const int nx = s + STAGES - 1;
+    if (nx < nsteps) {
+      const int q = nx % STAGES;
+      load_stage<TRANS, NT, XV>(g, As + q * ASZ, Bs + q * BSZ, m0, n0, kbeg + nx * BK, kend);
+    }
+    cp_async_commit();
+    const double* A = As + (s % STAGES) * ASZ;
+    const double* B = Bs + (s % STAGES) * BSZ;
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      const double a0 = sm.A[st][kk + tig][wm + gid];
-      const double a1 = sm.A[st][kk + tig][wm + gid + 8];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const double b0 = sm.B[st][kk + tig][t * 8 + gid];
-        mma_16x8x4(acc[t], a0, a1, b0);
+    for (int k4 = 0; k4 < BK / 2; k4 += 4) {
+      const int kk = kh + k4;
+      double a0, a1;
+      if (!TRANS) {
+        a0 = A[(kk + tig) * (BM + PAD) + wm + gid];
+        a1 = A[(kk + tig) * (BM + PAD) + wm + gid + 8];
+      } else {
+        a0 = A[(wm + gid) * (BK + PAD) + kk + tig];
+        a1 = A[(wm + gid + 8) * (BK + PAD) + kk + tig];
       }
+#pragma unroll
+      for (int t = 0; t < NT; ++t) mma_16x8x4(acc[t], a0, a1, B[(t * 8 + gid) * (BK + PAD) + kk + tig]);
     }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // partial tile -> shared memory, [c][r] with row stride BM + 1; the second
+  // k half is added to the first in a fixed order
+  double* red = smem;
+  double* fin = red + BN * (BM + 1);
+  double* ws = fin + BN * BM;
+  for (int h = 0; h < 2; ++h) {
+    if ((warp >> 2) == h) {
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int r = wm + gid + ((e >> 1) << 3);
+          const int c = t * 8 + tig * 2 + (e & 1);
+          if (h == 0) red[c * (BM + 1) + r] = acc[t][e];
+          else red[c * (BM + 1) + r] += acc[t][e];
+        }
+    }
+    if (h == 0) __syncthreads();
+  }
+  if (splits > 1) {
+    cluster_arrive();
+    cluster_wait();
+  } else {
     __syncthreads();
   }
-  cp_async_wait_all();
-  // C fragment: c0,c1 at row gid, cols 2*tig + {0,1}; c2,c3 at row gid + 8
-  double* out = g.part + (size_t)blockIdx.z * g.S * g.Mo;
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int r = m0 + wm + gid + ((e >> 1) << 3);
-      const int c = n0 + t * 8 + tig * 2 + (e & 1);
-      if (r < g.Mo && c < g.S) out[(size_t)c * g.Mo + r] = acc[t][e];
+  // sum this CTA's rows over the cluster's partials, fixed order
+  const int rows = BM / splits;
+  const int rl0 = z * rows;
+  for (int e = threadIdx.x; e < rows * BN; e += NTH) {
+    const int r = e % rows, c = e / rows;
+    const double* p = red + c * (BM + 1) + rl0 + r;
+    double v = 0.0;
+    if (splits > 1) {
+      for (int q = 0; q < splits; ++q) v += ld_cluster(p, (unsigned)q);
+    } else {
+      v += *p;
     }
+    fin[c * rows + r] = v;
   }
+  if (splits > 1) cluster_arrive();  // this CTA is done reading its peers
+  __syncthreads();
+  epi(m0 + rl0, min(rows, g.Mo - (m0 + rl0)), n0, BN, fin, rows, ws);
+  if (splits > 1) cluster_wait();  // peers are done reading this CTA
 }
 
-#endif  // RWIG_DGEMM_DEFINE_KERNEL
+// Epilogue that stores the tile: Y[r + c*ldy] for columns < W.
+struct EpiStore {
+  double* Y;
+  long long ldy;
+  int W;
+  __device__ void operator()(int r0, int nr, int c0, int nc, const double* t, int ldt, double*) const {
+    if (nr <= 0) return;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr;
+      if (c0 + c < W) Y[(r0 + r) + (long long)(c0 + c) * ldy] = t[c * ldt + r];
+    }
+  }
+};
 
-// Fixed-order sum of the split partials of entry (r, c).
-__device__ __forceinline__ double reduce_splits(const double* part, int splits, int Mo, int S, int r, int c) {
-  double s = 0.0;
-  const size_t stride = (size_t)S * Mo, off = (size_t)c * Mo + r;
-  for (int z = 0; z < splits; ++z) s += part[z * stride + off];
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+// Largest power of two <= kMaxSplits that keeps the grid within about the
+// resident CTAs of one wave (two per SM for NT = 4, one for NT = 8) and
+// leaves every slice at least four BK steps.
+inline int pick_splits(const Context* ctx, int Mo, int Kd, int W, int NT) {
+  const long long tiles = (long long)((Mo + BM - 1) / BM) * ((W + NT * 8 - 1) / (NT * 8));
+  const long long target = (NT <= 4 ? 2LL : 1LL) * ctx->sm_count;
+  int s = 1;
+  while (s < kMaxSplits && tiles * s * 2 <= target && Kd >= s * 2 * 4 * BK) s *= 2;
   return s;
+}
+
+inline int clamp_splits(int s) { return s >= 8 ? 8 : s >= 4 ? 4 : s >= 2 ? 2 : 1; }
+
+template <int TRANS, int NT, int XV, class Epi>
+int launch_kernel(const GemmArgs& g, const Epi& epi, cudaStream_t st) {
+  constexpr size_t bytes = sizeof(double) * smem_doubles<TRANS, NT>();
+  auto kern = dgemm_kernel<TRANS, NT, XV, Epi>;
+  static bool attr_set = false;  // once per instantiation (callers hold the context lock)
+  if (!attr_set) {
+    RWIG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    attr_set = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((g.Mo + BM - 1) / BM, (g.W + NT * 8 - 1) / (NT * 8), g.splits);
+  cfg.blockDim = dim3(NTH);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 1;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = (unsigned)g.splits;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  RWIG_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, g, epi));
+  return 0;
+}
+
+// Y = op(K) X with epilogue `epi`.  g.splits <= 0 picks the split count,
+// otherwise it is rounded down to 1, 2, 4 or 8.  W <= 32 runs 32-column
+// tiles, wider outputs 64-column tiles (epilogues that need a whole row of Y
+// in one tile require W <= 64).  Returns 0 or an engine error code.
+template <int TRANS, class Epi>
+int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st) {
+  if (!g.K || !g.X || g.Mo < 1 || g.Kd < 1 || g.W < 1)
+    return set_error(RWIG_E_INVALID, "GEMM: null operand or empty shape");
+  if ((g.ldk % 2) != 0 || (reinterpret_cast<uintptr_t>(g.K) % 16) != 0)
+    return set_error(RWIG_E_INVALID, "GEMM operand K needs an even leading dimension and 16-byte alignment");
+  if (g.ldk < (TRANS ? g.Kd : g.Mo) || g.ldx < g.Kd)
+    return set_error(RWIG_E_INVALID, "GEMM: leading dimension smaller than the operand");
+  const int NT = g.W <= 32 ? 4 : 8;
+  g.splits = g.splits <= 0 ? pick_splits(ctx, g.Mo, g.Kd, g.W, NT) : clamp_splits(g.splits);
+  const bool xv2 = (g.ldx % 2) == 0 && (reinterpret_cast<uintptr_t>(g.X) % 16) == 0;
+  if (NT == 4) return xv2 ? launch_kernel<TRANS, 4, 2>(g, epi, st) : launch_kernel<TRANS, 4, 1>(g, epi, st);
+  return xv2 ? launch_kernel<TRANS, 8, 2>(g, epi, st) : launch_kernel<TRANS, 8, 1>(g, epi, st);
 }
 
 }  // namespace dg

@@ -13,6 +13,15 @@
 
 namespace rwig {
 
+// A captured launch sequence, replayed when a call repeats with the same
+// arguments and buffers (key).
+struct GraphEntry {
+  std::vector<unsigned long long> key;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+};
+enum { kGraphBaryParallel = 0, kGraphBaryLog = 1, kGraphSites = 4 };
+
 struct Context {
   int device = -1;
   int sm_count = 0;
@@ -24,6 +33,8 @@ struct Context {
   std::vector<size_t> slot_bytes;
   void* pinned = nullptr;  // small pinned staging buffer for scalars
   size_t pinned_bytes = 0;
+  GraphEntry graphs[kGraphSites];
+  std::vector<unsigned long long> seen[kGraphSites];  // key of the previous call per site
 };
 
 // Returns the context of the current (or first) device, initialising it on

@@ -1,4 +1,4 @@
-"""The engine's FP64 tensor-core GEMM (mma.sync m16n8k4 .f64, split-K) against
+"""The engine's FP64 tensor-core GEMM (mma.sync m16n8k4 .f64, cluster split-K) against
 numpy on the host, for both orientations and ragged shapes."""
 import ctypes
 
@@ -27,6 +27,7 @@ def _run(K, X, trans, splits=0, ldy_extra=0):
     rc = _lib.check(_lib.load().rwig_selftest_dgemm(vp(tK), ldk, int(trans), Mo, Kd, S, vp(tX), Kd, vp(tY), ldy,
                                                     splits, None))
     assert rc >= 1
+    _run.splits = rc
     return tY.cpu().numpy().T[:Mo, :]
 
 
@@ -42,11 +43,35 @@ def test_against_numpy(trans, Mk, Nk, S):
     assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * np.sqrt(X.shape[0])
 
 
-@pytest.mark.parametrize("splits", [1, 3, 17])
-def test_split_counts_agree(splits):
+@pytest.mark.parametrize("splits,used", [(1, 1), (2, 2), (3, 2), (4, 4), (8, 8), (17, 8)])
+def test_split_counts_agree(splits, used):
+    """Cluster split-K: requested counts round down to 1, 2, 4 or 8."""
     g = np.random.default_rng(5)
     K = g.random((512, 384))
     X = g.random((384, 32))
     ref = K @ X
     got = _run(K, X, 0, splits=splits)
+    assert _run.splits == used
     assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("trans", [0, 1])
+def test_bitwise_repeatable(trans):
+    """Fixed-order split reduction: identical bits on every run."""
+    g = np.random.default_rng(11)
+    K = g.standard_normal((2048, 2048))
+    X = g.standard_normal((2048, 32))
+    first = _run(K, X, trans)
+    for _ in range(3):
+        assert np.array_equal(_run(K, X, trans), first)
+
+
+@pytest.mark.parametrize("W", [65, 130, 1024])
+def test_wide_outputs(W):
+    """Outputs wider than one 64-column tile."""
+    g = np.random.default_rng(W)
+    K = g.standard_normal((300, 257))
+    X = g.standard_normal((257, W))
+    ref = K @ X
+    got = _run(K, X, 0)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max() * 16
