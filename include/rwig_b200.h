@@ -145,6 +145,38 @@ RWIG_API int rwig_barycenter_log_dev(double* F, double* G, double* b, double* gr
                                      int N, int S, double reg, int withgrad, int max_iter,
                                      double zero_tol, void* stream);
 
+/* Wasserstein dictionary learning.
+ *
+ * rwig_wdl replaces cuda_wdl (inst/include/cuda_interface.cuh:31-39, called
+ * from src/wdl.cpp:76) with the same argument meaning, host pointers: Y
+ * (N x M documents), C (N x N cost); outputs A (N x S topics), W (S x M
+ * weights) and Yhat (N x M barycenters of the documents; NULL skips the
+ * inference).  max_iter is the fixed iteration count L of each training
+ * batch and the iteration cap of the inference barycenters (tolerance
+ * zero_tol); B batch size, E epochs; opt 0 SGD, 1 Adam, 2 AdamW with eta,
+ * gamma (AdamW decay), beta1, beta2, eps.  Added arguments: Alpha0 (N x S)
+ * and Lambda0 (S x M) initial logits (NULL: N(0,1) draws from mt19937(seed),
+ * Alpha first, as the reference GPU path does), and max_steps (> 0: stop
+ * after that many batches).  S <= 64.  Returns 0 or a negative error.
+ *
+ * rwig_wdl_batch_grad is one batched step (WassersteinDictionaryLearning::
+ * _train_batch_batched, src/wdl_impl.cpp:87-247; wdl_batch,
+ * src/cuda_wdl.cu:385): the batch-mean gradients g_Alpha (N x S) and
+ * g_lambda (S) of the D documents Y_B (N x D) with weights W_B (S x D) under
+ * topics A (N x S), after the softmax Jacobians.  mode 0: K_or_C is the
+ * Gibbs kernel K (N x N); mode 1: it is C and K = exp(-C/reg).  L fixed
+ * iterations.  The _dev form takes device pointers and a stream. */
+RWIG_API int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, const double* C, int N, int M,
+                      int S, double reg, int max_iter, double zero_tol, int B, int E, int opt, double eta,
+                      double gamma, double beta1, double beta2, double eps, int seed, int verbose,
+                      const double* Alpha0, const double* Lambda0, int max_steps);
+RWIG_API int rwig_wdl_batch_grad(double* g_Alpha, double* g_lambda, const double* A, const double* W_B,
+                                 const double* Y_B, const double* K_or_C, int N, int S, int D, double reg,
+                                 int L, int mode);
+RWIG_API int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const double* A,
+                                     const double* W_B, const double* Y_B, const double* K_or_C, int N,
+                                     int S, int D, double reg, int L, int mode, void* stream);
+
 /* Self-check of the engine's internal exponential (no counterpart in the
  * reference): evaluates it and CUDA's exp on n device doubles x, writing
  * y_engine and y_cuda (device).  Used by the test suite to bound its error. */

@@ -177,6 +177,61 @@ def barycenter(A, C, w, b_ext=None, barycenter_control: dict | None = None) -> d
     return out
 
 
+def wdl_cpp(Y, C, reg, S, batch_size, epochs, sinkhorn_mode=1, max_iter=1000, zero_tol=1e-6, optimizer=2,
+            eta=0.001, gamma=0.01, beta1=0.9, beta2=0.999, eps=1e-8, verbose=False, seed=42, Alpha0=None,
+            Lambda0=None, max_steps=0) -> dict:
+    """Wasserstein dictionary learning on a document matrix Y (N x M) and cost
+    C (N x N): the numeric core of rwig's wdl(), with wdl_cpp_cuda's argument
+    list (src/wdl.cpp:57-65).  Returns {"A": topics N x S, "W": weights S x M,
+    "Yhat": barycenters N x M}.  Training runs the batched parallel
+    barycenter, as the reference does on every path; the inference
+    barycenters are parallel, as on the reference's GPU path (sinkhorn_mode
+    is accepted for signature compatibility).  Alpha0 / Lambda0 give the
+    initial logits (otherwise N(0, 1) draws from mt19937(seed)); max_steps > 0
+    stops training after that many batches."""
+    Y = _mat(Y, "Y")
+    C = _mat(C, "C")
+    N, M = Y.shape
+    if C.shape != (N, N):
+        raise ValueError("C must be N x N for N rows of Y")
+    if optimizer not in (0, 1, 2):
+        raise ValueError("optimizer must be 0 (SGD), 1 (Adam) or 2 (AdamW)")
+    S = int(S)
+    a0 = None if Alpha0 is None else np.asfortranarray(np.asarray(Alpha0, dtype=np.float64))
+    l0 = None if Lambda0 is None else np.asfortranarray(np.asarray(Lambda0, dtype=np.float64))
+    if a0 is not None and a0.shape != (N, S):
+        raise ValueError("Alpha0 must be N x S")
+    if l0 is not None and l0.shape != (S, M):
+        raise ValueError("Lambda0 must be S x M")
+    A = np.zeros((N, S), order="F")
+    W = np.zeros((S, M), order="F")
+    Yhat = np.zeros((N, M), order="F")
+    rc = _lib.load().rwig_wdl(_dp(A), _dp(W), _dp(Yhat), _dp(Y), _dp(C), N, M, S, float(reg), int(max_iter),
+                              float(zero_tol), int(batch_size), int(epochs), int(optimizer), float(eta),
+                              float(gamma), float(beta1), float(beta2), float(eps), int(seed), int(bool(verbose)),
+                              _dp(a0), _dp(l0), int(max_steps))
+    _lib.check(rc)
+    return {"A": A, "W": W, "Yhat": Yhat}
+
+
+def wdl_batch_grad(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0):
+    """One batched WDL gradient step (WassersteinDictionaryLearning::
+    _train_batch_batched, src/wdl_impl.cpp:87-247): returns (g_Alpha (N x S),
+    g_lambda (S)).  mode 0: K_or_C is the Gibbs kernel; 1: it is the cost C."""
+    A = _mat(A, "A")
+    W_B = _mat(W_B, "W_B")
+    Y_B = _mat(Y_B, "Y_B")
+    KC = _mat(K_or_C, "K_or_C")
+    N, S = A.shape
+    D = W_B.shape[1]
+    if W_B.shape[0] != S or Y_B.shape != (N, D) or KC.shape != (N, N):
+        raise ValueError("A (N x S), W_B (S x D), Y_B (N x D) and K_or_C (N x N) do not match")
+    gA, gl = np.zeros((N, S), order="F"), np.zeros(S)
+    _lib.check(_lib.load().rwig_wdl_batch_grad(_dp(gA), _dp(gl), _dp(A), _dp(W_B), _dp(Y_B), _dp(KC), N, S, D,
+                                               float(reg), int(L), int(mode)))
+    return gA, gl
+
+
 # ---------------------------------------------------------------------------
 # device-resident entry points (torch CUDA tensors as plain device buffers)
 # ---------------------------------------------------------------------------

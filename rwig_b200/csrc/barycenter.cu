@@ -28,6 +28,7 @@
 #include <cstring>
 #include <vector>
 
+#include "barycenter.h"
 #include "dgemm.cuh"
 #include "engine.h"
 
@@ -53,8 +54,8 @@ __global__ void fill_kernel(double* x, long long n, double v) {
 }
 
 // GEMM epilogues (dgemm.cuh interface): each receives rows r0 .. r0+nr-1 of
-// the product, column s at t[s*ldt + r], and uses ws ((S+1)*ldt doubles) as
-// scratch.  Per-row reductions over s run in the fixed order s = 0..S-1.
+// the product, column s at t[s*ldt + r], and uses ws ((S+1)*ldt doubles of
+// it) as scratch.  Per-row reductions over s run in the fixed order s = 0..S-1.
 
 // After Z = K^T U_l: store Z, V = b / Z and the barycenter entry.
 // logdomain: b_j = exp(sum_s w_s log Z_js), bl[j] = log b_j;
@@ -65,7 +66,7 @@ struct EpiZ {
   double* V;
   double* bl;
   int N, S, logdomain;
-  __device__ void operator()(int r0, int nr, int, int, const double* t, int ldt, double* ws) const {
+  __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double* ws) const {
     if (nr <= 0) return;
     const int n = nr * S;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -101,7 +102,7 @@ struct EpiY {
   double* Unext;
   double* D;
   int M, S, ldd, logdomain;
-  __device__ void operator()(int r0, int nr, int, int, const double* t, int ldt, double*) const {
+  __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double*) const {
     if (nr <= 0) return;
     for (int e = threadIdx.x; e < nr * S; e += blockDim.x) {
       const int r = e % nr, s = e / nr, i = r0 + r;
@@ -130,7 +131,7 @@ struct EpiB1 {
   int N, S, logdomain, seed;
   double* T2;
   double* gw_part;
-  __device__ void operator()(int r0, int nr, int, int, const double* t, int ldt, double* ws) const {
+  __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double* ws) const {
     if (nr <= 0) return;
     const int n = nr * S;
     if (!seed) {
@@ -192,7 +193,7 @@ struct EpiB2 {
   int M, S, logdomain;
   double* gradA;
   double* Tnext;
-  __device__ void operator()(int r0, int nr, int, int, const double* t, int ldt, double*) const {
+  __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double*) const {
     if (nr <= 0) return;
     for (int e = threadIdx.x; e < nr * S; e += blockDim.x) {
       const int r = e % nr, s = e / nr;

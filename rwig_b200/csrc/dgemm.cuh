@@ -23,8 +23,12 @@
 // __syncthreads):
 //     epi(r0, nr, c0, nc, t, ldt, ws)
 // rows r0 .. r0+nr-1 of Y (nr <= 0: nothing to do), columns c0 .. c0+nc-1
-// (nc = BN), value (r0 + r, c0 + c) at t[c * ldt + r]; ws: (BN + 1) * ldt
-// doubles of shared scratch.  Columns at or beyond W hold zeros.
+// (nc = the tile's column count, tcols), value (r0 + r, c0 + c) at
+// t[c * ldt + r] (the epilogue may overwrite t); ws: 2 * (BN + 1) * ldt
+// doubles of shared scratch.  Columns at
+// or beyond W hold zeros.  Tiles are numbered with the column tiles fastest,
+// so the CTAs resident at one time share rows of K (one HBM pass over K when
+// it does not fit in L2).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -47,6 +51,8 @@ struct GemmArgs {
   const double* X;   // Kd x W, column-major
   long long ldx;
   int splits;        // cluster size along z: 1, 2, 4 or 8
+  int tcols;         // output columns per tile (<= BN; 0: BN).  A multiple of an
+                     // epilogue's column group keeps every group inside one tile.
 };
 
 template <int TRANS>
@@ -59,10 +65,11 @@ __host__ __device__ constexpr int b_stage_doubles() {
 }
 template <int TRANS, int NT>
 __host__ __device__ constexpr int smem_doubles() {
-  // pipeline ring, or (after the main loop) partial tile + summed rows + epilogue scratch
-  return (STAGES * (a_stage_doubles<TRANS>() + b_stage_doubles<NT>()) > NT * 8 * (3 * BM + 1) + BM)
+  // pipeline ring, or (after the main loop) partial tile + summed rows +
+  // epilogue scratch (two blocks of (BN + 1) x BM)
+  return (STAGES * (a_stage_doubles<TRANS>() + b_stage_doubles<NT>()) > NT * 8 * (2 * BM + 1) + 2 * (NT * 8 + 1) * BM)
              ? STAGES * (a_stage_doubles<TRANS>() + b_stage_doubles<NT>())
-             : NT * 8 * (3 * BM + 1) + BM;
+             : NT * 8 * (2 * BM + 1) + 2 * (NT * 8 + 1) * BM;
 }
 
 __device__ __forceinline__ void cp_async16(double* smem, const double* gmem, int src_bytes) {
@@ -109,8 +116,8 @@ __device__ __forceinline__ double ld_cluster(const double* p, unsigned rank) {
 // XV = 2: X columns copied as 16-byte pairs (ldx even, X 16-byte aligned);
 // XV = 1: 8-byte copies.  Out-of-range elements are zero-filled.
 template <int TRANS, int NT, int XV>
-__device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double* Bs, int m0, int n0, int k0,
-                                           int kend) {
+__device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double* Bs, int m0, int n0, int tc,
+                                           int k0, int kend) {
   const int tid = threadIdx.x;
   if (!TRANS) {
     // A[k][m] = K[m + k*ldk]: 32 k x 32 m-pairs
@@ -152,7 +159,7 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double
       const int gk = k0 + kp, gn = n0 + nn;
       int bytes = 0;
       const double* src = g.X;
-      if (gk < kend && gn < g.W) {
+      if (gk < kend && gn < g.W && nn < tc) {
         bytes = (gk + 1 < kend) ? 16 : 8;
         src = g.X + gk + (long long)gn * g.ldx;
       }
@@ -166,7 +173,7 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double
       const int gk = k0 + kk, gn = n0 + nn;
       int bytes = 0;
       const double* src = g.X;
-      if (gk < kend && gn < g.W) {
+      if (gk < kend && gn < g.W && nn < tc) {
         bytes = 8;
         src = g.X + gk + (long long)gn * g.ldx;
       }
@@ -182,7 +189,9 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
   constexpr int ASZ = a_stage_doubles<TRANS>(), BSZ = b_stage_doubles<NT>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gid = lane >> 2, tig = lane & 3;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tc = g.tcols > 0 ? g.tcols : BN;
+  const int ntiles = (g.W + tc - 1) / tc;
+  const int m0 = (blockIdx.x / ntiles) * BM, n0 = (blockIdx.x % ntiles) * tc;
   const int splits = g.splits;
   // the launch must form one cluster of `splits` CTAs along z
   if (splits > 1 && (int)cluster_nctarank() != splits) return;
@@ -203,7 +212,7 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
   double* Bs = smem + STAGES * ASZ;
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < nsteps) load_stage<TRANS, NT, XV>(g, As + s * ASZ, Bs + s * BSZ, m0, n0, kbeg + s * BK, kend);
+    if (s < nsteps) load_stage<TRANS, NT, XV>(g, As + s * ASZ, Bs + s * BSZ, m0, n0, tc, kbeg + s * BK, kend);
     cp_async_commit();
   }
   const int wm = (warp & 3) * 16, kh = (warp >> 2) * (BK / 2);
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
     const int nx = s + STAGES - 1;
     if (nx < nsteps) {
       const int q = nx % STAGES;
-      load_stage<TRANS, NT, XV>(g, As + q * ASZ, Bs + q * BSZ, m0, n0, kbeg + nx * BK, kend);
+      load_stage<TRANS, NT, XV>(g, As + q * ASZ, Bs + q * BSZ, m0, n0, tc, kbeg + nx * BK, kend);
     }
     cp_async_commit();
     const double* A = As + (s % STAGES) * ASZ;
@@ -277,7 +286,7 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
   }
   if (splits > 1) cluster_arrive();  // this CTA is done reading its peers
   __syncthreads();
-  epi(m0 + rl0, min(rows, g.Mo - (m0 + rl0)), n0, BN, fin, rows, ws);
+  epi(m0 + rl0, min(rows, g.Mo - (m0 + rl0)), n0, tc, fin, rows, ws);
   if (splits > 1) cluster_wait();  // peers are done reading this CTA
 }
 
@@ -286,7 +295,7 @@ struct EpiStore {
   double* Y;
   long long ldy;
   int W;
-  __device__ void operator()(int r0, int nr, int c0, int nc, const double* t, int ldt, double*) const {
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double*) const {
     if (nr <= 0) return;
     for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
       const int r = e % nr, c = e / nr;
@@ -301,8 +310,9 @@ struct EpiStore {
 // Largest power of two <= kMaxSplits that keeps the grid within about the
 // resident CTAs of one wave (two per SM for NT = 4, one for NT = 8) and
 // leaves every slice at least four BK steps.
-inline int pick_splits(const Context* ctx, int Mo, int Kd, int W, int NT) {
-  const long long tiles = (long long)((Mo + BM - 1) / BM) * ((W + NT * 8 - 1) / (NT * 8));
+inline int pick_splits(const Context* ctx, int Mo, int Kd, int W, int NT, int tc = 0) {
+  if (tc <= 0) tc = NT * 8;
+  const long long tiles = (long long)((Mo + BM - 1) / BM) * ((W + tc - 1) / tc);
   const long long target = (NT <= 4 ? 2LL : 1LL) * ctx->sm_count;
   int s = 1;
   while (s < kMaxSplits && tiles * s * 2 <= target && Kd >= s * 2 * 4 * BK) s *= 2;
@@ -321,7 +331,8 @@ int launch_kernel(const GemmArgs& g, const Epi& epi, cudaStream_t st) {
     attr_set = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((g.Mo + BM - 1) / BM, (g.W + NT * 8 - 1) / (NT * 8), g.splits);
+  const int tc = g.tcols > 0 ? g.tcols : NT * 8;
+  cfg.gridDim = dim3((unsigned)(((g.Mo + BM - 1) / BM) * ((g.W + tc - 1) / tc)), 1, g.splits);
   cfg.blockDim = dim3(NTH);
   cfg.dynamicSmemBytes = bytes;
   cfg.stream = st;
@@ -337,9 +348,9 @@ int launch_kernel(const GemmArgs& g, const Epi& epi, cudaStream_t st) {
 }
 
 // Y = op(K) X with epilogue `epi`.  g.splits <= 0 picks the split count,
-// otherwise it is rounded down to 1, 2, 4 or 8.  W <= 32 runs 32-column
-// tiles, wider outputs 64-column tiles (epilogues that need a whole row of Y
-// in one tile require W <= 64).  Returns 0 or an engine error code.
+// otherwise it is rounded down to 1, 2, 4 or 8.  Tiles of at most 32 columns
+// run on 32-column CTAs, wider ones on 64-column CTAs; g.tcols (<= 64) fixes
+// the columns per tile.  Returns 0 or an engine error code.
 template <int TRANS, class Epi>
 int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st) {
   if (!g.K || !g.X || g.Mo < 1 || g.Kd < 1 || g.W < 1)
@@ -348,8 +359,12 @@ int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st) {
     return set_error(RWIG_E_INVALID, "GEMM operand K needs an even leading dimension and 16-byte alignment");
   if (g.ldk < (TRANS ? g.Kd : g.Mo) || g.ldx < g.Kd)
     return set_error(RWIG_E_INVALID, "GEMM: leading dimension smaller than the operand");
-  const int NT = g.W <= 32 ? 4 : 8;
-  g.splits = g.splits <= 0 ? pick_splits(ctx, g.Mo, g.Kd, g.W, NT) : clamp_splits(g.splits);
+  const int NT = (g.tcols > 0 ? g.tcols : g.W) <= 32 ? 4 : 8;
+  if (g.tcols < 0 || g.tcols > NT * 8) return set_error(RWIG_E_INVALID, "GEMM: tile columns above 64");
+  if ((long long)((g.Mo + BM - 1) / BM) * ((g.W + (g.tcols > 0 ? g.tcols : NT * 8) - 1) /
+                                          (g.tcols > 0 ? g.tcols : NT * 8)) > 0x7fffffffLL)
+    return set_error(RWIG_E_INVALID, "GEMM: too many tiles");
+  g.splits = g.splits <= 0 ? pick_splits(ctx, g.Mo, g.Kd, g.W, NT, g.tcols) : clamp_splits(g.splits);
   const bool xv2 = (g.ldx % 2) == 0 && (reinterpret_cast<uintptr_t>(g.X) % 16) == 0;
   if (NT == 4) return xv2 ? launch_kernel<TRANS, 4, 2>(g, epi, st) : launch_kernel<TRANS, 4, 1>(g, epi, st);
   return xv2 ? launch_kernel<TRANS, 8, 2>(g, epi, st) : launch_kernel<TRANS, 8, 1>(g, epi, st);

@@ -1,0 +1,630 @@
+// wdl.cu -- Wasserstein dictionary learning (WassersteinDictionaryLearning,
+// src/wdl_impl.cpp; GPU path cuda_wdl, src/cuda_wdl.cu).
+//
+// Batched step (_train_batch_batched, wdl_impl.cpp:87-247; wdl_batch,
+// cuda_wdl.cu:385): the D documents of a batch are D parallel barycenters
+// sharing the topics A (N x S) and K = exp(-C/eps), stacked as SD = S*D
+// columns (column d*S + s).  Forward, L fixed iterations l = 0..L-1:
+//   KVB_l = K VB_l (VB_0 = 1),  UB_{l+1} = A_tiled / KVB_l,
+//   KTUB_{l+1} = K^T UB_{l+1},  bB_{l+1}[:,d] = prod_s KTUB[:,dS+s]^{W_B[s,d]},
+//   VB_{l+1} = bB_{l+1} / KTUB_{l+1};
+// backward l = L..1 (the parallel-barycenter adjoint, per document):
+//   l = L: bBbar = 2 (bB_L - Y_B), T2 = (bBbar W_B) o VB_L
+//   l < L: VBbar = -K^T T, bBbar = sum_s VBbar / KTUB_l,
+//          T2 = (bBbar W_B - VBbar / KTUB_l) o VB_l
+//   UBbar = K T2;  ABbar += UBbar / KVB_{l-1};  T = UBbar o UB_l / KVB_{l-1}
+//   wBbar += log(KTUB_l)^T (bBbar o bB_l)
+// then the softmax Jacobians and the batch means (:223-243).  Each product
+// is one FP64 tensor-core GEMM (dgemm.cuh) over all SD columns, its column
+// tiles holding whole documents, with the elementwise work fused into the
+// epilogue; every reduction runs in a fixed order.
+//
+// Training (_compute_serial, wdl_impl.cpp:254-347; cuda_wdl.cu:539-730):
+// per batch the step above, one optimizer update of the logits Alpha (N x S)
+// and Lambda (S x M) -- the Lambda gradient is g_lambda broadcast to every
+// document (:246) -- and the column softmaxes A = softmax(Alpha),
+// W = softmax(Lambda).  Inference (:349-377): the parallel barycenter of
+// every document under the learned A and W.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "barycenter.h"
+#include "dgemm.cuh"
+#include "engine.h"
+
+namespace rwig {
+namespace wdl {
+
+constexpr int TPB = 256;
+
+int grid_for(const Context* ctx, long long n) {
+  return (int)std::max<long long>(1, std::min<long long>((n + TPB - 1) / TPB, 8LL * ctx->sm_count));
+}
+
+__global__ void gibbs(const double* C, int N, long long ldk, double reg, double* K) {
+  const long long total = ldk * (long long)N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % ldk), j = (int)(k / ldk);
+    K[k] = (i < N) ? exp(-C[i + (long long)j * N] / reg) : 0.0;
+  }
+}
+
+// K given: copy into the padded layout.
+__global__ void copy_k(const double* Kin, int N, long long ldk, double* K) {
+  const long long total = ldk * (long long)N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % ldk), j = (int)(k / ldk);
+    K[k] = (i < N) ? Kin[i + (long long)j * N] : 0.0;
+  }
+}
+
+__global__ void fill(double* x, long long n, double v) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    x[k] = v;
+}
+
+// ---------------------------------------------------------------------------
+// GEMM epilogues over document groups of S columns (tile columns are whole
+// groups, c0 a multiple of S); W = S*D columns in all.
+// ---------------------------------------------------------------------------
+// After KVB_l = K VB_l: store it and UB_{l+1} = A_tiled / KVB_l.
+struct EpiY {
+  const double* A;
+  int N, S, W;
+  double* KVB;
+  double* UB;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double*) const {
+    if (nr <= 0) return;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      if (gc >= W) continue;
+      const int i = r0 + r;
+      const size_t k = (size_t)i + (size_t)gc * N;
+      const double y = t[c * ldt + r];
+      KVB[k] = y;
+      UB[k] = A[i + (size_t)(gc % S) * N] / y;
+    }
+  }
+};
+
+// After KTUB = K^T UB: store it, the barycenters bB (N x D) and VB = bB / KTUB.
+struct EpiZ {
+  const double* Wb;  // S x D weights of the batch, flat index = column
+  int N, S, W;
+  double* KTUB;
+  double* VB;
+  double* bB;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double* ws) const {
+    if (nr <= 0) return;
+    double* wb = ws + nc * ldt;  // per (group, row) barycenter entry
+    const int ng = nc / S;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      ws[c * ldt + r] = gc < W ? pow(t[c * ldt + r], Wb[gc]) : 1.0;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < nr * ng; p += blockDim.x) {
+      const int r = p % nr, q = p / nr, g0 = c0 + q * S;
+      if (g0 >= W) continue;
+      double acc = 1.0;  // barycenter_impl_parallel.cpp:120 order
+      for (int s = 0; s < S; ++s) acc *= ws[(q * S + s) * ldt + r];
+      bB[(size_t)(r0 + r) + (size_t)(g0 / S) * N] = acc;
+      wb[q * ldt + r] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      if (gc >= W) continue;
+      const size_t k = (size_t)(r0 + r) + (size_t)gc * N;
+      const double z = t[c * ldt + r];
+      KTUB[k] = z;
+      VB[k] = wb[(c / S) * ldt + r] / z;
+    }
+  }
+};
+
+// Backward after K^T T (t == nullptr at the seed step L, which has no
+// product): bBbar per (row, document), the next operand T2 and the wBbar
+// shares, summed per 8-row group into gw_part[(j/8)*W + column].
+struct EpiB1 {
+  const double* KTU;  // KTUB_l
+  const double* VB;   // VB_l
+  const double* Wb;
+  const double* bBl;  // bB_l (N x D)
+  const double* Yb;   // documents of the batch (N x D)
+  int N, S, W, seed;
+  double* T2;
+  double* gw_part;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double* ws) const {
+    if (nr <= 0) return;
+    double* wg = ws + nc * ldt;  // bBbar per (group, row)
+    const int ng = nc / S;
+    if (!seed) {
+      for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+        const int r = e % nr, c = e / nr, gc = c0 + c;
+        if (gc >= W) continue;
+        const size_t k = (size_t)(r0 + r) + (size_t)gc * N;
+        ws[c * ldt + r] = (-t[c * ldt + r]) / KTU[k];  // VBbar / KTUB_l
+      }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < nr * ng; p += blockDim.x) {
+      const int r = p % nr, q = p / nr, g0 = c0 + q * S;
+      if (g0 >= W) continue;
+      const size_t jd = (size_t)(r0 + r) + (size_t)(g0 / S) * N;
+      double bb;
+      if (seed) {
+        bb = 2.0 * (bBl[jd] - Yb[jd]);  // wdl_impl.cpp:176
+      } else {
+        bb = 0.0;
+        for (int s = 0; s < S; ++s) bb += ws[(q * S + s) * ldt + r];
+      }
+      wg[q * ldt + r] = bb;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      if (gc >= W) {
+        ws[c * ldt + r] = 0.0;
+        continue;
+      }
+      const size_t k = (size_t)(r0 + r) + (size_t)gc * N;
+      const double bb = wg[(c / S) * ldt + r];
+      double tt = bb * Wb[gc];
+      if (!seed) tt -= (-t[c * ldt + r]) / KTU[k];
+      T2[k] = tt * VB[k];
+      ws[c * ldt + r] = log(KTU[k]) * (bb * bBl[(size_t)(r0 + r) + (size_t)(gc / S) * N]);
+    }
+    __syncthreads();
+    const int n8 = (nr + 7) / 8;
+    for (int p = threadIdx.x; p < n8 * nc; p += blockDim.x) {
+      const int c = p % nc, g8 = p / nc, gc = c0 + c;
+      if (gc >= W) continue;
+      double v = 0.0;
+      for (int r = g8 * 8; r < min(nr, g8 * 8 + 8); ++r) v += ws[c * ldt + r];
+      gw_part[(size_t)(r0 / 8 + g8) * W + gc] += v;
+    }
+  }
+};
+
+// Backward after UBbar = K T2: ABbar += UBbar / KVB_{l-1} and the next
+// step's operand T = UBbar o UB_l / KVB_{l-1}.
+struct EpiB2 {
+  const double* UBl;
+  const double* KVBprev;
+  int N, W;
+  double* ABbar;
+  double* T;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double*) const {
+    if (nr <= 0) return;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      if (gc >= W) continue;
+      const size_t k = (size_t)(r0 + r) + (size_t)gc * N;
+      const double y = t[c * ldt + r];
+      ABbar[k] += y / KVBprev[k];
+      T[k] = (y * UBl[k]) / KVBprev[k];
+    }
+  }
+};
+
+// The seed step: EpiB1 over 8-row groups x column tiles, without a product.
+__global__ void seed_b1(EpiB1 epi, int N, int tc) {
+  extern __shared__ double ws[];  // 2 * tc * 8
+  const int r0 = blockIdx.x * 8, c0 = blockIdx.y * tc;
+  epi(r0, min(8, N - r0), c0, tc, nullptr, 8, ws);
+}
+
+// dot[c] = sum_i A[i, c % S] * X[i, c]; one block per column, fixed tree.
+__global__ void col_dots(const double* A, const double* X, int N, int S, double* dot) {
+  __shared__ double sh[TPB];
+  const int c = blockIdx.x, s = c % S;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) v += A[i + (size_t)s * N] * X[i + (size_t)c * N];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) dot[c] = sh[0];
+}
+
+// g_Alpha[i,s] = sum_d (a x_d - a dot_d) / D with a = A[i,s], x_d = ABbar[i, dS+s]
+// (softmax Jacobian per column, wdl_impl.cpp:223-228, then the batch mean :236-238).
+__global__ void alpha_grad(const double* A, const double* X, const double* dot, int N, int S, int D, double* g) {
+  const long long total = (long long)N * S;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % N), s = (int)(k / N);
+    const double a = A[k];
+    double acc = 0.0;
+    for (int d = 0; d < D; ++d) {
+      const int c = d * S + s;
+      acc += a * X[i + (size_t)c * N] - a * dot[c];
+    }
+    g[k] = acc / D;
+  }
+}
+
+// out[c] = sum over the 8-row groups of part[q*W + c]; one block per column.
+__global__ void reduce_cols(const double* part, int ngrp, int W, double* out) {
+  __shared__ double sh[TPB];
+  const int c = blockIdx.x;
+  double v = 0.0;
+  for (int q = threadIdx.x; q < ngrp; q += blockDim.x) v += part[(size_t)q * W + c];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[c] = sh[0];
+}
+
+// Softmax Jacobian of every document's weights (wdl_impl.cpp:229-233) and the
+// batch mean g_lambda (:239-243); x = wBbar (S x D), updated in place.
+__global__ void lambda_grad(const double* Wb, double* x, int S, int D, double* gl) {
+  for (int d = threadIdx.x; d < D; d += blockDim.x) {
+    const double* wd = Wb + (size_t)d * S;
+    double* xd = x + (size_t)d * S;
+    double dot = 0.0;
+    for (int s = 0; s < S; ++s) dot += wd[s] * xd[s];
+    for (int s = 0; s < S; ++s) xd[s] = wd[s] * xd[s] - wd[s] * dot;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double acc = 0.0;
+    for (int d = 0; d < D; ++d) acc += x[s + (size_t)d * S];
+    gl[s] = acc / D;
+  }
+}
+
+// Column softmax of an r x c matrix (wdl_impl.hpp:80-96; cuda_wdl.cu:45),
+// one block per column, fixed-order trees.
+__global__ void col_softmax(const double* X, int r, double* out) {
+  __shared__ double sh[TPB];
+  const double* x = X + (size_t)blockIdx.x * r;
+  double* o = out + (size_t)blockIdx.x * r;
+  double mx = -INFINITY;
+  for (int i = threadIdx.x; i < r; i += blockDim.x) mx = fmax(mx, x[i]);
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + h]);
+    __syncthreads();
+  }
+  mx = sh[0];
+  __syncthreads();
+  double sum = 0.0;
+  for (int i = threadIdx.x; i < r; i += blockDim.x) {
+    const double e = exp(x[i] - mx);
+    o[i] = e;
+    sum += e;
+  }
+  sh[threadIdx.x] = sum;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+    __syncthreads();
+  }
+  sum = sh[0];
+  for (int i = threadIdx.x; i < r; i += blockDim.x) o[i] = o[i] / sum;
+}
+
+// One optimizer update (optimizer.hpp:72-99; cuda_optimizer.cu:64): opt 0 SGD,
+// 1 Adam, 2 AdamW; c1 = 1 - beta1^step, c2 = 1 - beta2^step.  The gradient of
+// element k is g[gmod ? k % gmod : k] (gmod = S broadcasts g_lambda over the
+// documents).
+__global__ void opt_step(double* th, double* m, double* v, const double* g, int gmod, long long n, int opt,
+                         double eta, double gamma, double b1, double b2, double eps, double c1, double c2) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double gk = g[gmod ? k % gmod : k];
+    if (opt == 0) {
+      th[k] = th[k] - eta * gk;
+      continue;
+    }
+    m[k] = b1 * m[k] + (1.0 - b1) * gk;
+    v[k] = b2 * v[k] + (1.0 - b2) * (gk * gk);
+    const double mh = m[k] / c1, vh = v[k] / c2;
+    if (opt == 1) th[k] = th[k] - eta * (mh / (sqrt(vh) + eps));
+    else th[k] = (1.0 - eta * gamma) * th[k] - eta * (mh / (sqrt(vh) + eps));
+  }
+}
+
+enum {
+  SW_UH = 120, SW_VH, SW_KVH, SW_KTH, SW_BH, SW_T, SW_T2, SW_AB, SW_GWP, SW_DOT, SW_WBAR, SW_K,
+  SW_Y, SW_C, SW_ALPHA, SW_LAMBDA, SW_A, SW_W, SW_MA, SW_VA, SW_ML, SW_VL, SW_GA, SW_GL, SW_YHAT,
+  SW_HA, SW_HW, SW_HY, SW_HK, SW_HOUT
+};
+
+// Columns per GEMM tile: whole documents, at most 64.
+int tile_cols(int S, int SD) { return std::min((64 / S) * S, SD); }
+
+// Batched gradient on device buffers: K padded (ldk), A (N x S), Wb (S x D),
+// Yb (N x D); outputs gA (N x S) and gl (S).
+int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const double* A, const double* Wb,
+               const double* Yb, const double* K, long long ldk, int N, int S, int D, int L, int* launches) {
+  const int SD = S * D;
+  const size_t NW = (size_t)N * SD, ND = (size_t)N * D;
+  if (L <= 0) {
+    RWIG_CUDA_TRY(cudaMemsetAsync(gA, 0, sizeof(double) * N * S, st));
+    RWIG_CUDA_TRY(cudaMemsetAsync(gl, 0, sizeof(double) * S, st));
+    return 0;
+  }
+  const int ngrp = (N + 7) / 8;
+  double* Uh = (double*)scratch(ctx, SW_UH, sizeof(double) * NW * (L + 1));
+  double* Vh = (double*)scratch(ctx, SW_VH, sizeof(double) * NW * (L + 1));
+  double* KVh = (double*)scratch(ctx, SW_KVH, sizeof(double) * NW * (L + 1));
+  double* KTh = (double*)scratch(ctx, SW_KTH, sizeof(double) * NW * (L + 1));
+  double* Bh = (double*)scratch(ctx, SW_BH, sizeof(double) * ND * (L + 1));
+  double* T = (double*)scratch(ctx, SW_T, sizeof(double) * NW);
+  double* T2 = (double*)scratch(ctx, SW_T2, sizeof(double) * NW);
+  double* AB = (double*)scratch(ctx, SW_AB, sizeof(double) * NW);
+  double* gwp = (double*)scratch(ctx, SW_GWP, sizeof(double) * (size_t)ngrp * SD);
+  double* dot = (double*)scratch(ctx, SW_DOT, sizeof(double) * SD);
+  double* wbar = (double*)scratch(ctx, SW_WBAR, sizeof(double) * SD);
+  if (!Uh || !Vh || !KVh || !KTh || !Bh || !T || !T2 || !AB || !gwp || !dot || !wbar) return RWIG_E_NOMEM;
+  auto U = [&](int l) { return Uh + NW * l; };
+  auto V = [&](int l) { return Vh + NW * l; };
+  auto KV = [&](int l) { return KVh + NW * l; };
+  auto KT = [&](int l) { return KTh + NW * l; };
+  auto Bb = [&](int l) { return Bh + ND * l; };
+  const int tc = tile_cols(S, SD);
+  auto gemm = [&](int trans, const double* X, auto epi) -> int {
+    ++*launches;
+    const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
+    return trans ? dg::gemm<1>(ctx, g, epi, st) : dg::gemm<0>(ctx, g, epi, st);
+  };
+  fill<<<grid_for(ctx, NW), TPB, 0, st>>>(V(0), NW, 1.0);
+  ++*launches;
+  int rc;
+  for (int l = 0; l < L; ++l) {  // wdl_impl.cpp:124-160
+    rc = gemm(0, V(l), EpiY{A, N, S, SD, KV(l), U(l + 1)});
+    if (rc) return rc;
+    rc = gemm(1, U(l + 1), EpiZ{Wb, N, S, SD, KT(l + 1), V(l + 1), Bb(l + 1)});
+    if (rc) return rc;
+  }
+  RWIG_CUDA_TRY(cudaMemsetAsync(AB, 0, sizeof(double) * NW, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(gwp, 0, sizeof(double) * (size_t)ngrp * SD, st));
+  for (int l = L; l >= 1; --l) {  // :169-218
+    const bool seed = (l == L);
+    const EpiB1 e1{KT(l), V(l), Wb, Bb(l), Yb, N, S, SD, seed ? 1 : 0, T2, gwp};
+    if (seed) {
+      dim3 grid(ngrp, (SD + tc - 1) / tc);
+      seed_b1<<<grid, TPB, sizeof(double) * 2 * tc * 8, st>>>(e1, N, tc);
+      ++*launches;
+    } else {
+      rc = gemm(1, T, e1);  // K^T T
+      if (rc) return rc;
+    }
+    rc = gemm(0, T2, EpiB2{U(l), KV(l - 1), N, SD, AB, T});  // K T2
+    if (rc) return rc;
+  }
+  col_dots<<<SD, TPB, 0, st>>>(A, AB, N, S, dot);
+  alpha_grad<<<grid_for(ctx, (long long)N * S), TPB, 0, st>>>(A, AB, dot, N, S, D, gA);
+  reduce_cols<<<SD, TPB, 0, st>>>(gwp, ngrp, SD, wbar);
+  lambda_grad<<<1, TPB, 0, st>>>(Wb, wbar, S, D, gl);
+  *launches += 4;
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int check_dims(int N, int S, int D) {
+  if (N < 1 || S < 1 || D < 1) return set_error(RWIG_E_INVALID, "N, S and D must be >= 1");
+  if (S > 64) return set_error(RWIG_E_UNSUPPORTED, "more than 64 topics");
+  if ((long long)S * D > (1LL << 24)) return set_error(RWIG_E_UNSUPPORTED, "S * D too large");
+  return 0;
+}
+
+// K (padded, ldk) from K itself (mode 0) or from C (mode 1).
+int make_k(Context* ctx, cudaStream_t st, const double* KorC, int N, double reg, int mode, double** Kout,
+           long long* ldk_out) {
+  const long long ldk = ((N + 1) / 2) * 2;
+  double* K = (double*)scratch(ctx, SW_K, sizeof(double) * ldk * N);
+  if (!K) return RWIG_E_NOMEM;
+  if (mode == 1) gibbs<<<grid_for(ctx, ldk * N), TPB, 0, st>>>(KorC, N, ldk, reg, K);
+  else copy_k<<<grid_for(ctx, ldk * N), TPB, 0, st>>>(KorC, N, ldk, K);
+  RWIG_CUDA_TRY(cudaGetLastError());
+  *Kout = K;
+  *ldk_out = ldk;
+  return 0;
+}
+
+int batch_grad_entry(Context* ctx, cudaStream_t st, double* gA, double* gl, const double* A, const double* Wb,
+                     const double* Yb, const double* KorC, int N, int S, int D, double reg, int L, int mode) {
+  reset_report();
+  if (!gA || !gl || !A || !Wb || !Yb || !KorC) return set_error(RWIG_E_INVALID, "null pointer argument");
+  int rc = check_dims(N, S, D);
+  if (rc) return rc;
+  if (mode != 0 && mode != 1) return set_error(RWIG_E_INVALID, "mode must be 0 (K given) or 1 (C given)");
+  if (mode == 1 && (!(reg > 0.0) || !std::isfinite(reg))) return set_error(RWIG_E_INVALID, "reg must be > 0");
+  if (L < 0) return set_error(RWIG_E_INVALID, "L must be >= 0");
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
+  double* K = nullptr;
+  long long ldk = 0;
+  rc = make_k(ctx, st, KorC, N, reg, mode, &K, &ldk);
+  if (rc) return rc;
+  int launches = 1;
+  rc = batch_grad(ctx, st, gA, gl, A, Wb, Yb, K, ldk, N, S, D, L, &launches);
+  if (rc) return rc;
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  rwig_report& R = report();
+  R.iter = L;
+  R.device_ms = ms;
+  R.kernel_ms = ms;
+  R.kernel_launches = launches;
+  return 0;
+}
+
+}  // namespace wdl
+}  // namespace rwig
+
+using namespace rwig;
+
+extern "C" int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const double* A, const double* W_B,
+                                       const double* Y_B, const double* K_or_C, int N, int S, int D, double reg,
+                                       int L, int mode, void* stream) {
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return wdl::batch_grad_entry(ctx, stream ? (cudaStream_t)stream : ctx->stream, g_Alpha, g_lambda, A, W_B, Y_B,
+                               K_or_C, N, S, D, reg, L, mode);
+}
+
+extern "C" int rwig_wdl_batch_grad(double* g_Alpha, double* g_lambda, const double* A, const double* W_B,
+                                   const double* Y_B, const double* K_or_C, int N, int S, int D, double reg, int L,
+                                   int mode) {
+  if (!g_Alpha || !g_lambda || !A || !W_B || !Y_B || !K_or_C) {
+    reset_report();
+    return set_error(RWIG_E_INVALID, "null pointer argument");
+  }
+  {
+    const int rc = wdl::check_dims(N, S, D);
+    if (rc) return rc;
+  }
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaStream_t st = ctx->stream;
+  const size_t NS = (size_t)N * S, SD = (size_t)S * D, ND = (size_t)N * D, NN = (size_t)N * N;
+  double* dA = (double*)scratch(ctx, wdl::SW_HA, sizeof(double) * NS);
+  double* dW = (double*)scratch(ctx, wdl::SW_HW, sizeof(double) * SD);
+  double* dY = (double*)scratch(ctx, wdl::SW_HY, sizeof(double) * ND);
+  double* dK = (double*)scratch(ctx, wdl::SW_HK, sizeof(double) * NN);
+  double* dO = (double*)scratch(ctx, wdl::SW_HOUT, sizeof(double) * (NS + S));
+  if (!dA || !dW || !dY || !dK || !dO) return RWIG_E_NOMEM;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dA, A, sizeof(double) * NS, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dW, W_B, sizeof(double) * SD, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dY, Y_B, sizeof(double) * ND, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dK, K_or_C, sizeof(double) * NN, cudaMemcpyHostToDevice, st));
+  const int rc = wdl::batch_grad_entry(ctx, st, dO, dO + NS, dA, dW, dY, dK, N, S, D, reg, L, mode);
+  if (rc) return rc;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(g_Alpha, dO, sizeof(double) * NS, cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(g_lambda, dO + NS, sizeof(double) * S, cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  return 0;
+}
+
+extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, const double* C, int N, int M, int S,
+                        double reg, int max_iter, double zero_tol, int B, int E, int opt, double eta, double gamma,
+                        double beta1, double beta2, double eps, int seed, int verbose, const double* Alpha0,
+                        const double* Lambda0, int max_steps) {
+  reset_report();
+  if (!Y || !C) return set_error(RWIG_E_INVALID, "Y and C must be non-null");
+  if (M < 1 || B < 1 || E < 0) return set_error(RWIG_E_INVALID, "M, B must be >= 1 and E >= 0");
+  if (opt < 0 || opt > 2) return set_error(RWIG_E_INVALID, "opt must be 0 (SGD), 1 (Adam) or 2 (AdamW)");
+  if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
+  if (max_iter < 0) return set_error(RWIG_E_INVALID, "max_iter must be >= 0");
+  {
+    const int rc = wdl::check_dims(N, S, std::min(B, M));
+    if (rc) return rc;
+  }
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaStream_t st = ctx->stream;
+  using namespace wdl;
+  const size_t NS = (size_t)N * S, SM = (size_t)S * M, NM = (size_t)N * M, NN = (size_t)N * N;
+  double* dY = (double*)scratch(ctx, SW_Y, sizeof(double) * NM);
+  double* dC = (double*)scratch(ctx, SW_C, sizeof(double) * NN);
+  double* dAl = (double*)scratch(ctx, SW_ALPHA, sizeof(double) * NS);
+  double* dLa = (double*)scratch(ctx, SW_LAMBDA, sizeof(double) * SM);
+  double* dA = (double*)scratch(ctx, SW_A, sizeof(double) * NS);
+  double* dW = (double*)scratch(ctx, SW_W, sizeof(double) * SM);
+  double* mA = (double*)scratch(ctx, SW_MA, sizeof(double) * NS);
+  double* vA = (double*)scratch(ctx, SW_VA, sizeof(double) * NS);
+  double* mL = (double*)scratch(ctx, SW_ML, sizeof(double) * SM);
+  double* vL = (double*)scratch(ctx, SW_VL, sizeof(double) * SM);
+  double* gA = (double*)scratch(ctx, SW_GA, sizeof(double) * NS);
+  double* gl = (double*)scratch(ctx, SW_GL, sizeof(double) * S);
+  if (!dY || !dC || !dAl || !dLa || !dA || !dW || !mA || !vA || !mL || !vL || !gA || !gl) return RWIG_E_NOMEM;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dY, Y, sizeof(double) * NM, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dC, C, sizeof(double) * NN, cudaMemcpyHostToDevice, st));
+  // initial logits: given, or N(0, 1) draws from mt19937(seed), Alpha first
+  // then Lambda (cuda_wdl.cu:592-689)
+  std::vector<double> h;
+  if (!Alpha0 || !Lambda0) {
+    std::mt19937 rng((unsigned)seed);
+    std::normal_distribution<double> randn(0.0, 1.0);
+    h.resize(NS + SM);
+    for (auto& x : h) x = randn(rng);
+  }
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dAl, Alpha0 ? Alpha0 : h.data(), sizeof(double) * NS, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(
+      cudaMemcpyAsync(dLa, Lambda0 ? Lambda0 : h.data() + NS, sizeof(double) * SM, cudaMemcpyHostToDevice, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(mA, 0, sizeof(double) * NS, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(vA, 0, sizeof(double) * NS, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(mL, 0, sizeof(double) * SM, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(vL, 0, sizeof(double) * SM, st));
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
+  int launches = 0;
+  double* K = nullptr;
+  long long ldk = 0;
+  int rc = make_k(ctx, st, dC, N, reg, 1, &K, &ldk);  // K = exp(-C/reg) (wdl_impl.cpp:297)
+  if (rc) return rc;
+  col_softmax<<<S, TPB, 0, st>>>(dAl, N, dA);
+  col_softmax<<<M, TPB, 0, st>>>(dLa, S, dW);
+  launches += 3;
+  const int batches = (M % B) ? (M / B + 1) : (M / B);
+  int steps = 0;
+  for (int e = 0; e < E; ++e) {
+    for (int bi = 0; bi < batches; ++bi) {
+      if (max_steps > 0 && steps >= max_steps) break;
+      const int D = (bi == M / B) ? (M % B) : B;  // wdl_impl.cpp:91
+      rc = batch_grad(ctx, st, gA, gl, dA, dW + (size_t)bi * B * S, dY + (size_t)bi * B * N, K, ldk, N, S, D,
+                      max_iter, &launches);
+      if (rc) return rc;
+      ++steps;
+      const double c1 = 1.0 - std::pow(beta1, steps), c2 = 1.0 - std::pow(beta2, steps);
+      opt_step<<<grid_for(ctx, NS), TPB, 0, st>>>(dAl, mA, vA, gA, 0, NS, opt, eta, gamma, beta1, beta2, eps, c1,
+                                                  c2);
+      opt_step<<<grid_for(ctx, SM), TPB, 0, st>>>(dLa, mL, vL, gl, S, SM, opt, eta, gamma, beta1, beta2, eps, c1,
+                                                  c2);
+      col_softmax<<<S, TPB, 0, st>>>(dAl, N, dA);
+      col_softmax<<<M, TPB, 0, st>>>(dLa, S, dW);
+      launches += 4;
+      RWIG_CUDA_TRY(cudaGetLastError());
+      if (verbose) {
+        RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+        std::fprintf(stderr, "rwig_wdl: epoch %d of %d, batch %d of %d done\n", e + 1, E, bi + 1, batches);
+      }
+    }
+  }
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  float train_ms = 0.f;
+  cudaEventElapsedTime(&train_ms, ctx->ev0, ctx->ev1);
+  if (A) RWIG_CUDA_TRY(cudaMemcpyAsync(A, dA, sizeof(double) * NS, cudaMemcpyDeviceToHost, st));
+  if (W) RWIG_CUDA_TRY(cudaMemcpyAsync(W, dW, sizeof(double) * SM, cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (Yhat) {
+    // inference: the parallel barycenter of every document (wdl_impl.cpp:349-377)
+    double* dYh = (double*)scratch(ctx, SW_YHAT, sizeof(double) * NM);
+    if (!dYh) return RWIG_E_NOMEM;
+    for (int m = 0; m < M; ++m) {
+      rc = bary::run(ctx, st, false, nullptr, nullptr, dYh + (size_t)m * N, nullptr, nullptr, nullptr, nullptr,
+                     nullptr, dA, dW + (size_t)m * S, dC, nullptr, N, N, S, reg, 0, max_iter, zero_tol);
+      if (rc < 0) return rc;
+    }
+    RWIG_CUDA_TRY(cudaMemcpyAsync(Yhat, dYh, sizeof(double) * NM, cudaMemcpyDeviceToHost, st));
+    RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  reset_report();
+  rwig_report& R = report();
+  R.iter = steps;
+  R.device_ms = train_ms;
+  R.kernel_ms = train_ms;
+  R.kernel_launches = launches;
+  return 0;
+}

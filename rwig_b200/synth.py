@@ -62,3 +62,27 @@ def barycenter_config(n=2048, S=32, dim=50, salt: int = 0):
     w = dirichlet(rng(SEED_W, salt), 1.0, S)
     b_ext = dirichlet(rng(SEED_DOC, salt), 0.3, n)
     return A, C, w, b_ext
+
+
+def wdl_config(V=5000, M=2048, S=16, dim=64, salt: int = 0):
+    """WDL corpus: V embeddings ~ N(0, I_dim) with squared-Euclidean cost / max;
+    M documents of U{20..200} tokens whose ids follow Zipf(1.1) truncated to V
+    (redrawn until in range), as normalised count columns (V x M); initial
+    logits Alpha0 (V x S), Lambda0 (S x M) ~ N(0, 0.01) (variance 0.01,
+    standard deviation 0.1)."""
+    x = rng(SEED_X, salt).standard_normal((V, dim))
+    C = sq_euclid_cost(x, x)
+    g = rng(SEED_DOC, salt)
+    Y = np.zeros((V, M), order="F")
+    lengths = g.integers(20, 201, size=M)
+    for m in range(M):
+        ids = np.empty(0, dtype=np.int64)
+        while ids.size < lengths[m]:
+            z = g.zipf(1.1, size=2 * int(lengths[m]))
+            ids = np.concatenate([ids, z[z <= V] - 1])
+        np.add.at(Y[:, m], ids[:lengths[m]], 1.0)
+        Y[:, m] /= Y[:, m].sum()
+    gl = rng(SEED_W, salt)
+    Alpha0 = np.asfortranarray(0.1 * gl.standard_normal((V, S)))
+    Lambda0 = np.asfortranarray(0.1 * gl.standard_normal((S, M)))
+    return Y, C, Alpha0, Lambda0

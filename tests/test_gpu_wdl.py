@@ -1,0 +1,103 @@
+"""Parity of the CUDA Wasserstein dictionary learning (rwig_wdl_batch_grad,
+rwig_wdl) with the CPU oracle (WassersteinDictionaryLearning::
+_train_batch_batched and _compute_serial restated).  WDL has no known-answer
+vectors in the reference's own tests, so the oracle is the pin here; its
+batched adjoint is the parallel-barycenter adjoint, which the barycenter tests
+check against finite differences."""
+import numpy as np
+import pytest
+
+import oracle
+import rwig_b200 as rw
+from rwig_b200 import RwigError, synth
+from tests.util import PARITY_TOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(N, M, S, dim, reg, salt):
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=dim, salt=salt)
+    A = oracle.col_softmax(A0)
+    W = oracle.col_softmax(L0)
+    K = np.asfortranarray(np.exp(-C / reg))
+    return Y, C, K, A, W
+
+
+@pytest.mark.parametrize("N,D,S,L", [(200, 8, 4, 5), (333, 5, 16, 3), (150, 9, 7, 4), (64, 1, 3, 6),
+                                     (257, 3, 64, 2), (100, 4, 5, 1)])
+def test_batch_grad_matches_oracle(N, D, S, L):
+    reg = 0.1
+    Y, C, K, A, W = _batch(N, D, S, 8, reg, salt=N + D + S)
+    ref_gA, ref_gl = oracle.wdl_batch_grad(A, W, Y, K, L)
+    gA, gl = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+    assert rel_err(gA, ref_gA) <= PARITY_TOL, rel_err(gA, ref_gA)
+    assert rel_err(gl, ref_gl) <= PARITY_TOL, rel_err(gl, ref_gl)
+    # mode 1: the engine forms K = exp(-C/reg) itself
+    gA1, gl1 = rw.wdl_batch_grad(A, W, Y, C, reg, L, mode=1)
+    assert rel_err(gA1, ref_gA) <= PARITY_TOL and rel_err(gl1, ref_gl) <= PARITY_TOL
+
+
+def test_batch_grad_zero_iterations_is_zero():
+    Y, C, K, A, W = _batch(50, 3, 4, 4, 0.1, salt=3)
+    gA, gl = rw.wdl_batch_grad(A, W, Y, K, 0.1, 0, mode=0)
+    assert not gA.any() and not gl.any()
+
+
+def test_batch_grad_repeatable():
+    Y, C, K, A, W = _batch(300, 16, 16, 8, 0.1, salt=9)
+    first = rw.wdl_batch_grad(A, W, Y, K, 0.1, 4, mode=0)
+    for _ in range(2):
+        again = rw.wdl_batch_grad(A, W, Y, K, 0.1, 4, mode=0)
+        assert np.array_equal(again[0], first[0]) and np.array_equal(again[1], first[1])
+
+
+@pytest.mark.parametrize("opt", [0, 1, 2])
+def test_training_matches_oracle(opt):
+    """Training with a ragged last batch (M % B != 0) over two epochs."""
+    N, M, S, B, E, L, reg = 120, 21, 4, 8, 2, 5, 0.1
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=6, salt=opt + 40)
+    ref = oracle.wdl_train(Y, C, S, reg, L, B, E, A0, L0, opt=opt, eta=1e-2)
+    got = rw.wdl_cpp(Y, C, reg, S, B, E, max_iter=L, zero_tol=1e-6, optimizer=opt, eta=1e-2, Alpha0=A0,
+                     Lambda0=L0)
+    assert rel_err(got["A"], ref["A"]) <= PARITY_TOL, rel_err(got["A"], ref["A"])
+    assert rel_err(got["W"], ref["W"]) <= PARITY_TOL, rel_err(got["W"], ref["W"])
+    assert rw.last_report()["iter"] == ref["steps"] == E * 3
+
+
+def test_max_steps_and_inference():
+    """max_steps stops training early; Yhat is the parallel barycenter of every
+    document under the learned topics (wdl_impl.cpp:349-377)."""
+    N, M, S, B, L, reg = 90, 10, 3, 4, 6, 0.1
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=7)
+    ref = oracle.wdl_train(Y, C, S, reg, L, B, 3, A0, L0, opt=2, eta=5e-3, max_steps=4)
+    got = rw.wdl_cpp(Y, C, reg, S, B, 3, max_iter=L, zero_tol=1e-6, optimizer=2, eta=5e-3, Alpha0=A0,
+                     Lambda0=L0, max_steps=4)
+    assert rel_err(got["A"], ref["A"]) <= PARITY_TOL and rel_err(got["W"], ref["W"]) <= PARITY_TOL
+    for m in range(M):
+        b = oracle.barycenter_parallel(ref["A"], C, ref["W"][:, m], None, reg, with_grad=False, max_iter=L,
+                                       zero_tol=1e-6)["b"]
+        assert rel_err(got["Yhat"][:, m], b) <= 1e-9, m
+
+
+def test_seeded_initialisation_is_deterministic():
+    N, M, S = 60, 6, 3
+    Y, C, _, _ = synth.wdl_config(V=N, M=M, S=S, dim=4, salt=1)
+    r1 = rw.wdl_cpp(Y, C, 0.1, S, 3, 1, max_iter=3, seed=5)
+    r2 = rw.wdl_cpp(Y, C, 0.1, S, 3, 1, max_iter=3, seed=5)
+    r3 = rw.wdl_cpp(Y, C, 0.1, S, 3, 1, max_iter=3, seed=6)
+    assert np.array_equal(r1["A"], r2["A"]) and not np.array_equal(r1["A"], r3["A"])
+    np.testing.assert_allclose(r1["A"].sum(axis=0), 1.0, rtol=1e-12)
+    np.testing.assert_allclose(r1["W"].sum(axis=0), 1.0, rtol=1e-12)
+
+
+def test_invalid_arguments():
+    Y, C, K, A, W = _batch(40, 2, 3, 3, 0.1, salt=2)
+    with pytest.raises(RwigError):
+        rw.wdl_batch_grad(A, W, Y, K, 0.1, 3, mode=2)
+    with pytest.raises(RwigError):
+        rw.wdl_batch_grad(A, W, Y, C, -1.0, 3, mode=1)
+    Abig = np.full((40, 65), 1 / 40)
+    with pytest.raises(RwigError):
+        rw.wdl_batch_grad(Abig, np.full((65, 2), 1 / 65), Y, K, 0.1, 3)
+    with pytest.raises(ValueError):
+        rw.wdl_cpp(Y, C[:, :-1], 0.1, 3, 2, 1)
