@@ -5,7 +5,8 @@ problem per solve, a, b ~ Dirichlet(0.5), support points uniform in [0,1]^2,
 squared-Euclidean cost normalised by its max, eps = 0.01, max_iter = 2000,
 zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
 --workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)),
---workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50).
+--workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50),
+--workload wdl5000 (WDL training steps, V = 5000, K = 16, batch 64, L = 20, Adam).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
@@ -484,10 +485,118 @@ class BarycenterWorkload:
         return sum(secs), threads, sample
 
 
+class WdlWorkload:
+    """WDL training steps (one batch each: batched barycenter forward, adjoint,
+    softmax Jacobians, Adam update, softmax)."""
+
+    higher_is_better = True
+
+    def __init__(self, V=5000, M=2048, S=16, dim=64, B=64, reg=0.05, L=20, lr=1e-3):
+        self.V, self.M, self.S, self.dim, self.B, self.reg, self.L, self.lr = V, M, S, dim, B, reg, L, lr
+        self.unit = "steps/s"
+        self.metric = f"WDL training steps/s (V={V}, M={M}, K={S} topics, batch {B}, L={L}, Adam, FP64)"
+        self.desc = (f"WDL training: V={V} vocabulary embeddings ~ N(0, I_{dim}), squared-Euclidean cost / max; "
+                     f"M={M} documents of U{{20..200}} Zipf(1.1) tokens as normalised counts; K={S} topics with "
+                     f"N(0, 0.01) logits; batch {B}, eps={reg:g}, L={L} unrolled parallel-barycenter iterations, "
+                     f"quadratic loss, Adam lr={lr:g} (0.9, 0.999, 1e-8)")
+        self._data = None
+
+    def data(self):
+        if self._data is None:
+            from rwig_b200 import synth
+            self._data = synth.wdl_config(V=self.V, M=self.M, S=self.S, dim=self.dim)
+        return self._data
+
+    def products(self):
+        return 2 * self.L + 2 * self.L - 1  # forward K V, K^T U per iteration; backward K T2, K^T T
+
+    def step_flops(self):
+        return self.products() * 2.0 * self.V * self.V * self.S * self.B
+
+    def cpu_seconds(self, threads):
+        """Oracle batched gradient on a bounded sample (one document, L = 1:
+        three products of width S), scaled by FLOPs to one full step."""
+        import oracle
+        Y, C, A0, L0 = self.data()
+        K = np.asfortranarray(np.exp(-C / self.reg))
+        A = oracle.col_softmax(A0)
+        W = oracle.col_softmax(L0)
+        t0 = time.perf_counter()
+        oracle.wdl_batch_grad(A, W[:, :1], Y[:, :1], K, 1)
+        dt = time.perf_counter() - t0
+        scale = self.step_flops() / (3 * 2.0 * self.V * self.V * self.S)
+        sample = (f"oracle batched gradient of 1 document at L=1 (3 products of width {self.S}, 1 thread): "
+                  f"{dt:.2f} s, scaled by FLOPs x{scale:.0f} to one {self.B}-document L={self.L} step")
+        return dt * scale, 1, sample
+
+    def run(self, args, dev, world, rank, clocks_cls):
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        Y, C, A0, L0 = self.data()
+        L = _lib.load()
+        N, M, S = self.V, self.M, self.S
+        A = np.zeros((N, S), order="F")
+        W = np.zeros((S, M), order="F")
+        dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+
+        def train(steps):
+            rc = L.rwig_wdl(dp(A), dp(W), None, dp(Y), dp(C), N, M, S, self.reg, self.L, 1e-6, self.B, 1000, 1,
+                            self.lr, 0.01, 0.9, 0.999, 1e-8, 42, 0, dp(A0), dp(L0), int(steps))
+            _lib.check(rc)
+            return rw.last_report()
+
+        train(args.warmup)
+        torch.cuda.synchronize()
+        with clocks_cls(dev.index) as clocks:
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rep = train(args.steps)
+            wall = time.perf_counter() - t0
+            torch.cuda.synchronize()
+        dev_ms = max_over_ranks(rep["device_ms"], world, dev)
+        wall = max_over_ranks(wall, world, dev)
+        if rank != 0:
+            return None
+        tf_peak = measured_dgemm_tflops(dev)
+        achieved = self.step_flops() * args.steps / (dev_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
+                "frac": achieved / tf_peak, "traffic": None,
+                "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
+                "kernel": "dgemm_kernel with fused WDL epilogues (whole step, device time)",
+                "flops_per_step": self.step_flops(), "products_per_step": self.products()}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            secs, cores, sample = self.cpu_seconds(1)
+            cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
+        return {"value": args.steps * world / (dev_ms / 1e3), "ms_per_step": dev_ms / args.steps,
+                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
+                           "timing": "device events inside rwig_wdl around the training steps",
+                           "l2": "inputs larger than L2 (K = 200 MB)"},
+                "e2e": {"value": args.steps * world / wall, "unit": self.unit,
+                        "h2d_bytes_per_step": (N * M + N * N + N * S + S * M) * 8 / args.steps,
+                        "d2h_bytes_per_step": (N * S + S * M) * 8 / args.steps,
+                        "note": "one rwig_wdl call with host buffers (copies, K, training) over all steps"},
+                "gpu_launches": rep["kernel_launches"], "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clocks.summary()}
+
+    def reference(self, args):
+        secs, sample, cores = [], "", 1
+        for _ in range(args.steps):
+            s_, cores, sample = self.cpu_seconds(1)
+            secs.append(s_)
+        return sum(secs), cores, sample
+
+
 WORKLOADS = {
     "log4096": SinkhornWorkload("log", 4096, 4096, 0.01, 0.5, 2000, 1e-9),
     "vanilla256": SinkhornWorkload("vanilla", 256, 256, 0.1, 1.0, 1000, 1e-9),
     "barycenter2048": BarycenterWorkload(),
+    "wdl5000": WdlWorkload(),
 }
 
 
