@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--iters", type=int, default=20)
-    ap.add_argument("--s", type=int, default=32, help="histograms (barycenter --single)")
+    ap.add_argument("--s", type=int, default=32, help="histograms / topics (barycenter, wdl --single)")
     ap.add_argument("--l2-hot", type=float, default=None, help="engine option log_sinkhorn.l2_hot")
     return ap.parse_args()
 
@@ -661,6 +661,27 @@ def run_single(args):
 
     import rwig_b200 as rw
     from rwig_b200 import synth
+    if args.workload.startswith("wdl"):
+        # one batched WDL gradient step on device buffers: V = --n words,
+        # --s topics, --m documents, --iters iterations
+        from rwig_b200 import _lib
+        Y, C, A0, L0 = synth.wdl_config(V=args.n, M=args.m, S=args.s, dim=64)
+        dev = torch.device("cuda", 0)
+        A = torch.from_numpy(np.ascontiguousarray(np.exp(A0) / np.exp(A0).sum(0)).T.copy()).to(dev)
+        W = torch.from_numpy(np.ascontiguousarray((np.exp(L0) / np.exp(L0).sum(0)).T)).to(dev)
+        tY = torch.from_numpy(np.ascontiguousarray(Y.T)).to(dev)
+        tC = torch.from_numpy(np.ascontiguousarray(C.T)).to(dev)
+        gA = torch.empty((args.s, args.n), dtype=torch.float64, device=dev)
+        gl = torch.empty(args.s, dtype=torch.float64, device=dev)
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        L = _lib.load()
+        for _ in range(2):
+            _lib.check(L.rwig_wdl_batch_grad_dev(vp(gA), vp(gl), vp(A), vp(W), vp(tY), vp(tC), args.n, args.s,
+                                                 args.m, 0.05, args.iters, 1, None))
+        rep = rw.last_report()
+        print(json.dumps({"V": args.n, "S": args.s, "D": args.m, "L": args.iters, "device_ms": rep["device_ms"],
+                          "launches": rep["kernel_launches"]}))
+        return 0
     if args.workload.startswith("barycenter"):
         A, C, w, be = synth.barycenter_config(n=args.n, S=args.s, dim=50)
         for _ in range(2):
