@@ -177,6 +177,43 @@ RWIG_API int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const do
                                      const double* W_B, const double* Y_B, const double* K_or_C, int N,
                                      int S, int D, double reg, int L, int mode, void* stream);
 
+/* ---- batched log-Sinkhorn ---------------------------------------------
+ * Many independent problems with the semantics of rwig_sinkhorn_log in one
+ * call (no counterpart in the reference, whose GPU path solves one problem
+ * per call; the semantics are those of Sinkhorn::compute_log,
+ * src/sinkhorn_impl_log.cpp:225).  Problems with M <= 8192 and M*N <= 16 Mi
+ * run in one persistent launch, one CTA per problem (results identical
+ * whatever else is in the batch); others, and any problem the scaling form
+ * cannot treat (a zero mass, scalings beyond e^650), go through the per-call
+ * path.  Host pointers for rwig_batch_sinkhorn_log, device pointers for the
+ * _dev form.  P may be NULL.  The call returns 0 or a negative error for the
+ * whole batch; each out[i].status is the problem's own status (0/1/2, or a
+ * negative RWIG_E_* for a rejected problem). */
+typedef struct rwig_problem {
+  const double* a; /* M */
+  const double* b; /* N */
+  const double* C; /* M x N, column-major */
+  int M, N;
+  double reg;
+  int max_iter;
+  double zero_tol;
+  double* P;       /* M x N plan or NULL */
+  double* f;       /* M potentials */
+  double* g;       /* N potentials */
+} rwig_problem;
+
+typedef struct rwig_result {
+  double loss, err;
+  int iter, status;
+  double marg_l1_row, marg_l1_col;
+  int path;        /* 0: batched kernel, 1: per-call path */
+  int reserved;
+} rwig_result;
+
+RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_result* out);
+RWIG_API int rwig_batch_sinkhorn_log_dev(const rwig_problem* probs, int count, rwig_result* out,
+                                         void* stream);
+
 /* Self-check of the engine's internal exponential (no counterpart in the
  * reference): evaluates it and CUDA's exp on n device doubles x, writing
  * y_engine and y_cuda (device).  Used by the test suite to bound its error. */

@@ -60,6 +60,21 @@ class Report(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Problem(ctypes.Structure):
+    """rwig_problem (include/rwig_b200.h)."""
+    _fields_ = [("a", _vp), ("b", _vp), ("C", _vp), ("M", _i), ("N", _i), ("reg", _d), ("max_iter", _i),
+                ("zero_tol", _d), ("P", _vp), ("f", _vp), ("g", _vp)]
+
+
+class Result(ctypes.Structure):
+    """rwig_result (include/rwig_b200.h)."""
+    _fields_ = [("loss", _d), ("err", _d), ("iter", _i), ("status", _i), ("marg_l1_row", _d),
+                ("marg_l1_col", _d), ("path", _i), ("reserved", _i)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "rwig_init": (_i, [_i]),
@@ -90,6 +105,8 @@ SIGNATURES = {
                       _dp, _dp, _i]),
     "rwig_wdl_batch_grad": (_i, [_dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _i, _d, _i, _i]),
     "rwig_wdl_batch_grad_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _i, _i, _vp]),
+    "rwig_batch_sinkhorn_log": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result)]),
+    "rwig_batch_sinkhorn_log_dev": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result), _vp]),
 }
 
 _lib = None

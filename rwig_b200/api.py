@@ -232,6 +232,42 @@ def wdl_batch_grad(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0):
     return gA, gl
 
 
+def batch_sinkhorn_log(problems, with_plan=False) -> list:
+    """Solve many log-stabilised Sinkhorn problems in one call
+    (rwig_batch_sinkhorn_log).  `problems`: iterable of dicts with a, b, C
+    and optional reg (0.1), max_iter (1000), zero_tol (1e-6), as in
+    sinkhorn(..., method="log").  Returns one dict per problem with f, g,
+    (P), loss, iter, err, return_status, marginal violations and the path
+    taken (0: batched kernel, 1: per-call path)."""
+    problems = list(problems)
+    n = len(problems)
+    arr = (_lib.Problem * max(n, 1))()
+    res = (_lib.Result * max(n, 1))()
+    keep = []
+    for i, q in enumerate(problems):
+        a, b, C = _vec(q["a"], "a"), _vec(q["b"], "b"), _mat(q["C"], "C")
+        if a.shape[0] != C.shape[0] or b.shape[0] != C.shape[1]:
+            raise ValueError("a, b, C don't match in dimension!")
+        M, N = C.shape
+        f, g = np.zeros(M), np.zeros(N)
+        P = np.zeros((M, N), order="F") if with_plan else None
+        keep.append((a, b, C, f, g, P))
+        vp = lambda x: ctypes.c_void_p(x.ctypes.data) if x is not None else None  # noqa: E731
+        arr[i] = _lib.Problem(vp(a), vp(b), vp(C), M, N, float(q.get("reg", 0.1)), int(q.get("max_iter", 1000)),
+                              float(q.get("zero_tol", 1e-6)), vp(P), vp(f), vp(g))
+    _lib.check(_lib.load().rwig_batch_sinkhorn_log(arr, n, res))
+    out = []
+    for i in range(n):
+        r = res[i].as_dict()
+        d = {"f": keep[i][3], "g": keep[i][4], "loss": r["loss"], "iter": r["iter"], "err": r["err"],
+             "return_status": r["status"], "marg_l1_row": r["marg_l1_row"], "marg_l1_col": r["marg_l1_col"],
+             "path": r["path"]}
+        if with_plan:
+            d["P"] = keep[i][5]
+        out.append(d)
+    return out
+
+
 # ---------------------------------------------------------------------------
 # device-resident entry points (torch CUDA tensors as plain device buffers)
 # ---------------------------------------------------------------------------

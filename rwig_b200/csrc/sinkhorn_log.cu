@@ -704,7 +704,7 @@ __global__ void scatter_kernel(const double* x, const int* idx, int n, double* o
 // Shared driver of the vanilla and log-stabilised Sinkhorn entry points; inputs
 // on the device.  Log: f, g are the dual potentials (-inf off the support).
 // Vanilla: f, g receive the scalings u, v (0 off the support).
-static int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, double* grad_a, double* f,
+int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, double* grad_a, double* f,
                            double* g, double* loss, int* iter, double* err, const double* a,
                            const double* b, const double* C, int M, int N, double reg,
                            int withgrad, int max_iter, double zero_tol) {

@@ -43,4 +43,11 @@ int launch_absorb(Context* ctx, const double* C, long long ldc, const double* ft
                   int n, double inv_eps, double* K, cudaStream_t st);
 int launch_fill_ones(Context* ctx, double* x, int n, cudaStream_t st);
 
+// The per-call Sinkhorn driver (sinkhorn_log.cu) on device inputs: vanilla
+// (f, g receive u, v) or log-stabilised (f, g the potentials).  Returns the
+// reference status (0, 1, 2) or a negative engine error; fills report().
+int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, double* grad_a, double* f, double* g,
+                    double* loss, int* iter, double* err, const double* a, const double* b, const double* C,
+                    int M, int N, double reg, int withgrad, int max_iter, double zero_tol);
+
 }  // namespace rwig
