@@ -6,7 +6,8 @@ squared-Euclidean cost normalised by its max, eps = 0.01, max_iter = 2000,
 zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
 --workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)),
 --workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50),
---workload wdl5000 (WDL training steps, V = 5000, K = 16, batch 64, L = 20, Adam).
+--workload wdl5000 (WDL training steps, V = 5000, K = 16, batch 64, L = 20, Adam),
+--workload stream (200 mixed-size log-Sinkhorn requests, batched vs per call).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
@@ -592,11 +593,184 @@ class WdlWorkload:
         return sum(secs), cores, sample
 
 
+def device_cost(x, y, dev):
+    """sq_euclid_cost(x, y) built on the device (same elementwise operations in
+    the same order, so the same bits): an (n, m) tensor holding C column-major."""
+    import torch
+    tx = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    ty = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+    C = torch.zeros((ty.shape[0], tx.shape[0]), dtype=torch.float64, device=dev)
+    for k in range(tx.shape[1]):
+        d = tx[None, :, k] - ty[:, k, None]
+        C += d * d
+    C /= C.max()
+    return C
+
+
+class StreamWorkload:
+    """A stream of mixed-size log-Sinkhorn requests, solved by the batched
+    launch (value) and, for comparison, one rwig_sinkhorn_log_dev call per
+    request on the same device-resident inputs."""
+
+    higher_is_better = True
+
+    def __init__(self, R=200, max_iter=2000, tol=1e-9):
+        self.R, self.max_iter, self.tol = R, max_iter, tol
+        self.unit = "solves/s"
+        self.metric = "batched log-Sinkhorn solves/s on the mixed-size request stream (FP64)"
+        self.desc = (f"{R} log-Sinkhorn requests: n, m log-uniform in [64, 8192], eps from {{0.01, 0.05, 0.1}}, "
+                     f"Dirichlet(1) histograms, points uniform in [0,1]^d with d from {{2, 3, 64}}, "
+                     f"squared-Euclidean cost / max, tol {tol:g}, max_iter {max_iter}, outputs f, g, loss")
+
+    def build(self, dev):
+        import torch
+        from rwig_b200 import synth
+        reqs = synth.stream_requests(self.R)
+        data = []
+        for q in reqs:
+            a, b, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
+            C = device_cost(x, y, dev)
+            data.append({"q": q, "a": torch.from_numpy(a).to(dev), "b": torch.from_numpy(b).to(dev), "C": C,
+                         "f": torch.empty(q["m"], dtype=torch.float64, device=dev),
+                         "g": torch.empty(q["n"], dtype=torch.float64, device=dev),
+                         "ha": a, "hb": b})
+        return data
+
+    def problems(self, data, rng_idx=None):
+        from rwig_b200 import _lib
+        idx = list(range(len(data))) if rng_idx is None else rng_idx
+        arr = (_lib.Problem * len(idx))()
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        for k, i in enumerate(idx):
+            d = data[i]
+            arr[k] = _lib.Problem(vp(d["a"]), vp(d["b"]), vp(d["C"]), d["q"]["m"], d["q"]["n"], d["q"]["eps"],
+                                  self.max_iter, self.tol, None, vp(d["f"]), vp(d["g"]))
+        return arr
+
+    def run(self, args, dev, world, rank, clocks_cls):
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        L = _lib.load()
+        data = self.build(dev)
+        R = len(data)
+        stream = torch.cuda.current_stream()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        probs = self.problems(data)
+        res = (_lib.Result * R)()
+        # warm-up: the batched launch on a slice, and one per-call solve
+        for _ in range(max(1, args.warmup)):
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(self.problems(data, list(range(min(16, R)))), min(16, R),
+                                                     res, sp))
+        torch.cuda.synchronize()
+        with clocks_cls(dev.index) as clocks:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
+            e1.record(stream)
+            e1.synchronize()
+            batch_ms = e0.elapsed_time(e1)
+        launches = rw.last_report()["kernel_launches"]
+        bres = [res[i].as_dict() for i in range(R)]
+        bf = [d["f"].cpu().numpy() for d in data]
+        # the per-call path on the same inputs
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        piters = []
+        for d in data:
+            q = d["q"]
+            _lib.check(L.rwig_sinkhorn_log_dev(None, None, vp(d["f"]), vp(d["g"]), ctypes.byref(loss),
+                                               ctypes.byref(it), ctypes.byref(err), vp(d["a"]), vp(d["b"]),
+                                               vp(d["C"]), q["m"], q["n"], q["eps"], 0, self.max_iter, self.tol,
+                                               sp))
+            piters.append(it.value)
+        p1.record(stream)
+        p1.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+        # agreement of the two paths (same iteration counts, potentials to 1e-10)
+        worst = 0.0
+        for i, d in enumerate(data):
+            assert bres[i]["iter"] == piters[i], (i, bres[i]["iter"], piters[i])
+            pf = d["f"].cpu().numpy()
+            worst = max(worst, float(np.abs(bf[i] - pf).max() / max(np.abs(pf).max(), 1e-300)))
+        # end to end: host inputs through rwig_batch_sinkhorn_log
+        hC = [d["C"].cpu().numpy() for d in data]  # (n, m) row-major = column-major m x n
+        harr = (_lib.Problem * R)()
+        keep = []
+        for i, d in enumerate(data):
+            q = d["q"]
+            f, g = np.zeros(q["m"]), np.zeros(q["n"])
+            keep.append((f, g))
+            hv = lambda x: ctypes.c_void_p(x.ctypes.data)  # noqa: E731
+            harr[i] = _lib.Problem(hv(d["ha"]), hv(d["hb"]), hv(hC[i]), q["m"], q["n"], q["eps"], self.max_iter,
+                                   self.tol, None, hv(f), hv(g))
+        t0 = time.perf_counter()
+        _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
+        e2e_s = time.perf_counter() - t0
+        if rank != 0:
+            return None
+        hbm, src = measured_peaks()
+        elems = [d["q"]["m"] * d["q"]["n"] for d in data]
+        alg = sum((bres[i]["iter"] + 2) * elems[i] * 8.0 for i in range(R))
+        achieved = alg / (batch_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "peak_source": src,
+                "kernel": "batch_kernel (one CTA per problem) + per-call path for the largest",
+                "alg_bytes": alg, "note": "K read once per iteration plus the K build and final passes; "
+                                           "small problems stay in L2, so frac may exceed 1"}
+        in_kernel = sum(1 for r in bres if r["path"] == 0)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = self.cpu_baseline(data, bres)
+        return {"value": R * world / (batch_ms / 1e3), "ms_per_step": batch_ms / R,
+                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
+                           "step": "one request; the whole stream is one batched call",
+                           "requests_in_batched_kernel": in_kernel,
+                           "l2": "no flush (the stream itself is the workload)"},
+                "plain": {"value": R / (plain_ms / 1e3), "unit": self.unit,
+                          "path": "one rwig_sinkhorn_log_dev call per request, device-resident inputs",
+                          "speedup_batched_over_plain": plain_ms / batch_ms,
+                          "max_rel_diff_f_vs_batched": worst},
+                "e2e": {"value": R / e2e_s, "unit": self.unit,
+                        "h2d_bytes_per_step": sum((e + d["q"]["m"] + d["q"]["n"]) * 8 for e, d in zip(elems, data)) / R,
+                        "d2h_bytes_per_step": sum((d["q"]["m"] + d["q"]["n"]) * 8 for d in data) / R},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
+
+    def cpu_baseline(self, data, bres):
+        """The oracle (all host threads) on the three smallest requests, scaled
+        to the stream by element-iterations."""
+        import oracle
+        order = sorted(range(len(data)), key=lambda i: data[i]["q"]["m"] * data[i]["q"]["n"])[:3]
+        t = 0.0
+        work = 0.0
+        for i in order:
+            d = data[i]
+            C = d["C"].cpu().numpy().T
+            t0 = time.perf_counter()
+            r = oracle.sinkhorn_log(d["ha"], d["hb"], C, d["q"]["eps"], max_iter=self.max_iter, zero_tol=self.tol,
+                                    n_threads=os.cpu_count() or 1, want_P=False)
+            t += time.perf_counter() - t0
+            work += (r["iter"] + 2) * d["q"]["m"] * d["q"]["n"]
+        total = sum((bres[i]["iter"] + 2) * data[i]["q"]["m"] * data[i]["q"]["n"] for i in range(len(data)))
+        secs = t * total / work
+        return {"value": len(data) / secs, "unit": self.unit, "cores": os.cpu_count() or 1, "kind": "port",
+                "sample": f"3 smallest requests solved by the oracle ({t:.2f} s), scaled by element-iterations"}
+
+    def reference(self, args):
+        raise NotImplementedError
+
+
 WORKLOADS = {
     "log4096": SinkhornWorkload("log", 4096, 4096, 0.01, 0.5, 2000, 1e-9),
     "vanilla256": SinkhornWorkload("vanilla", 256, 256, 0.1, 1.0, 1000, 1e-9),
     "barycenter2048": BarycenterWorkload(),
     "wdl5000": WdlWorkload(),
+    "stream": StreamWorkload(),
 }
 
 

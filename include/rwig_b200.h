@@ -70,7 +70,9 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "log_sinkhorn.tau": absorption bound on |log u|, |log v| (default 100);
  *   "log_sinkhorn.l2_hot": share of each CTA's column groups of the scaled
  *       kernel copied with an L2 evict_last hint, the rest evict_first
- *       (default 0: all evict_first; negative: no hint). */
+ *       (default 0: all evict_first; negative: no hint);
+ *   "batch.profile": 1 prints the per-phase device time of every batched
+ *       Sinkhorn launch (CTA 0) to stderr (default 0). */
 RWIG_API int rwig_set_option(const char* name, double value);
 
 /* ---- vanilla Sinkhorn --------------------------------------------------
@@ -181,11 +183,11 @@ RWIG_API int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const do
  * Many independent problems with the semantics of rwig_sinkhorn_log in one
  * call (no counterpart in the reference, whose GPU path solves one problem
  * per call; the semantics are those of Sinkhorn::compute_log,
- * src/sinkhorn_impl_log.cpp:225).  Problems with M <= 8192 and M*N <= 16 Mi
- * run in one persistent launch, one CTA per problem (results identical
- * whatever else is in the batch); others, and any problem the scaling form
- * cannot treat (a zero mass, scalings beyond e^650), go through the per-call
- * path.  Host pointers for rwig_batch_sinkhorn_log, device pointers for the
+ * src/sinkhorn_impl_log.cpp:225).  Problems with M <= 8192 and M*N <= 4 Mi
+ * are iterated together in one cooperative launch, each on its own team of
+ * CTAs (results bitwise identical whatever else is in the batch); larger
+ * ones, and any problem the scaling form cannot treat (a zero mass, scalings
+ * beyond e^650), go through the per-call path.  Host pointers for rwig_batch_sinkhorn_log, device pointers for the
  * _dev form.  P may be NULL.  The call returns 0 or a negative error for the
  * whole batch; each out[i].status is the problem's own status (0/1/2, or a
  * negative RWIG_E_* for a rejected problem). */
@@ -206,6 +208,7 @@ typedef struct rwig_result {
   double loss, err;
   int iter, status;
   double marg_l1_row, marg_l1_col;
+  double device_us; /* device time of this problem's solve (start to end on its CTA, or the per-call solve) */
   int path;        /* 0: batched kernel, 1: per-call path */
   int reserved;
 } rwig_result;

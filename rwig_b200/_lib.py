@@ -69,7 +69,7 @@ class Problem(ctypes.Structure):
 class Result(ctypes.Structure):
     """rwig_result (include/rwig_b200.h)."""
     _fields_ = [("loss", _d), ("err", _d), ("iter", _i), ("status", _i), ("marg_l1_row", _d),
-                ("marg_l1_col", _d), ("path", _i), ("reserved", _i)]
+                ("marg_l1_col", _d), ("device_us", _d), ("path", _i), ("reserved", _i)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -51,7 +51,7 @@ int init_device(int dev, Context** out) {
 namespace {
 std::mutex g_opt_mu;
 std::map<std::string, double> g_opts;
-const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "log_sinkhorn.l2_hot"};
+const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "log_sinkhorn.l2_hot", "batch.profile"};
 }  // namespace
 
 double option(const char* name, double dflt) {

@@ -86,3 +86,34 @@ def wdl_config(V=5000, M=2048, S=16, dim=64, salt: int = 0):
     Alpha0 = np.asfortranarray(0.1 * gl.standard_normal((V, S)))
     Lambda0 = np.asfortranarray(0.1 * gl.standard_normal((S, M)))
     return Y, C, Alpha0, Lambda0
+
+
+SEED_STREAM = 1007
+
+
+def stream_requests(R=200, salt: int = 0):
+    """Mixed-size log-Sinkhorn request stream: n and m independently
+    log-uniform in [64, 8192] (rounded), eps uniform from {0.01, 0.05, 0.1},
+    point dimension d uniform from {2, 3, 64}; unit-rate exponential
+    inter-arrival gaps (Poisson arrivals, scaled by the caller).  Returns a
+    list of dicts (m, n, eps, d, salt, gap); request i's data come from
+    stream_request_data(m, n, d, salt)."""
+    g = rng(SEED_STREAM, salt)
+    lo, hi = np.log(64.0), np.log(8192.0)
+    ms = np.clip(np.rint(np.exp(g.uniform(lo, hi, R))), 64, 8192).astype(int)
+    ns = np.clip(np.rint(np.exp(g.uniform(lo, hi, R))), 64, 8192).astype(int)
+    eps = g.choice([0.01, 0.05, 0.1], size=R)
+    dims = g.choice([2, 3, 64], size=R)
+    gaps = g.exponential(1.0, size=R)
+    return [{"m": int(ms[i]), "n": int(ns[i]), "eps": float(eps[i]), "d": int(dims[i]), "salt": 10000 * salt + i,
+             "gap": float(gaps[i])} for i in range(R)]
+
+
+def stream_request_data(m, n, d, salt):
+    """Histograms a (m), b (n) ~ Dirichlet(1) and points x (m x d), y (n x d)
+    uniform in [0,1]^d; the cost is sq_euclid_cost(x, y)."""
+    x = rng(SEED_X, salt).random((m, d))
+    y = rng(SEED_Y, salt).random((n, d))
+    a = dirichlet(rng(SEED_A, salt), 1.0, m)
+    b = dirichlet(rng(SEED_B, salt), 1.0, n)
+    return a, b, x, y
