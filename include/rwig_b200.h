@@ -214,6 +214,25 @@ typedef struct rwig_result {
 } rwig_result;
 
 RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_result* out);
+
+/* ---- serving (continuous batching of log-Sinkhorn requests) -------------
+ * No counterpart in the reference.  A server keeps one service launch of the
+ * batched kernel running while requests arrive: rwig_server_submit copies a
+ * request (host pointers; M <= 8192) to the device and publishes it to the
+ * running kernel, which admits it at its next iteration and iterates it
+ * together with the others; rwig_server_poll returns 1 once the request is
+ * finished (f, g and P copied to the pointers given at submit; out filled),
+ * 0 while it runs.  submit returns the request's ticket (>= 0), or
+ * RWIG_E_BUSY when admitting it would exceed the device-memory budget or the
+ * slot table (512 requests) is full -- poll and retry.  The kernel ends after
+ * idle_ms without work and is restarted by the next submit or poll.
+ * Results are bitwise those of rwig_batch_sinkhorn_log for the same problem.
+ * One thread drives a server. */
+typedef struct rwig_server rwig_server;
+RWIG_API int rwig_server_create(rwig_server** out, double mem_budget_bytes, double idle_ms);
+RWIG_API int rwig_server_submit(rwig_server* server, const rwig_problem* prob);
+RWIG_API int rwig_server_poll(rwig_server* server, int ticket, rwig_result* out);
+RWIG_API int rwig_server_destroy(rwig_server* server);
 RWIG_API int rwig_batch_sinkhorn_log_dev(const rwig_problem* probs, int count, rwig_result* out,
                                          void* stream);
 

@@ -8,7 +8,7 @@ The compute path is the CUDA library rwig_b200/librwig_b200.so; importing this
 package does not load it until the first call.
 """
 from ._lib import RwigError, last_report, load  # noqa: F401
-from .api import (barycenter, batch_sinkhorn_log, check_barycenter_args, check_sinkhorn_args, choose_sinkhorn_method,  # noqa: F401
+from .api import (Server, barycenter, batch_sinkhorn_log, check_barycenter_args, check_sinkhorn_args, choose_sinkhorn_method,  # noqa: F401
                   sinkhorn, sinkhorn_log_device, sinkhorn_vanilla_device, wdl_batch_grad, wdl_cpp)
 
-__all__ = ["sinkhorn", "barycenter", "wdl_cpp", "wdl_batch_grad", "batch_sinkhorn_log", "sinkhorn_log_device", "sinkhorn_vanilla_device", "RwigError", "last_report", "load"]
+__all__ = ["sinkhorn", "barycenter", "wdl_cpp", "wdl_batch_grad", "batch_sinkhorn_log", "Server", "sinkhorn_log_device", "sinkhorn_vanilla_device", "RwigError", "last_report", "load"]

@@ -107,6 +107,10 @@ SIGNATURES = {
     "rwig_wdl_batch_grad_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _i, _i, _vp]),
     "rwig_batch_sinkhorn_log": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result)]),
     "rwig_batch_sinkhorn_log_dev": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result), _vp]),
+    "rwig_server_create": (_i, [ctypes.POINTER(_vp), _d, _d]),
+    "rwig_server_submit": (_i, [_vp, ctypes.POINTER(Problem)]),
+    "rwig_server_poll": (_i, [_vp, _i, ctypes.POINTER(Result)]),
+    "rwig_server_destroy": (_i, [_vp]),
 }
 
 _lib = None

@@ -268,6 +268,61 @@ def batch_sinkhorn_log(problems, with_plan=False) -> list:
     return out
 
 
+class Server:
+    """Continuous-batching log-Sinkhorn server (rwig_server_*): submit()
+    admits a request into the running service kernel, poll() returns its
+    result once finished.  One thread drives a server."""
+
+    def __init__(self, mem_budget_bytes=8e9, idle_ms=2.0):
+        self._L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self._L.rwig_server_create(ctypes.byref(h), float(mem_budget_bytes), float(idle_ms)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, a, b, C, reg=0.1, max_iter=1000, zero_tol=1e-6, with_plan=False):
+        """Returns a ticket (>= 0), or None when the server is full (poll and retry)."""
+        a, b, C = _vec(a, "a"), _vec(b, "b"), _mat(C, "C")
+        if a.shape[0] != C.shape[0] or b.shape[0] != C.shape[1]:
+            raise ValueError("a, b, C don't match in dimension!")
+        M, N = C.shape
+        f, g = np.zeros(M), np.zeros(N)
+        P = np.zeros((M, N), order="F") if with_plan else None
+        vp = lambda x: ctypes.c_void_p(x.ctypes.data) if x is not None else None  # noqa: E731
+        q = _lib.Problem(vp(a), vp(b), vp(C), M, N, float(reg), int(max_iter), float(zero_tol), vp(P), vp(f), vp(g))
+        rc = self._L.rwig_server_submit(self._h, ctypes.byref(q))
+        if rc == -7:  # RWIG_E_BUSY
+            return None
+        _lib.check(rc)
+        self._pending[rc] = (a, b, C, f, g, P)
+        return rc
+
+    def poll(self, ticket):
+        """The result dict once the request is finished, else None."""
+        r = _lib.Result()
+        rc = _lib.check(self._L.rwig_server_poll(self._h, int(ticket), ctypes.byref(r)))
+        if rc == 0:
+            return None
+        a, b, C, f, g, P = self._pending.pop(ticket)
+        d = r.as_dict()
+        out = {"f": f, "g": g, "loss": d["loss"], "iter": d["iter"], "err": d["err"], "return_status": d["status"],
+               "marg_l1_row": d["marg_l1_row"], "marg_l1_col": d["marg_l1_col"]}
+        if P is not None:
+            out["P"] = P
+        return out
+
+    def close(self):
+        if self._h:
+            self._L.rwig_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 # ---------------------------------------------------------------------------
 # device-resident entry points (torch CUDA tensors as plain device buffers)
 # ---------------------------------------------------------------------------

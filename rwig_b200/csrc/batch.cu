@@ -30,8 +30,10 @@
 // Every wait is bounded (2 s); on expiry the kernel sets an error word and
 // returns, and the host reports RWIG_E_TIMEOUT.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <numeric>
 #include <vector>
 
@@ -933,5 +935,250 @@ extern "C" int rwig_batch_sinkhorn_log_dev(const rwig_problem* probs, int count,
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   report().device_ms = ms;
   report().kernel_ms = ms;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Serving: requests are admitted into the running service kernel as they
+// arrive (continuous batching).  The caller drives the server from one
+// thread: submit() copies a request in and publishes it, poll() collects
+// finished ones.  Admission is bounded by a device-memory budget and by the
+// slot table of one launch (kMaxProbs); a full table is reused once every
+// slot of it has been collected and the kernel has gone idle.
+// ---------------------------------------------------------------------------
+struct rwig_server {
+  rwig::Context* ctx = nullptr;
+  cudaStream_t ks = nullptr, cs = nullptr;  // kernel stream, copy stream
+  rwig::batch::Prob* dprob = nullptr;       // device, kMaxProbs descriptors
+  unsigned* hpub = nullptr;                 // mapped: [0] published count, [1] stop
+  unsigned* dpub = nullptr;
+  unsigned* hdone = nullptr;                // mapped: done flag per slot
+  unsigned* ddone = nullptr;
+  double* hres = nullptr;                   // mapped: 10 results per slot
+  double* dres = nullptr;
+  unsigned* dctl = nullptr;                 // device control words
+  unsigned hctl_err = 0;
+  int nslots = 0, ptr = 0, unit0 = 0, next_ticket = 0;
+  bool launched = false;
+  double budget = 0.0, inflight = 0.0;
+  unsigned long long idle_ns = 0;
+  struct Slot {
+    int ticket = -1;
+    void* mem = nullptr;
+    double bytes = 0.0;
+    double *df = nullptr, *dg = nullptr, *dP = nullptr;
+    double *hf = nullptr, *hg = nullptr, *hP = nullptr;
+    int M = 0, N = 0;
+    bool collected = true;
+  };
+  std::vector<Slot> slots;
+};
+
+namespace rwig {
+namespace {
+
+bool kernel_running(rwig_server* s) {
+  if (!s->launched) return false;
+  const cudaError_t e = cudaStreamQuery(s->ks);
+  if (e == cudaErrorNotReady) return true;
+  s->launched = false;
+  (void)cudaGetLastError();
+  return false;
+}
+
+int ensure_running(rwig_server* s) {
+  if (kernel_running(s)) return 0;
+  unsigned err = 0;
+  RWIG_CUDA_TRY(cudaMemcpy(&err, s->dctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (err) return set_error(RWIG_E_TIMEOUT, "a bounded wait in the serving kernel expired");
+  bool pending = false;
+  for (int i = 0; i < s->nslots; ++i)
+    if (!s->hdone[i]) pending = true;
+  if (!pending) return 0;
+  const int rc = launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns);
+  if (rc) return rc;
+  s->launched = true;
+  return 0;
+}
+
+}  // namespace
+}  // namespace rwig
+
+extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, double idle_ms) {
+  reset_report();
+  if (!out) return set_error(RWIG_E_INVALID, "out is null");
+  *out = nullptr;
+  if (!(mem_budget_bytes > 0.0)) return set_error(RWIG_E_INVALID, "memory budget must be > 0");
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  if (ctx->sm_count > batch::kMaxTeam) return set_error(RWIG_E_UNSUPPORTED, "more SMs than the team limit");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto* s = new rwig_server();
+  s->ctx = ctx;
+  s->budget = mem_budget_bytes;
+  s->idle_ns = (unsigned long long)(std::max(0.0, idle_ms) * 1e6);
+  s->slots.resize(batch::kMaxProbs);
+  auto fail = [&](cudaError_t e, const char* what) {
+    rwig_server_destroy(s);
+    return cuda_fail(e, what);
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&s->ks, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+  if ((e = cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+  if ((e = cudaMalloc(&s->dprob, sizeof(batch::Prob) * batch::kMaxProbs)) != cudaSuccess) return fail(e, "descriptors");
+  if ((e = cudaMalloc(&s->dctl, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
+  if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
+    return fail(e, "done");
+  if ((e = cudaHostAlloc(&s->hres, sizeof(double) * 10 * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
+    return fail(e, "results");
+  if ((e = cudaHostGetDevicePointer(&s->dpub, s->hpub, 0)) != cudaSuccess) return fail(e, "pub map");
+  if ((e = cudaHostGetDevicePointer(&s->ddone, s->hdone, 0)) != cudaSuccess) return fail(e, "done map");
+  if ((e = cudaHostGetDevicePointer(&s->dres, s->hres, 0)) != cudaSuccess) return fail(e, "results map");
+  if ((e = cudaMemset(s->dctl, 0, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  s->hpub[0] = 0;
+  s->hpub[1] = 0;
+  std::memset(s->hdone, 0, sizeof(unsigned) * batch::kMaxProbs);
+  *out = s;
+  return 0;
+}
+
+extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
+  reset_report();
+  if (!s || !q) return set_error(RWIG_E_INVALID, "null server or problem");
+  if (!q->a || !q->b || !q->C || !q->f || !q->g || q->M < 1 || q->N < 1 || !(q->reg > 0.0) ||
+      !std::isfinite(q->reg) || q->max_iter < 1)
+    return set_error(RWIG_E_INVALID, "bad problem");
+  if (q->M > batch::kMaxRows) return set_error(RWIG_E_UNSUPPORTED, "M above 8192");
+  std::lock_guard<std::mutex> lk(s->ctx->mu);
+  using namespace batch;
+  // a fresh slot table once every slot of the current one has been collected
+  if (s->nslots == kMaxProbs) {
+    bool all = true;
+    for (int i = 0; i < s->nslots; ++i) all = all && s->slots[i].collected;
+    if (!all || kernel_running(s)) return RWIG_E_BUSY;
+    s->nslots = 0;
+    std::memset(s->hdone, 0, sizeof(unsigned) * kMaxProbs);
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    *(volatile unsigned*)s->hpub = 0u;
+  }
+  Prob d{};
+  long long kd = 0, wd = 0;
+  int ptr = s->ptr, unit0 = s->unit0;
+  place(*q, s->ctx->sm_count, ptr, unit0, d, kd, wd);
+  auto al = [](long long x) { return ((x + 31) / 32) * 32; };
+  const long long M = q->M, N = q->N;
+  const long long io = al(M) + al(N) + al(M * N) + al(M) + al(N) + (q->P ? al(M * N) : 0);
+  const double bytes = 8.0 * (double)(io + kd + wd);
+  if (s->inflight + bytes > s->budget) return RWIG_E_BUSY;
+  void* mem = nullptr;
+  RWIG_CUDA_TRY(cudaMallocAsync(&mem, (size_t)bytes, s->cs));
+  double* base = (double*)mem;
+  double* da = base;
+  double* db = da + al(M);
+  double* dC = db + al(N);
+  double* df = dC + al(M * N);
+  double* dg = df + al(M);
+  double* dP = q->P ? dg + al(N) : nullptr;
+  double* dk = base + io;
+  double* dw = dk + kd;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(da, q->a, sizeof(double) * M, cudaMemcpyHostToDevice, s->cs));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(db, q->b, sizeof(double) * N, cudaMemcpyHostToDevice, s->cs));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q->C, sizeof(double) * M * N, cudaMemcpyHostToDevice, s->cs));
+  const int slot = s->nslots;
+  d.a = da;
+  d.b = db;
+  d.C = dC;
+  d.f = df;
+  d.g = dg;
+  d.P = dP;
+  bind(d, dk, dw, s->dres + 10 * (size_t)slot);
+  RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &d, sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(s->cs));
+  s->ptr = ptr;
+  s->unit0 = unit0;
+  auto& sl = s->slots[slot];
+  sl.ticket = s->next_ticket++;
+  sl.mem = mem;
+  sl.bytes = bytes;
+  sl.df = df;
+  sl.dg = dg;
+  sl.dP = dP;
+  sl.hf = q->f;
+  sl.hg = q->g;
+  sl.hP = q->P;
+  sl.M = q->M;
+  sl.N = q->N;
+  sl.collected = false;
+  s->inflight += bytes;
+  s->hdone[slot] = 0u;
+  s->nslots = slot + 1;
+  std::atomic_thread_fence(std::memory_order_seq_cst);  // descriptor and buffers before the count
+  *(volatile unsigned*)s->hpub = (unsigned)s->nslots;
+  const int rc = ensure_running(s);
+  if (rc) return rc;
+  return sl.ticket;
+}
+
+extern "C" int rwig_server_poll(rwig_server* s, int ticket, rwig_result* out) {
+  reset_report();
+  if (!s || !out) return set_error(RWIG_E_INVALID, "null server or result");
+  std::lock_guard<std::mutex> lk(s->ctx->mu);
+  int slot = -1;
+  for (int i = 0; i < s->nslots; ++i)
+    if (s->slots[i].ticket == ticket && !s->slots[i].collected) slot = i;
+  if (slot < 0) return set_error(RWIG_E_INVALID, "unknown or already collected ticket");
+  if (!*(volatile unsigned*)(s->hdone + slot)) {
+    const int rc = ensure_running(s);  // a kernel that went idle before this request was seen
+    return rc ? rc : 0;
+  }
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  auto& sl = s->slots[slot];
+  const double* r = s->hres + 10 * (size_t)slot;
+  *out = rwig_result{};
+  if (r[3] == batch::kUnsafeStatus) {
+    out->status = RWIG_E_UNSUPPORTED;  // outside the scaling form: solve with rwig_sinkhorn_log
+  } else {
+    out->loss = r[0];
+    out->err = r[1];
+    out->iter = (int)r[2];
+    out->status = (int)r[3];
+    out->marg_l1_row = r[4];
+    out->marg_l1_col = r[5];
+    RWIG_CUDA_TRY(cudaMemcpyAsync(sl.hf, sl.df, sizeof(double) * sl.M, cudaMemcpyDeviceToHost, s->cs));
+    RWIG_CUDA_TRY(cudaMemcpyAsync(sl.hg, sl.dg, sizeof(double) * sl.N, cudaMemcpyDeviceToHost, s->cs));
+    if (sl.hP)
+      RWIG_CUDA_TRY(cudaMemcpyAsync(sl.hP, sl.dP, sizeof(double) * sl.M * sl.N, cudaMemcpyDeviceToHost, s->cs));
+  }
+  out->path = 0;
+  RWIG_CUDA_TRY(cudaFreeAsync(sl.mem, s->cs));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(s->cs));
+  s->inflight -= sl.bytes;
+  sl.collected = true;
+  sl.mem = nullptr;
+  return 1;
+}
+
+extern "C" int rwig_server_destroy(rwig_server* s) {
+  if (!s) return 0;
+  {
+    std::lock_guard<std::mutex> lk(s->ctx->mu);
+    if (s->hpub) {
+      s->hpub[1] = 1u;  // stop: the kernel ends once nothing runs
+      std::atomic_thread_fence(std::memory_order_seq_cst);
+    }
+    if (s->ks) cudaStreamSynchronize(s->ks);
+    for (auto& sl : s->slots)
+      if (sl.mem) cudaFreeAsync(sl.mem, s->cs);
+    if (s->cs) cudaStreamSynchronize(s->cs);
+    if (s->dprob) cudaFree(s->dprob);
+    if (s->dctl) cudaFree(s->dctl);
+    if (s->hpub) cudaFreeHost(s->hpub);
+    if (s->hdone) cudaFreeHost(s->hdone);
+    if (s->hres) cudaFreeHost(s->hres);
+    if (s->ks) cudaStreamDestroy(s->ks);
+    if (s->cs) cudaStreamDestroy(s->cs);
+  }
+  delete s;
   return 0;
 }

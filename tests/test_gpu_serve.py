@@ -1,0 +1,86 @@
+"""Continuous-batching server (rwig_server_*): requests admitted while others
+run give the same bits as the same requests solved alone, agree with the
+batched call and with the CPU oracle, and the server applies its memory
+budget and restarts after going idle."""
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+import rwig_b200 as rw
+from rwig_b200 import synth
+from tests.util import PARITY_TOL, dual_scale, rel_err
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(64, 64, 0.05, 2), (300, 200, 0.1, 3), (700, 1500, 0.01, 3), (1024, 1024, 0.05, 2), (2048, 700, 0.1, 64),
+         (5000, 90, 0.1, 3), (37, 100, 0.1, 64), (1500, 1200, 0.05, 2)]
+
+
+def _prob(i, m, n, reg, dim):
+    a, b, C = synth.sinkhorn_problem(m, n, 1.0, dim=dim, salt=500 + i)
+    return {"a": a, "b": b, "C": C, "reg": reg, "max_iter": 2000, "zero_tol": 1e-9}
+
+
+def _wait(server, tickets, timeout=60.0):
+    out, t0 = {}, time.time()
+    while len(out) < len(tickets):
+        for t in tickets:
+            if t not in out:
+                r = server.poll(t)
+                if r is not None:
+                    out[t] = r
+        assert time.time() - t0 < timeout, "server did not finish"
+    return [out[t] for t in tickets]
+
+
+def _submit(server, q):
+    while True:
+        t = server.submit(q["a"], q["b"], q["C"], q["reg"], q["max_iter"], q["zero_tol"])
+        if t is not None:
+            return t
+        time.sleep(0.001)
+
+
+def test_in_mix_equals_alone_and_oracle():
+    probs = [_prob(i, *s) for i, s in enumerate(SIZES)]
+    with rw.Server(idle_ms=5.0) as srv:
+        alone = []
+        for q in probs:  # one at a time
+            alone.append(_wait(srv, [_submit(srv, q)])[0])
+        # staggered: half now, the rest while the first half runs
+        first = [_submit(srv, q) for q in probs[::2]]
+        time.sleep(0.002)
+        second = [_submit(srv, q) for q in probs[1::2]]
+        mix = _wait(srv, first + second)
+    order = list(range(0, len(probs), 2)) + list(range(1, len(probs), 2))
+    for k, i in enumerate(order):
+        for key in ("f", "g"):
+            assert np.array_equal(mix[k][key], alone[i][key]), (i, key)
+        assert mix[k]["loss"] == alone[i]["loss"] and mix[k]["iter"] == alone[i]["iter"]
+    batch = rw.batch_sinkhorn_log(probs)
+    for i, q in enumerate(probs):
+        assert np.array_equal(batch[i]["f"], alone[i]["f"]) and batch[i]["iter"] == alone[i]["iter"]
+    for i in (0, 2, 5):
+        q = probs[i]
+        ref = oracle.sinkhorn_log(q["a"], q["b"], q["C"], q["reg"], max_iter=q["max_iter"], zero_tol=q["zero_tol"],
+                                  n_threads=8, want_P=False)
+        assert alone[i]["iter"] == ref["iter"]
+        sc = dual_scale(ref["f"], ref["g"])
+        assert rel_err(alone[i]["f"], ref["f"], sc) <= PARITY_TOL and rel_err(alone[i]["g"], ref["g"], sc) <= PARITY_TOL
+        assert abs(alone[i]["loss"] - ref["loss"]) <= PARITY_TOL * abs(ref["loss"])
+
+
+def test_memory_budget_and_idle_restart():
+    q = _prob(0, 400, 300, 0.05, 2)
+    big = _prob(1, 1000, 1000, 0.05, 2)
+    with rw.Server(mem_budget_bytes=12e6, idle_ms=1.0) as srv:  # holds the small one (~2 MB), not the big one (~17 MB)
+        t1 = srv.submit(q["a"], q["b"], q["C"], q["reg"], 2000, 1e-9)
+        assert t1 is not None
+        assert srv.submit(big["a"], big["b"], big["C"], big["reg"], 2000, 1e-9) is None  # over the budget
+        r1 = _wait(srv, [t1])[0]
+        time.sleep(0.05)  # the kernel goes idle and ends
+        t2 = _submit(srv, q)
+        r2 = _wait(srv, [t2])[0]
+    assert np.array_equal(r1["f"], r2["f"]) and r1["iter"] == r2["iter"]
