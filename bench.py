@@ -712,6 +712,7 @@ class StreamWorkload:
         t0 = time.perf_counter()
         _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
         e2e_s = time.perf_counter() - t0
+        serving = self.serve(data, hC, R / (batch_ms / 1e3))
         if rank != 0:
             return None
         hbm, src = measured_peaks()
@@ -739,7 +740,57 @@ class StreamWorkload:
                 "e2e": {"value": R / e2e_s, "unit": self.unit,
                         "h2d_bytes_per_step": sum((e + d["q"]["m"] + d["q"]["n"]) * 8 for e, d in zip(elems, data)) / R,
                         "d2h_bytes_per_step": sum((d["q"]["m"] + d["q"]["n"]) * 8 for d in data) / R},
+                "serving": serving,
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
+
+    def serve(self, data, hC, capacity):
+        """Poisson arrivals at 80 % of the batched throughput, in the stream's
+        order: the continuous-batching server (rwig_server_*) in real time, and
+        the per-call path (rwig_sinkhorn_log, host buffers) as a FIFO queue of
+        measured service times under the same arrivals.  Latency = completion
+        - arrival."""
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        L = _lib.load()
+        R = len(data)
+        rate = 0.8 * capacity
+        arrivals = np.cumsum([d["q"]["gap"] for d in data]) / rate
+        reqs = [(d["ha"], d["hb"], hC[i].T, d["q"]["eps"]) for i, d in enumerate(data)]
+        lat = np.zeros(R)
+        with rw.Server(mem_budget_bytes=64e9, idle_ms=5.0) as srv:
+            pending, idx, done = {}, 0, 0
+            t0 = time.perf_counter()
+            while done < R:
+                now = time.perf_counter() - t0
+                while idx < R and arrivals[idx] <= now:
+                    a, b, C, eps = reqs[idx]
+                    t = srv.submit(a, b, C, eps, self.max_iter, self.tol)
+                    if t is None:
+                        break
+                    pending[t] = idx
+                    idx += 1
+                for t in list(pending):
+                    if srv.poll(t) is not None:
+                        i = pending.pop(t)
+                        lat[i] = time.perf_counter() - t0 - arrivals[i]
+                        done += 1
+            span = time.perf_counter() - t0 - arrivals[0]
+        # per-call path: service times, then the FIFO queue under the same arrivals
+        svc = np.zeros(R)
+        for i, (a, b, C, eps) in enumerate(reqs):
+            t1 = time.perf_counter()
+            rw.sinkhorn(a, b, C, {"reg": eps, "method": "log", "max_iter": self.max_iter, "zero_tol": self.tol})
+            svc[i] = time.perf_counter() - t1
+        fin, plat = 0.0, np.zeros(R)
+        for i in range(R):
+            fin = max(fin, arrivals[i]) + svc[i]
+            plat[i] = fin - arrivals[i]
+        pspan = fin - arrivals[0]
+        ms = lambda x, q: float(np.percentile(x, q) * 1e3)  # noqa: E731
+        return {"arrival_rate_per_s": rate, "arrivals": "Poisson (unit-rate exponential gaps of the stream / rate)",
+                "server": {"solves_per_s": R / span, "p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99)},
+                "per_call_fifo": {"solves_per_s": R / pspan, "p50_ms": ms(plat, 50), "p99_ms": ms(plat, 99),
+                                  "mean_service_ms": float(svc.mean() * 1e3)}}
 
     def cpu_baseline(self, data, bres):
         """The oracle (all host threads) on the three smallest requests, scaled

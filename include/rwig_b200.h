@@ -202,6 +202,13 @@ typedef struct rwig_problem {
   double* P;       /* M x N plan or NULL */
   double* f;       /* M potentials */
   double* g;       /* N potentials */
+  /* Instead of C (C = NULL): source points X (M x d) and target points Y
+   * (N x d), column-major; the engine builds C_ij = sum_k (x_ik - y_jk)^2
+   * (ascending k, every operation rounded separately) divided by its
+   * maximum, on the device.  Batched and served problems only. */
+  const double* X;
+  const double* Y;
+  int d;
 } rwig_problem;
 
 typedef struct rwig_result {

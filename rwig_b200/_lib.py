@@ -63,7 +63,7 @@ class Report(ctypes.Structure):
 class Problem(ctypes.Structure):
     """rwig_problem (include/rwig_b200.h)."""
     _fields_ = [("a", _vp), ("b", _vp), ("C", _vp), ("M", _i), ("N", _i), ("reg", _d), ("max_iter", _i),
-                ("zero_tol", _d), ("P", _vp), ("f", _vp), ("g", _vp)]
+                ("zero_tol", _d), ("P", _vp), ("f", _vp), ("g", _vp), ("X", _vp), ("Y", _vp), ("d", _i)]
 
 
 class Result(ctypes.Structure):

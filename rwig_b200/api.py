@@ -232,6 +232,21 @@ def wdl_batch_grad(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0):
     return gA, gl
 
 
+def _cost_or_points(q):
+    """(C, None, None) from q["C"], or (None, X, Y) from point clouds q["x"]
+    (M x d), q["y"] (N x d), column-major; sizes checked against a, b."""
+    M, N = len(q["a"]), len(q["b"])
+    if q.get("C") is not None:
+        C = _mat(q["C"], "C")
+        if C.shape != (M, N):
+            raise ValueError("a, b, C don't match in dimension!")
+        return C, None, None
+    X, Y = _mat(q["x"], "x"), _mat(q["y"], "y")
+    if X.shape[0] != M or Y.shape[0] != N or X.shape[1] != Y.shape[1]:
+        raise ValueError("points don't match a, b or each other")
+    return None, X, Y
+
+
 def batch_sinkhorn_log(problems, with_plan=False) -> list:
     """Solve many log-stabilised Sinkhorn problems in one call
     (rwig_batch_sinkhorn_log).  `problems`: iterable of dicts with a, b, C
@@ -245,16 +260,16 @@ def batch_sinkhorn_log(problems, with_plan=False) -> list:
     res = (_lib.Result * max(n, 1))()
     keep = []
     for i, q in enumerate(problems):
-        a, b, C = _vec(q["a"], "a"), _vec(q["b"], "b"), _mat(q["C"], "C")
-        if a.shape[0] != C.shape[0] or b.shape[0] != C.shape[1]:
-            raise ValueError("a, b, C don't match in dimension!")
-        M, N = C.shape
+        a, b = _vec(q["a"], "a"), _vec(q["b"], "b")
+        C, X, Y = _cost_or_points(q)
+        M, N = a.shape[0], b.shape[0]
         f, g = np.zeros(M), np.zeros(N)
         P = np.zeros((M, N), order="F") if with_plan else None
-        keep.append((a, b, C, f, g, P))
+        keep.append((a, b, C, f, g, P, X, Y))
         vp = lambda x: ctypes.c_void_p(x.ctypes.data) if x is not None else None  # noqa: E731
         arr[i] = _lib.Problem(vp(a), vp(b), vp(C), M, N, float(q.get("reg", 0.1)), int(q.get("max_iter", 1000)),
-                              float(q.get("zero_tol", 1e-6)), vp(P), vp(f), vp(g))
+                              float(q.get("zero_tol", 1e-6)), vp(P), vp(f), vp(g), vp(X), vp(Y),
+                              0 if X is None else X.shape[1])
     _lib.check(_lib.load().rwig_batch_sinkhorn_log(arr, n, res))
     out = []
     for i in range(n):
@@ -280,21 +295,23 @@ class Server:
         self._h = h
         self._pending = {}
 
-    def submit(self, a, b, C, reg=0.1, max_iter=1000, zero_tol=1e-6, with_plan=False):
-        """Returns a ticket (>= 0), or None when the server is full (poll and retry)."""
-        a, b, C = _vec(a, "a"), _vec(b, "b"), _mat(C, "C")
-        if a.shape[0] != C.shape[0] or b.shape[0] != C.shape[1]:
-            raise ValueError("a, b, C don't match in dimension!")
-        M, N = C.shape
+    def submit(self, a, b, C=None, reg=0.1, max_iter=1000, zero_tol=1e-6, with_plan=False, x=None, y=None):
+        """Returns a ticket (>= 0), or None when the server is full (poll and
+        retry).  Give C, or point clouds x (M x d), y (N x d) for a cost built
+        on the device.  The arrays must stay alive until the result is polled."""
+        a, b = _vec(a, "a"), _vec(b, "b")
+        C, X, Y = _cost_or_points({"a": a, "b": b, "C": C, "x": x, "y": y})
+        M, N = a.shape[0], b.shape[0]
         f, g = np.zeros(M), np.zeros(N)
         P = np.zeros((M, N), order="F") if with_plan else None
-        vp = lambda x: ctypes.c_void_p(x.ctypes.data) if x is not None else None  # noqa: E731
-        q = _lib.Problem(vp(a), vp(b), vp(C), M, N, float(reg), int(max_iter), float(zero_tol), vp(P), vp(f), vp(g))
+        vp = lambda z: ctypes.c_void_p(z.ctypes.data) if z is not None else None  # noqa: E731
+        q = _lib.Problem(vp(a), vp(b), vp(C), M, N, float(reg), int(max_iter), float(zero_tol), vp(P), vp(f), vp(g),
+                         vp(X), vp(Y), 0 if X is None else X.shape[1])
         rc = self._L.rwig_server_submit(self._h, ctypes.byref(q))
         if rc == -7:  # RWIG_E_BUSY
             return None
         _lib.check(rc)
-        self._pending[rc] = (a, b, C, f, g, P)
+        self._pending[rc] = (a, b, C, f, g, P, X, Y)
         return rc
 
     def poll(self, ticket):
@@ -303,7 +320,7 @@ class Server:
         rc = _lib.check(self._L.rwig_server_poll(self._h, int(ticket), ctypes.byref(r)))
         if rc == 0:
             return None
-        a, b, C, f, g, P = self._pending.pop(ticket)
+        a, b, C, f, g, P, X, Y = self._pending.pop(ticket)
         d = r.as_dict()
         out = {"f": f, "g": g, "loss": d["loss"], "iter": d["iter"], "err": d["err"], "return_status": d["status"],
                "marg_l1_row": d["marg_l1_row"], "marg_l1_col": d["marg_l1_col"]}

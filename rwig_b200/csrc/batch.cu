@@ -62,7 +62,10 @@ constexpr double kUnsafeStatus = -100.0;
 struct Prob {
   const double* a;
   const double* b;
-  const double* C;   // m x n, column-major, leading dimension m
+  const double* C;   // m x n, column-major, leading dimension m (built here when X, Y are given)
+  const double* X;   // m x d source points (column-major) or null
+  const double* Y;   // n x d target points or null
+  int d;
   double* K;         // m x n, leading dimension ldk (even), 16-byte aligned
   long long ldk;
   double* P;         // optional plan (leading dimension m)
@@ -79,8 +82,8 @@ struct Prob {
 };
 
 struct State {  // per problem, identical in every CTA
-  int st, iter, par, init;
-  double err;
+  int st, iter, par, init;  // init: 2 cost from points pending, 1 first pass pending, 0 iterating
+  double err, cmax;
 };
 
 __host__ __device__ constexpr size_t smem_bytes() {
@@ -307,12 +310,43 @@ __device__ void final_pass(const Prob& p, const State& s, int k, double* red, in
     for (int i = 0; i < 4; ++i) p.colp[(size_t)k * 4 + i] = tt[i];
 }
 
+// Cost from points over this CTA's strip: C_ij = sum_k (x_ik - y_jk)^2 in
+// ascending k, each step rounded separately (the same operations and order as
+// a host that computes the differences, squares and sums elementwise, so the
+// same bits), stored un-normalised; the strip's maximum -> colp[k][2].
+__device__ void cost_pass(const Prob& p, int k, double* red, int& par) {
+  const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
+  const int m = p.m, n = p.n;
+  double mx = 0.0;
+  for (int j = c0; j < c1; ++j)
+    for (int i = threadIdx.x; i < m; i += NTT) {
+      double acc = 0.0;
+      for (int q = 0; q < p.d; ++q) {
+        const double t = __dsub_rn(p.X[i + (size_t)q * m], p.Y[j + (size_t)q * n]);
+        acc = __dadd_rn(acc, __dmul_rn(t, t));
+      }
+      const_cast<double*>(p.C)[i + (size_t)j * m] = acc;
+      mx = fmax(mx, acc);
+    }
+  // block maximum (exact, order-free)
+  mx = warp_max(mx);
+  __syncthreads();  // red is free
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int q = 0; q < NW; ++q) v = fmax(v, red[q]);
+    p.colp[(size_t)k * 4 + 2] = v;
+  }
+  __syncthreads();
+}
+
 // First pass of a problem over this CTA's strip: K = exp(-C/eps)
 // (sinkhorn_impl_vanilla.cpp:41 form) into its buffer, row partials of K 1
 // -> rowp[k] (the merge turns them into u_1 = a / (K 1)), and whether a mass
 // of the strip's columns or (member 0) of the rows is not positive -> colp[k][1].
 template <int RPT>
-__device__ void init_pass(const Prob& p, int k, double* red, int& par) {
+__device__ void init_pass(const Prob& p, int k, double cmax, double* red, int& par) {
   const int tid = threadIdx.x;
   const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
   const int m = p.m;
@@ -330,7 +364,12 @@ __device__ void init_pass(const Prob& p, int k, double* red, int& par) {
 #pragma unroll
     for (int t = 0; t < RPT; ++t)
       if (valid[t]) {
-        const double x = exp(-cj[tid + t * NTT] / p.eps);
+        double c = cj[tid + t * NTT];
+        if (p.X) {  // C /= max C
+          c = c / cmax;
+          const_cast<double*>(cj)[tid + t * NTT] = c;
+        }
+        const double x = exp(-c / p.eps);
         kj[tid + t * NTT] = x;
         r[t] += x;
       }
@@ -423,7 +462,7 @@ __global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const 
   if (cta == 0 && tid == 0) dctl[3] = min(pub[0], (unsigned)kMaxProbs);
   if (!gsync()) return;
   int np = (int)__ldcg(dctl + 3);
-  for (int q = tid; q < np; q += NTT) S[q] = State{done[q] ? ST_RETIRED : ST_RUN, 0, 0, 1, 1000.0};
+  for (int q = tid; q < np; q += NTT) S[q] = State{done[q] ? ST_RETIRED : ST_RUN, 0, 0, probs[q].X ? 2 : 1, 1000.0, 1.0};
   __syncthreads();
 
   const Ring ring{ringbuf, bar, l2_policy_evict_first()};
@@ -453,13 +492,16 @@ __global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const 
           case 3: final_pass<8, 2>(p, S[pi], k, red, par); break;
           default: final_pass<16, 1>(p, S[pi], k, red, par); break;
         }
+      } else if (S[pi].init == 2) {
+        cost_pass(p, k, red, par);
       } else if (S[pi].init) {
+        const double cm = S[pi].cmax;
         switch (p.cls) {
-          case 0: init_pass<1>(p, k, red, par); break;
-          case 1: init_pass<2>(p, k, red, par); break;
-          case 2: init_pass<4>(p, k, red, par); break;
-          case 3: init_pass<8>(p, k, red, par); break;
-          default: init_pass<16>(p, k, red, par); break;
+          case 0: init_pass<1>(p, k, cm, red, par); break;
+          case 1: init_pass<2>(p, k, cm, red, par); break;
+          case 2: init_pass<4>(p, k, cm, red, par); break;
+          case 3: init_pass<8>(p, k, cm, red, par); break;
+          default: init_pass<16>(p, k, cm, red, par); break;
         }
       } else {
         switch (p.cls) {
@@ -484,7 +526,7 @@ __global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const 
     // running problems, f and the row marginals for the finishing ones
     for (int pi = 0; pi < np; ++pi) {
       const int st = S[pi].st;
-      if (st != ST_RUN && st != ST_FIN) continue;
+      if ((st != ST_RUN && st != ST_FIN) || S[pi].init == 2) continue;
       const Prob& p = probs[pi];
       const double* ucur = S[pi].par ? p.u1 : p.u0;
       double* unext = S[pi].par ? p.u0 : p.u1;
@@ -558,6 +600,17 @@ __global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const 
         if (lane == 0) s.st = ST_RETIRED;
         continue;
       }
+      if (s.init == 2) {  // maximum of the cost over the team's strips
+        double mx = 0.0;
+        for (int k = lane; k < p.gp; k += 32) mx = fmax(mx, __ldcg(p.colp + (size_t)k * 4 + 2));
+        mx = warp_max(mx);
+        if (lane == 0) {
+          s.cmax = mx;
+          s.init = 1;
+          ++running;
+        }
+        continue;
+      }
       double er = 0.0, ec = 0.0, bad = 0.0;
       for (int u = lane; u < p.nunits; u += 32) {
         er += __ldcg(p.unitp + (size_t)u * 4 + 0);
@@ -591,7 +644,7 @@ __global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const 
       if (s.iter < p.max_iter && s.err >= p.tol) s.par ^= 1;
       else s.st = ST_FIN;
     }
-    for (int pi = np + tid; pi < np_new; pi += NTT) S[pi] = State{ST_RUN, 0, 0, 1, 1000.0};
+    for (int pi = np + tid; pi < np_new; pi += NTT) S[pi] = State{ST_RUN, 0, 0, probs[pi].X ? 2 : 1, 1000.0, 1.0};
     double t[1] = {(double)(running + (tid == 0 ? np_new - np : 0))};
     block_sum_cols<1, NW>(t, red, par);  // (also orders the state updates before the next pass)
     np = np_new;
@@ -644,11 +697,15 @@ void place(const rwig_problem& q, int G, int& ptr, int& unit0, batch::Prob& d, l
   d.a = q.a;
   d.b = q.b;
   d.C = q.C;
+  d.X = q.C ? nullptr : q.X;
+  d.Y = q.C ? nullptr : q.Y;
+  d.d = q.C ? 0 : q.d;
   d.P = q.P;
   d.f = q.f;
   d.g = q.g;
   kdoubles = al(d.ldk * q.N);
-  wdoubles = 2 * al(q.M) + al((long long)d.gp * q.M) + al(4LL * d.gp) + al(4LL * d.nunits) + 32;
+  wdoubles = 2 * al(q.M) + al((long long)d.gp * q.M) + al(4LL * d.gp) + al(4LL * d.nunits) + 32 +
+             (q.C ? 0 : al((long long)q.M * q.N));  // the cost built from points
 }
 
 // Points the work arrays of d into w (wdoubles doubles) and K into k.
@@ -661,6 +718,7 @@ void bind(batch::Prob& d, double* k, double* w, double* res) {
   d.colp = d.rowp + al((long long)d.gp * d.m);
   d.unitp = d.colp + al(4LL * d.gp);
   d.res = res;
+  if (d.X) d.C = d.unitp + al(4LL * d.nunits) + 32;
 }
 
 int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, const unsigned* pub, unsigned* done,
@@ -780,7 +838,8 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
     rwig_result& o = out[idx[t]];
     const double* r = hres.data() + 10 * (size_t)t;
     if (r[3] == kUnsafeStatus) {
-      percall.push_back(idx[t]);
+      if (probs[idx[t]].C) percall.push_back(idx[t]);
+      else o.status = RWIG_E_UNSUPPORTED;  // outside the scaling form; the per-call path takes C
       continue;
     }
     o.loss = r[0];
@@ -803,12 +862,20 @@ int batch_device(Context* ctx, cudaStream_t st, const rwig_problem* probs, int c
   for (int i = 0; i < count; ++i) {
     const rwig_problem& q = probs[i];
     out[i] = rwig_result{};
-    if (!q.a || !q.b || !q.C || !q.f || !q.g || q.M < 1 || q.N < 1 || !(q.reg > 0.0) || !std::isfinite(q.reg)) {
+    const bool pts = !q.C && q.X && q.Y && q.d >= 1;
+    if (!q.a || !q.b || !(q.C || pts) || !q.f || !q.g || q.M < 1 || q.N < 1 || !(q.reg > 0.0) ||
+        !std::isfinite(q.reg)) {
       out[i].status = RWIG_E_INVALID;
       continue;
     }
-    if (q.M <= kMaxRows && q.max_iter >= 1 && (long long)q.M * q.N <= kBatchMaxElems) eligible.push_back(i);
-    else percall.push_back(i);
+    if (pts && (q.M > kMaxRows || q.max_iter < 1)) {
+      out[i].status = RWIG_E_UNSUPPORTED;  // the per-call path takes a cost matrix
+      continue;
+    }
+    if (q.M <= kMaxRows && q.max_iter >= 1 && (pts || (long long)q.M * q.N <= kBatchMaxElems))
+      eligible.push_back(i);
+    else
+      percall.push_back(i);
   }
   int launches = 0;
   RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
@@ -869,17 +936,22 @@ extern "C" int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwi
   // one device block for every problem's a, b, C, P, f, g (256-byte aligned slices)
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   std::vector<long long> off(count + 1, 0);
+  auto cost_doubles = [&](const rwig_problem& q) -> long long {  // C, or the points
+    const long long M = std::max(q.M, 0), N = std::max(q.N, 0);
+    return q.C ? al(M * N) : al(M * std::max(q.d, 0)) + al(N * std::max(q.d, 0));
+  };
   for (int i = 0; i < count; ++i) {
     const rwig_problem& q = probs[i];
     const long long M = std::max(q.M, 0), N = std::max(q.N, 0);
-    off[i + 1] = off[i] + al(M) + al(N) + al(M * N) + (q.P ? al(M * N) : 0) + al(M) + al(N);
+    off[i + 1] = off[i] + al(M) + al(N) + cost_doubles(q) + (q.P ? al(M * N) : 0) + al(M) + al(N);
   }
   double* dev = (double*)scratch(ctx, SBT_HOSTIO, sizeof(double) * std::max<long long>(off[count], 32));
   if (!dev) return RWIG_E_NOMEM;
   std::vector<rwig_problem> dp(probs, probs + count);
   for (int i = 0; i < count; ++i) {
     const rwig_problem& q = probs[i];
-    if (!q.a || !q.b || !q.C || !q.f || !q.g || q.M < 1 || q.N < 1) {
+    const bool pts = !q.C && q.X && q.Y && q.d >= 1;
+    if (!q.a || !q.b || !(q.C || pts) || !q.f || !q.g || q.M < 1 || q.N < 1) {
       dp[i].a = nullptr;  // rejected by the device driver with RWIG_E_INVALID
       continue;
     }
@@ -887,12 +959,22 @@ extern "C" int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwi
     double* da = dev + off[i];
     double* db = da + al(M);
     double* dC = db + al(N);
-    double* dP = q.P ? dC + al(M * N) : nullptr;
-    double* df = q.P ? dP + al(M * N) : dC + al(M * N);
+    double* dP = q.P ? dC + cost_doubles(q) : nullptr;
+    double* df = q.P ? dP + al(M * N) : dC + cost_doubles(q);
     double* dg = df + al(M);
     RWIG_CUDA_TRY(cudaMemcpyAsync(da, q.a, sizeof(double) * M, cudaMemcpyHostToDevice, st));
     RWIG_CUDA_TRY(cudaMemcpyAsync(db, q.b, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-    RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q.C, sizeof(double) * M * N, cudaMemcpyHostToDevice, st));
+    if (pts) {
+      double* dX = dC;
+      double* dY = dC + al(M * q.d);
+      RWIG_CUDA_TRY(cudaMemcpyAsync(dX, q.X, sizeof(double) * M * q.d, cudaMemcpyHostToDevice, st));
+      RWIG_CUDA_TRY(cudaMemcpyAsync(dY, q.Y, sizeof(double) * N * q.d, cudaMemcpyHostToDevice, st));
+      dp[i].X = dX;
+      dp[i].Y = dY;
+      dC = nullptr;
+    } else {
+      RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q.C, sizeof(double) * M * N, cudaMemcpyHostToDevice, st));
+    }
     dp[i].a = da;
     dp[i].b = db;
     dp[i].C = dC;
@@ -958,7 +1040,7 @@ struct rwig_server {
   double* dres = nullptr;
   unsigned* dctl = nullptr;                 // device control words
   unsigned hctl_err = 0;
-  int nslots = 0, ptr = 0, unit0 = 0, next_ticket = 0;
+  int nslots = 0, npub = 0, ptr = 0, unit0 = 0, next_ticket = 0;
   bool launched = false;
   double budget = 0.0, inflight = 0.0;
   unsigned long long idle_ns = 0;
@@ -970,8 +1052,10 @@ struct rwig_server {
     double *hf = nullptr, *hg = nullptr, *hP = nullptr;
     int M = 0, N = 0;
     bool collected = true;
+    cudaEvent_t ev = nullptr;  // the slot's copies have landed
   };
   std::vector<Slot> slots;
+  std::vector<rwig::batch::Prob> staged;  // host copies of the descriptors (asynchronous copy sources)
 };
 
 namespace rwig {
@@ -992,13 +1076,29 @@ int ensure_running(rwig_server* s) {
   RWIG_CUDA_TRY(cudaMemcpy(&err, s->dctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (err) return set_error(RWIG_E_TIMEOUT, "a bounded wait in the serving kernel expired");
   bool pending = false;
-  for (int i = 0; i < s->nslots; ++i)
+  for (int i = 0; i < s->npub; ++i)
     if (!s->hdone[i]) pending = true;
   if (!pending) return 0;
   const int rc = launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns);
   if (rc) return rc;
   s->launched = true;
   return 0;
+}
+
+// Publishes, in slot order, the submitted requests whose copies have landed.
+int publish_ready(rwig_server* s) {
+  const int before = s->npub;
+  while (s->npub < s->nslots) {
+    const cudaError_t e = cudaEventQuery(s->slots[s->npub].ev);
+    if (e == cudaErrorNotReady) break;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+    ++s->npub;
+  }
+  if (s->npub != before) {
+    std::atomic_thread_fence(std::memory_order_seq_cst);  // descriptors and buffers before the count
+    *(volatile unsigned*)s->hpub = (unsigned)s->npub;
+  }
+  return ensure_running(s);
 }
 
 }  // namespace
@@ -1018,6 +1118,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   s->budget = mem_budget_bytes;
   s->idle_ns = (unsigned long long)(std::max(0.0, idle_ms) * 1e6);
   s->slots.resize(batch::kMaxProbs);
+  s->staged.resize(batch::kMaxProbs);
   auto fail = [&](cudaError_t e, const char* what) {
     rwig_server_destroy(s);
     return cuda_fail(e, what);
@@ -1036,6 +1137,8 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaHostGetDevicePointer(&s->ddone, s->hdone, 0)) != cudaSuccess) return fail(e, "done map");
   if ((e = cudaHostGetDevicePointer(&s->dres, s->hres, 0)) != cudaSuccess) return fail(e, "results map");
   if ((e = cudaMemset(s->dctl, 0, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  for (auto& sl : s->slots)
+    if ((e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "events");
   s->hpub[0] = 0;
   s->hpub[1] = 0;
   std::memset(s->hdone, 0, sizeof(unsigned) * batch::kMaxProbs);
@@ -1046,7 +1149,8 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
 extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   reset_report();
   if (!s || !q) return set_error(RWIG_E_INVALID, "null server or problem");
-  if (!q->a || !q->b || !q->C || !q->f || !q->g || q->M < 1 || q->N < 1 || !(q->reg > 0.0) ||
+  const bool pts = !q->C && q->X && q->Y && q->d >= 1;
+  if (!q->a || !q->b || !(q->C || pts) || !q->f || !q->g || q->M < 1 || q->N < 1 || !(q->reg > 0.0) ||
       !std::isfinite(q->reg) || q->max_iter < 1)
     return set_error(RWIG_E_INVALID, "bad problem");
   if (q->M > batch::kMaxRows) return set_error(RWIG_E_UNSUPPORTED, "M above 8192");
@@ -1058,6 +1162,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
     for (int i = 0; i < s->nslots; ++i) all = all && s->slots[i].collected;
     if (!all || kernel_running(s)) return RWIG_E_BUSY;
     s->nslots = 0;
+    s->npub = 0;
     std::memset(s->hdone, 0, sizeof(unsigned) * kMaxProbs);
     std::atomic_thread_fence(std::memory_order_seq_cst);
     *(volatile unsigned*)s->hpub = 0u;
@@ -1068,7 +1173,8 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   place(*q, s->ctx->sm_count, ptr, unit0, d, kd, wd);
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   const long long M = q->M, N = q->N;
-  const long long io = al(M) + al(N) + al(M * N) + al(M) + al(N) + (q->P ? al(M * N) : 0);
+  const long long cd = pts ? al(M * q->d) + al(N * q->d) : al(M * N);  // C, or the points
+  const long long io = al(M) + al(N) + cd + al(M) + al(N) + (q->P ? al(M * N) : 0);
   const double bytes = 8.0 * (double)(io + kd + wd);
   if (s->inflight + bytes > s->budget) return RWIG_E_BUSY;
   void* mem = nullptr;
@@ -1077,24 +1183,34 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   double* da = base;
   double* db = da + al(M);
   double* dC = db + al(N);
-  double* df = dC + al(M * N);
+  double* df = dC + cd;
   double* dg = df + al(M);
   double* dP = q->P ? dg + al(N) : nullptr;
   double* dk = base + io;
   double* dw = dk + kd;
   RWIG_CUDA_TRY(cudaMemcpyAsync(da, q->a, sizeof(double) * M, cudaMemcpyHostToDevice, s->cs));
   RWIG_CUDA_TRY(cudaMemcpyAsync(db, q->b, sizeof(double) * N, cudaMemcpyHostToDevice, s->cs));
-  RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q->C, sizeof(double) * M * N, cudaMemcpyHostToDevice, s->cs));
   const int slot = s->nslots;
+  if (pts) {
+    RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q->X, sizeof(double) * M * q->d, cudaMemcpyHostToDevice, s->cs));
+    RWIG_CUDA_TRY(
+        cudaMemcpyAsync(dC + al(M * q->d), q->Y, sizeof(double) * N * q->d, cudaMemcpyHostToDevice, s->cs));
+    d.X = dC;
+    d.Y = dC + al(M * q->d);
+    d.C = nullptr;
+  } else {
+    RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q->C, sizeof(double) * M * N, cudaMemcpyHostToDevice, s->cs));
+    d.C = dC;
+  }
   d.a = da;
   d.b = db;
-  d.C = dC;
   d.f = df;
   d.g = dg;
   d.P = dP;
   bind(d, dk, dw, s->dres + 10 * (size_t)slot);
-  RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &d, sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
-  RWIG_CUDA_TRY(cudaStreamSynchronize(s->cs));
+  s->staged[slot] = d;  // the copy source must outlive the asynchronous copy
+  RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &s->staged[slot], sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
+  RWIG_CUDA_TRY(cudaEventRecord(s->slots[slot].ev, s->cs));
   s->ptr = ptr;
   s->unit0 = unit0;
   auto& sl = s->slots[slot];
@@ -1113,9 +1229,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   s->inflight += bytes;
   s->hdone[slot] = 0u;
   s->nslots = slot + 1;
-  std::atomic_thread_fence(std::memory_order_seq_cst);  // descriptor and buffers before the count
-  *(volatile unsigned*)s->hpub = (unsigned)s->nslots;
-  const int rc = ensure_running(s);
+  const int rc = publish_ready(s);
   if (rc) return rc;
   return sl.ticket;
 }
@@ -1128,8 +1242,8 @@ extern "C" int rwig_server_poll(rwig_server* s, int ticket, rwig_result* out) {
   for (int i = 0; i < s->nslots; ++i)
     if (s->slots[i].ticket == ticket && !s->slots[i].collected) slot = i;
   if (slot < 0) return set_error(RWIG_E_INVALID, "unknown or already collected ticket");
-  if (!*(volatile unsigned*)(s->hdone + slot)) {
-    const int rc = ensure_running(s);  // a kernel that went idle before this request was seen
+  if (slot >= s->npub || !*(volatile unsigned*)(s->hdone + slot)) {
+    const int rc = publish_ready(s);  // and restart a kernel that went idle before seeing it
     return rc ? rc : 0;
   }
   std::atomic_thread_fence(std::memory_order_seq_cst);
@@ -1176,6 +1290,8 @@ extern "C" int rwig_server_destroy(rwig_server* s) {
     if (s->hpub) cudaFreeHost(s->hpub);
     if (s->hdone) cudaFreeHost(s->hdone);
     if (s->hres) cudaFreeHost(s->hres);
+    for (auto& sl : s->slots)
+      if (sl.ev) cudaEventDestroy(sl.ev);
     if (s->ks) cudaStreamDestroy(s->ks);
     if (s->cs) cudaStreamDestroy(s->cs);
   }

@@ -84,3 +84,29 @@ def test_memory_budget_and_idle_restart():
         t2 = _submit(srv, q)
         r2 = _wait(srv, [t2])[0]
     assert np.array_equal(r1["f"], r2["f"]) and r1["iter"] == r2["iter"]
+
+
+def test_cost_from_points_matches_host_cost():
+    """Requests given as point clouds (cost built on the device) give the same
+    bits as the same requests given the host-built cost matrix."""
+    cases = [(300, 200, 0.05, 2), (1000, 700, 0.01, 64), (64, 3000, 0.1, 3)]
+    with_c, with_pts = [], []
+    for i, (m, n, reg, dim) in enumerate(cases):
+        x = synth.rng(synth.SEED_X, 900 + i).random((m, dim))
+        y = synth.rng(synth.SEED_Y, 900 + i).random((n, dim))
+        a = synth.dirichlet(synth.rng(synth.SEED_A, 900 + i), 1.0, m)
+        b = synth.dirichlet(synth.rng(synth.SEED_B, 900 + i), 1.0, n)
+        with_c.append({"a": a, "b": b, "C": synth.sq_euclid_cost(x, y), "reg": reg, "max_iter": 2000,
+                       "zero_tol": 1e-9})
+        with_pts.append({"a": a, "b": b, "x": x, "y": y, "reg": reg, "max_iter": 2000, "zero_tol": 1e-9})
+    rc = rw.batch_sinkhorn_log(with_c, with_plan=True)
+    rp = rw.batch_sinkhorn_log(with_pts, with_plan=True)
+    for u, v in zip(rc, rp):
+        for k in ("f", "g", "P"):
+            assert np.array_equal(u[k], v[k]), k
+        assert u["loss"] == v["loss"] and u["iter"] == v["iter"]
+    with rw.Server(idle_ms=2.0) as srv:
+        tickets = [srv.submit(q["a"], q["b"], None, q["reg"], 2000, 1e-9, x=q["x"], y=q["y"]) for q in with_pts]
+        got = _wait(srv, tickets)
+    for u, v in zip(rc, got):
+        assert np.array_equal(u["f"], v["f"]) and u["iter"] == v["iter"]
