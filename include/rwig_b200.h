@@ -82,6 +82,10 @@ RWIG_API int rwig_set_option(const char* name, double value);
  * (src/sinkhorn_impl_vanilla.cpp:18): zero masses dropped, `err >= zero_tol`
  * continues, u, v zero off the support.  a: M, b: N, C: M x N.  Outputs (any
  * may be NULL): P (M x N), grad_a (M, needs withgrad), u (M), v (N), loss.
+ * grad_a is the unrolled backward Sinkhorn::_bwd_vanilla (:169-213), zero off
+ * the support; it needs at most 4096 non-zero entries of a and keeps every
+ * iteration's scalings on the device (8 (max_iter + 2)(M + N) bytes, at most
+ * 32 GiB), else RWIG_E_UNSUPPORTED.
  */
 RWIG_API int rwig_sinkhorn_vanilla(double* P, double* grad_a, double* u, double* v, double* loss,
                                    int* iter, double* err, const double* a, const double* b,
@@ -100,6 +104,9 @@ RWIG_API int rwig_sinkhorn_vanilla_dev(double* P, double* grad_a, double* u, dou
  * GPU entry for it (inst/include/cuda_interface.cuh:41, "TODO").
  * a: M, b: N, C: M x N.  Outputs (any may be NULL): P (M x N), grad_a (M,
  * needs withgrad), f (M), g (N; -inf off the support, as :267-270), loss.
+ * grad_a is the unrolled backward Sinkhorn::_bwd_log (:379-520), zero off the
+ * support; the forward of a gradient call runs every iteration in the log
+ * domain, with the limits of rwig_sinkhorn_vanilla's gradient.
  */
 RWIG_API int rwig_sinkhorn_log(double* P, double* grad_a, double* f, double* g, double* loss,
                       int* iter, double* err, const double* a, const double* b,

@@ -84,6 +84,10 @@ struct Params {
   double err0;
   double* f_state;
   double* g_state;
+  // optional history for the gradient: f_l at fh[l * m] (l = 1..L+1, the f
+  // computed at the end of iteration l - 1) and g_l at gh[l * n] (l = 1..L)
+  double* fh;
+  double* gh;
 };
 
 // Dynamic shared memory of one CTA: stage ring, mbarriers, reduction scratch,
@@ -163,6 +167,7 @@ __global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
   double* fcur = p.f0;
   double* fnext = p.f1;
   unsigned robust_seen = 0;
+  int hist = 1;  // history row the next row merge writes (iteration + 1)
 
   // ---------------------------------------------------------------- helpers
   auto load_f = [&](const double* src, double scale) {
@@ -270,7 +275,9 @@ __global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
         const double la = p.loga[i], ela = p.eloga[i], fc = __ldcg(fcur + i);
         const double d = -Rrow * inv_eps - la;
         errr += d * d;
-        fnext[i] = fc + (ela + Rrow);
+        const double fn = fc + (ela + Rrow);
+        fnext[i] = fn;
+        if (p.fh) p.fh[(size_t)hist * m + i] = fn;
       }
       __syncthreads();
     }
@@ -430,6 +437,7 @@ __global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
         const double gn = gj + (celogb[c] + rmin);
         cg[c] = gn;
         cmu[c] = sm;
+        if (p.gh) p.gh[(size_t)iter * p.n + ring.c0 + c] = gn;
         const double d = -(eps * sm - gn) * inv_eps - clogb[c];
         errc += d * d;
       }
@@ -439,6 +447,7 @@ __global__ void __launch_bounds__(NTT, 1) sinkhorn_log_kernel(Params p) {
       if (lane == 0) p.part[(size_t)cta * 8 + 1] = errc;
     }
     if (!gsync()) { ok = false; break; }
+    hist = iter + 1;
     row_merge(false);
     if (!gsync()) { ok = false; break; }
     const unsigned rob = *(volatile unsigned*)(p.ctrl + 3);
@@ -692,8 +701,11 @@ inline int dispatch_launch(Context* ctx, Params& p, cudaStream_t st, int* launch
 enum {
   SL_LOGA = 0, SL_ELOGA, SL_LOGB, SL_ELOGB, SL_F0, SL_F1, SL_G, SL_MU, SL_ROWP, SL_ROWPM, SL_PART,
   SL_CTRL, SL_RES, SL_CRED, SL_AR, SL_BR, SL_RIDX, SL_CIDX, SL_HOST_C, SL_HOST_A, SL_HOST_B,
-  SL_HOST_P, SL_HOST_F, SL_HOST_G, SL_FST, SL_GST, SL_FT, SL_GT, SL_KT, SL_U0, SL_U1
+  SL_HOST_P, SL_HOST_F, SL_HOST_G, SL_FST, SL_GST, SL_FT, SL_GT, SL_KT, SL_U0, SL_U1, SL_FH, SL_GH
 };
+
+// Largest forward history kept for the gradient (f and g of every iteration).
+constexpr size_t kMaxHistoryBytes = size_t(32) << 30;
 
 // Core of both log-Sinkhorn entry points: inputs on the device.
 __global__ void scatter_kernel(const double* x, const int* idx, int n, double* out) {
@@ -713,8 +725,8 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   if (!a || !b || !C) return set_error(RWIG_E_INVALID, "a, b and C must be non-null");
   if (M < 1 || N < 1) return set_error(RWIG_E_INVALID, "M and N must be >= 1");
   if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
-  if (withgrad && grad_a)
-    return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient is not available in this build");
+  const bool want_grad = withgrad && grad_a;
+  if (want_grad && max_iter < 0) return set_error(RWIG_E_INVALID, "max_iter must be >= 0");
   int launches = 0;
 
   // support reduction (src/sinkhorn_impl_log.cpp:238-249): drop zero masses
@@ -805,6 +817,24 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   p.G = Gmax;
   p.do_final = 1;
 
+  // gradient: every iteration's potentials (log) or scalings (vanilla), rows
+  // 1..max_iter+1 of f / u and 1..max_iter of g / v
+  double* fh = nullptr;
+  double* gh = nullptr;
+  if (want_grad) {
+    if (m > 4096) return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient supports up to 4096 rows of support");
+    const size_t hb_f = sizeof(double) * ((size_t)max_iter + 2) * m, hb_g = sizeof(double) * ((size_t)max_iter + 1) * n;
+    if (hb_f + hb_g > kMaxHistoryBytes)
+      return set_error(RWIG_E_UNSUPPORTED, "the gradient's iteration history (max_iter x (M + N)) exceeds 32 GiB");
+    fh = (double*)scratch(ctx, SL_FH, hb_f);
+    gh = (double*)scratch(ctx, SL_GH, hb_g);
+    if (!fh || !gh) return RWIG_E_NOMEM;
+    if (!vanilla) {
+      p.fh = fh;
+      p.gh = gh;
+    }
+  }
+
   prep_kernel<<<std::max(1, (std::max(m, n) + 255) / 256), 256, 0, st>>>(
       ar, br, m, n, reg, loga, eloga, logb, elogb, p.f0, p.g, p.mu, p.ctrl);
   ++launches;
@@ -850,7 +880,8 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
 
   RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
   int rc = 0;
-  const bool scaled = option("log_sinkhorn.scaled", 1.0) != 0.0 && max_iter > 1;
+  // the gradient replays the log-domain iterations, so its forward runs there
+  const bool scaled = option("log_sinkhorn.scaled", 1.0) != 0.0 && max_iter > 1 && !want_grad;
   if (vanilla) {
     // K = exp(-C/eps) (sinkhorn_impl_vanilla.cpp:41); u = a / (K 1), then the
     // scaled sweeps; P, loss and marginals from C with f = eps log u, g = eps log v
@@ -898,6 +929,8 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
       sp.g_state = gst;
       sp.l2_hot_fraction = option("log_sinkhorn.l2_hot", 0.0);
       sp.vanilla_init = 1;
+      sp.uh = fh;
+      sp.vh = gh;
       RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
       rc = run([&]() {
         int r = launch_scaled(ctx, sp, st, true);
@@ -1044,6 +1077,13 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
       rc = run(log_launch);
       if (rc != 0) return rc;
     }
+  }
+  if (want_grad) {
+    // vanilla: K = exp(-C/eps) is the kernel the scalings were computed on
+    const double* Kv = vanilla ? (const double*)scratch(ctx, SL_KT, sizeof(double) * ldc * n) : nullptr;
+    rc = sinkhorn_grad(ctx, st, vanilla, Cr, Kv, ldc, ar, br, loga, logb, fh, gh, m, n, (int)res[0], reg, d_ridx, M,
+                       vanilla ? 1.0 : reg, grad_a, &launches);
+    if (rc != 0) return rc;
   }
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   RWIG_CUDA_TRY(cudaEventSynchronize(ctx->ev1));

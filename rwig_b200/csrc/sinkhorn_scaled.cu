@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
         cvp[jl] = cv[jl];
         cv[jl] = v_l;
         csum[jl] = mine_s;
+        if (VAN && p.vh && !init) p.vh[(size_t)iter * p.n + jb + lane] = v_l;
       }
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
@@ -212,6 +213,7 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
           const double ui = __ldcg(ucur + i);
           const double un = p.a[i] / tot;
           unext[i] = un;
+          if (VAN && p.uh) p.uh[(size_t)(iter + 1) * m + i] = un;
           if (VAN) {
             const double d = ui * tot - p.a[i];
             errr += d * d;

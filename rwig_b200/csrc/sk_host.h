@@ -34,6 +34,10 @@ struct ScaledParams {
   int ncol_max;
   double l2_hot_fraction;  // share of each CTA's column groups kept in L2 (evict_last); < 0: no hint
   int vanilla_init;         // vanilla mode: start with the pass u = a / (K 1)
+  // vanilla mode, optional: the scalings of every iteration for the gradient,
+  // u_l at uh[l * m] (l = 1..L+1) and v_l at vh[l * n] (l = 1..L)
+  double* uh;
+  double* vh;
 };
 
 int launch_scaled(Context* ctx, ScaledParams& p, cudaStream_t st, bool vanilla);
@@ -46,6 +50,13 @@ int launch_fill_ones(Context* ctx, double* x, int n, cudaStream_t st);
 // The per-call Sinkhorn driver (sinkhorn_log.cu) on device inputs: vanilla
 // (f, g receive u, v) or log-stabilised (f, g the potentials).  Returns the
 // reference status (0, 1, 2) or a negative engine error; fills report().
+// Unrolled gradient of the Sinkhorn loss w.r.t. a from the forward's history
+// (sinkhorn_grad.cu); grad_a has M entries, zero off the support rows ridx.
+int sinkhorn_grad(Context* ctx, cudaStream_t st, bool vanilla, const double* C, const double* K, long long ldc,
+                  const double* a, const double* b, const double* loga, const double* logb, const double* fh,
+                  const double* gh, int m, int n, int L, double eps, const int* ridx, int M, double out_scale,
+                  double* grad_a, int* launches);
+
 int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, double* grad_a, double* f, double* g,
                     double* loss, int* iter, double* err, const double* a, const double* b, const double* C,
                     int M, int N, double reg, int withgrad, int max_iter, double zero_tol);
