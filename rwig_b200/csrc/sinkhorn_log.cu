@@ -701,7 +701,7 @@ inline int dispatch_launch(Context* ctx, Params& p, cudaStream_t st, int* launch
 enum {
   SL_LOGA = 0, SL_ELOGA, SL_LOGB, SL_ELOGB, SL_F0, SL_F1, SL_G, SL_MU, SL_ROWP, SL_ROWPM, SL_PART,
   SL_CTRL, SL_RES, SL_CRED, SL_AR, SL_BR, SL_RIDX, SL_CIDX, SL_HOST_C, SL_HOST_A, SL_HOST_B,
-  SL_HOST_P, SL_HOST_F, SL_HOST_G, SL_FST, SL_GST, SL_FT, SL_GT, SL_KT, SL_U0, SL_U1, SL_FH, SL_GH
+  SL_HOST_P, SL_HOST_F, SL_HOST_G, SL_FST, SL_GST, SL_FT, SL_GT, SL_KT, SL_U0, SL_U1, SL_FH, SL_GH, SL_HOST_GA
 };
 
 // Largest forward history kept for the gradient (f and g of every iteration).
@@ -1158,13 +1158,16 @@ static int sinkhorn_host(bool vanilla, double* P, double* grad_a, double* f, dou
   double* dP = P ? (double*)scratch(ctx, SL_HOST_P, sizeof(double) * MN) : nullptr;
   double* df = f ? (double*)scratch(ctx, SL_HOST_F, sizeof(double) * M) : nullptr;
   double* dg = g ? (double*)scratch(ctx, SL_HOST_G, sizeof(double) * N) : nullptr;
-  if (!dC || !da || !db || (P && !dP) || (f && !df) || (g && !dg)) return RWIG_E_NOMEM;
+  const bool want_grad = withgrad && grad_a;
+  double* dga = want_grad ? (double*)scratch(ctx, SL_HOST_GA, sizeof(double) * M) : nullptr;
+  if (!dC || !da || !db || (P && !dP) || (f && !df) || (g && !dg) || (want_grad && !dga)) return RWIG_E_NOMEM;
   RWIG_CUDA_TRY(cudaMemcpyAsync(dC, C, sizeof(double) * MN, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(da, a, sizeof(double) * M, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-  int rc = sinkhorn_device(ctx, st, vanilla, dP, grad_a, df, dg, loss, iter, err, da, db, dC, M, N, reg,
+  int rc = sinkhorn_device(ctx, st, vanilla, dP, dga, df, dg, loss, iter, err, da, db, dC, M, N, reg,
                            withgrad, max_iter, zero_tol);
   if (rc < 0) return rc;
+  if (want_grad) RWIG_CUDA_TRY(cudaMemcpyAsync(grad_a, dga, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
   if (P) RWIG_CUDA_TRY(cudaMemcpyAsync(P, dP, sizeof(double) * MN, cudaMemcpyDeviceToHost, st));
   if (f) RWIG_CUDA_TRY(cudaMemcpyAsync(f, df, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
   if (g) RWIG_CUDA_TRY(cudaMemcpyAsync(g, dg, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
