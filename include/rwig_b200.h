@@ -71,8 +71,22 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "log_sinkhorn.l2_hot": share of each CTA's column groups of the scaled
  *       kernel copied with an L2 evict_last hint, the rest evict_first
  *       (default 0: all evict_first; negative: no hint);
- *   "batch.profile": 1 prints the per-phase device time of every batched
- *       Sinkhorn launch (CTA 0) to stderr (default 0). */
+ *   "batch.profile": 1 prints each batched Sinkhorn launch's busy, team-wait
+ *       and claim time per CTA to stderr (default 0);
+ *   "batch.strip_kb": target K strip per team member of a batched problem,
+ *       at most 184 (default); strips up to that stay in shared memory;
+ *   "batch.max_team": largest team of CTAs per batched problem (default:
+ *       the SM count);
+ *   "batch.redundant_rows": teams with gp * M up to this (and M <= 4096)
+ *       merge row sums redundantly in every member, one team barrier per
+ *       iteration (default 16384);
+ *   "batch.l2_keep_mb": streamed problems whose K is at most this many MB
+ *       read it with an L2 evict_last hint (default 48);
+ *   "batch.max_elems": problems with more elements go through the per-call
+ *       path (default 2^26).
+ * The batch.* options change team shapes and therefore the summation order
+ * of a batched result (within rounding); a result is the same alone and in
+ * any mix under the same options. */
 RWIG_API int rwig_set_option(const char* name, double value);
 
 /* ---- vanilla Sinkhorn --------------------------------------------------

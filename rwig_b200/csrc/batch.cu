@@ -1,5 +1,5 @@
 // batch.cu -- many log-stabilised Sinkhorn problems of different sizes in one
-// cooperative launch, iterated in lockstep.
+// persistent launch, each solved by its own team of CTAs.
 //
 // Every problem has the semantics of rwig_sinkhorn_log (Sinkhorn::compute_log,
 // src/sinkhorn_impl_log.cpp:225-295), solved in stabilised scaling form with
@@ -11,24 +11,35 @@
 //   final:     f = eps log u, g = eps log v, P = exp(-((C - f) - g)/eps),
 //              loss = sum C o P + eps sum P o (log P - 1) (:266-277), marginals.
 //
-// Work split.  Problem p owns a team of gp consecutive CTAs, gp = min(G, n_p,
-// ceil(bytes of K_p / 128 KB)) -- a function of the problem alone
-// (offset off_p, wrapping); team member k holds the column strip
-// [k n/gp, (k+1) n/gp) of K_p with every row, so its column sums are complete
-// in the CTA and its row partials go to rowp_p[k].  Rows are merged in units
-// of 64 spread over the whole grid (lanes split the team's partials).  One iteration of the launch is
-//   column pass over all my strips of the running problems (one bulk-copy
-//   ring across problems) | grid barrier | row merge of my units | grid
-//   barrier | every CTA takes the same continue / stop decision for every
-//   problem.
-// The column split, the merge order (team members 0..gp-1) and the error sums
-// depend only on the problem, so a result is bitwise the same whatever else
+// Scheduling.  The grid is one CTA per SM.  Problem p is solved by a team of
+// gp CTAs (gp a function of the problem alone); a free CTA claims the next
+// member slot of the oldest problem whose team is not yet complete (one
+// atomic counter per problem), so teams form in problem order and at most one
+// team is incomplete at any time: its members wait only for CTAs that are
+// finishing other problems, never for each other in a cycle.  A team
+// synchronises through its own counter in global memory; nothing waits on the
+// whole grid.
+//
+// Work split.  Member k holds the column strip [k n/gp, (k+1) n/gp) of K with
+// every row, so its column sums are complete inside the CTA.
+//  * resident strips (<= 184 KB): K is built straight into shared memory by
+//    the first pass and stays there, so an iteration reads no K from memory;
+//  * streamed strips (larger problems): K is built in global memory and
+//    streamed through a bulk-copy ring every iteration (kept in L2 when it fits).
+// Rows with m <= 512 are processed warp per column (lanes own rows, a warp
+// reduction per column); larger m thread per row (a block reduction per
+// group of columns).  Row sums of the members are merged in a fixed order
+// either redundantly by every member (small teams: one team barrier per
+// iteration) or split over the members (two barriers).  Every reduction order
+// depends only on the problem, so a result is bitwise the same whatever else
 // is in the batch.  A problem whose scalings leave [e^-650, e^650], whose
 // masses are not all positive or whose sums leave the safe range is handed
 // back (status kUnsafe) and re-solved by the per-call path.
 //
-// Every wait is bounded (2 s); on expiry the kernel sets an error word and
-// returns, and the host reports RWIG_E_TIMEOUT.
+// Every wait is bounded: team barriers after 2 s, and a member waiting for its
+// team to form as long as other teams progress (2 s without progress ends it);
+// on expiry the kernel sets an error word, drains its copies and returns, and
+// the host reports RWIG_E_TIMEOUT.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -49,15 +60,23 @@ using sk::block_sum_cols;
 using sk::STAGES;
 
 constexpr int NTT = 512, NW = NTT / 32;
-constexpr int kSlot = 8192;   // doubles per ring stage (CW x 512 RPT = 8192 for every row class)
+constexpr int kSlot = 8192;                // doubles per streamed stage (64 KB: CW x 512 RPT for every row class)
+constexpr int kArea = 27648;               // doubles of the strip area (216 KB): stage ring or resident strip
+constexpr int kTree = 4096;                // doubles at the end of the area for the warp-mode row tree
+constexpr int kResident = kArea - kTree;   // largest resident strip (184 KB)
+constexpr int kWarpRows = 512;             // m <= this: warp-per-column passes
 constexpr int kMaxRows = 8192;
-constexpr int kUnit = 64;     // rows per merge unit (4 per warp)
+constexpr int kUnit = 64;                  // rows per merge unit (4 per warp)
 constexpr int kMaxProbs = 512;
-constexpr int kMaxTeam = 160;       // CTAs of a team (the grid is one CTA per SM)
-constexpr long long kStripBytes = 128 << 10;  // target bytes of K per team member
+constexpr int kMaxTeam = 160;              // CTAs of a team (the grid is one CTA per SM)
 constexpr double kScaleMin = 5.1e-283, kScaleMax = 1.95e282;  // e^-650, e^650
-enum { ST_RUN = 0, ST_FIN = 1, ST_RETIRED = 2 };
 constexpr double kUnsafeStatus = -100.0;
+constexpr unsigned kClosed = 0x80000000u;
+
+enum : int { MODE_RESIDENT = 1, MODE_WARP = 2, MODE_REDUNDANT = 4, MODE_KEEP_L2 = 8 };
+
+// Device control words of a launch.
+enum : int { DC_AVAIL = 0, DC_HEAD = 1, DC_ERR = 2, DC_PROGRESS = 3, DC_ACTIVE = 4 };
 
 struct Prob {
   const double* a;
@@ -66,199 +85,333 @@ struct Prob {
   const double* X;   // m x d source points (column-major) or null
   const double* Y;   // n x d target points or null
   int d;
-  double* K;         // m x n, leading dimension ldk (even), 16-byte aligned
-  long long ldk;
+  double* K;         // streamed strips: m x n, leading dimension ldk
+  long long ldk;     // even, >= m
   double* P;         // optional plan (leading dimension m)
   double* f;         // m
   double* g;         // n; holds v during the iterations
-  double* u0;        // u ping-pong (m each)
-  double* u1;
-  double* rowp;      // [gp][m] row partials
-  double* colp;      // [gp][4] column-strip partials
-  double* unitp;     // [nunits][4] merge-unit partials
-  double* res;       // [10]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, -, -
-  int m, n, max_iter, cls, gp, off, nunits, unit0;
+  double* rowp;      // [2][gp][m] row partials (by round parity)
+  double* colp;      // [2][gp][4] column-strip partials
+  double* mrgp;      // [2][gp][4] merge partials (split merges)
+  double* ug;        // [2][m] u (split merges)
+  unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals
+  double* res;       // [10]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, -
+  int m, n, max_iter, gp, mode, nunits;
   double eps, tol;
 };
 
-struct State {  // per problem, identical in every CTA
-  int st, iter, par, init;  // init: 2 cost from points pending, 1 first pass pending, 0 iterating
-  double err, cmax;
+struct Shared {
+  double* area;      // kArea doubles
+  uint64_t* bar;     // STAGES mbarriers
+  double* su;        // kWarpRows doubles: u in warp mode
+  double* red;       // 2 * NW * 16 doubles: block reductions
+  double* dec;       // 8 doubles: values broadcast to the CTA
+  int* flag;         // 4 ints
 };
 
+// dynamic shared memory of one CTA
 __host__ __device__ constexpr size_t smem_bytes() {
-  return (size_t)STAGES * kSlot * 8 + 64 + (size_t)2 * NW * 16 * 8 + (size_t)kMaxProbs * sizeof(State) + 256;
+  return (size_t)kArea * 8 + 64 + (size_t)kWarpRows * 8 + (size_t)2 * NW * 16 * 8 + 8 * 8 + 4 * 4 + sizeof(Prob) +
+         64;
 }
 
-__device__ __forceinline__ int class_cw(int cls) { return cls == 0 ? 16 : cls == 1 ? 8 : cls == 2 ? 4 : cls == 3 ? 2 : 1; }
+__device__ __forceinline__ int strip_begin(int n, int gp, int k) { return (int)(((long long)k * n) / gp); }
 
-// Team membership of this CTA in problem p: index k, or -1.
-__device__ __forceinline__ int team_index(const Prob& p, int cta, int G) {
-  const int k = (cta - p.off + G) % G;
-  return k < p.gp ? k : -1;
-}
-__device__ __forceinline__ int strip_begin(const Prob& p, int k) { return (int)(((long long)k * p.n) / p.gp); }
-
-// Column groups of this CTA across the running problems, in problem order:
-// the consumer and the issuer walk the same sequence.
-struct Cursor {
-  int p;   // problem index (np: exhausted; -1: before the first)
-  int jb;  // first column of the current group
-};
-
-__device__ __forceinline__ void next_group(Cursor& c, const Prob* probs, const State* S, int np, int cta, int G) {
-  if (c.p >= 0 && c.p < np) {
-    const Prob& p = probs[c.p];
-    const int k = team_index(p, cta, G);
-    c.jb += class_cw(p.cls);
-    if (c.jb < strip_begin(p, k + 1)) return;
+// Waits until the team counter reaches target (thread 0).  A forming team
+// waits as long as some other team makes progress; a formed team 2 s at most.
+__device__ bool team_wait(unsigned* cnt, unsigned target, unsigned* dctl, bool forming) {
+  __threadfence();
+  asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+  unsigned long long t0 = 0;
+  unsigned p0 = 0;
+  for (unsigned spin = 0;; ++spin) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+    if ((int)(v - target) >= 0) return true;
+    if ((spin & 63u) == 0u) {
+      if (*(volatile unsigned*)(dctl + DC_ERR) != 0u) return false;
+      const unsigned long long now = globaltimer_ns();
+      if (forming) {
+        const unsigned pv = *(volatile unsigned*)(dctl + DC_PROGRESS);
+        if (t0 == 0 || pv != p0) {
+          p0 = pv;
+          t0 = now;
+        }
+      } else if (t0 == 0) {
+        t0 = now;
+      }
+      if (now - t0 > kWaitLimitNs) {
+        atomicOr(dctl + DC_ERR, KERR_BARRIER_TIMEOUT);
+        return false;
+      }
+    }
   }
-  for (int q = c.p + 1; q < np; ++q) {
-    if (S[q].st != ST_RUN || S[q].init) continue;
-    const Prob& p = probs[q];
-    const int k = team_index(p, cta, G);
-    if (k < 0) continue;
-    c.p = q;
-    c.jb = strip_begin(p, k);
-    return;
-  }
-  c.p = np;
-  c.jb = 0;
 }
 
+// Team barrier (all threads).  Single-member teams need only the block barrier.
+__device__ __forceinline__ bool team_sync(const Prob& p, unsigned& nb, bool forming, unsigned* dctl, const Shared& sh,
+                                          double* prof_wait) {
+  __syncthreads();
+  if (p.gp == 1) return true;
+  ++nb;
+  if (threadIdx.x == 0) {
+    const unsigned long long t = prof_wait ? globaltimer_ns() : 0ull;
+    sh.flag[0] = team_wait(p.ctl + 1, nb * (unsigned)p.gp, dctl, forming) ? 1 : 0;
+    if (prof_wait) *prof_wait += (double)(globaltimer_ns() - t);
+  }
+  __syncthreads();
+  return sh.flag[0] != 0;
+}
+
+// ---------------------------------------------------------------- stage ring
+// Streamed strips: the strip's column groups cycle through STAGES shared
+// buffers; the q-th consumed stage (q counts across problems, so the mbarrier
+// phases stay consistent) holds group (q - q0) mod ngroups.  Thread 0 issues.
 struct Ring {
   double* buf;
   uint64_t* bar;
-  uint64_t pol;  // L2 evict_first: K is streamed once per iteration
+  uint64_t pol;
+  const double* K;
+  long long ldk;
+  int c0, c1, cw, ngroups;
+  unsigned q0;
   __device__ double* slot(unsigned seq) const { return buf + (size_t)(seq % STAGES) * kSlot; }
-  // thread 0: copy the group starting at column jb of problem p (strip end c1) into stage seq
-  __device__ void issue(unsigned seq, const Prob& p, int jb, int c1) const {
-    const unsigned bytes = (unsigned)(min(class_cw(p.cls), c1 - jb) * p.ldk * 8);
+  __device__ int group_begin(unsigned seq) const { return c0 + (int)((seq - q0) % (unsigned)ngroups) * cw; }
+  __device__ void issue(unsigned seq) const {
+    const int jb = group_begin(seq);
+    const unsigned bytes = (unsigned)(min(cw, c1 - jb) * ldk * 8);
     uint64_t* b = bar + (seq % STAGES);
     mbar_arrive_expect_tx(b, bytes);
-    bulk_g2s_hint(slot(seq), p.K + (size_t)jb * p.ldk, bytes, b, pol);
+    bulk_g2s_hint(slot(seq), K + (size_t)jb * ldk, bytes, b, pol);
   }
   __device__ bool wait(unsigned seq) const { return mbar_wait_bounded(bar + (seq % STAGES), (seq / STAGES) & 1u); }
 };
 
-// Thread 0 keeps up to STAGES groups in flight ahead of the consumer.
-struct Issuer {
-  Cursor c;
-  unsigned seq;
-};
-
-__device__ __forceinline__ void issue_ahead(Issuer& is, const Ring& ring, unsigned limit, const Prob* probs,
-                                            const State* S, int np, int cta, int G) {
-  while (is.seq < limit && is.c.p < np) {
-    const Prob& p = probs[is.c.p];
-    ring.issue(is.seq, p, is.c.jb, strip_begin(p, team_index(p, cta, G) + 1));
-    ++is.seq;
-    next_group(is.c, probs, S, np, cta, G);
-  }
+// ---------------------------------------------------------------- passes
+// Cost from points over this member's strip: C_ij = sum_k (x_ik - y_jk)^2 in
+// ascending k, each step rounded separately (the same operations and order as
+// a host that computes the differences, squares and sums elementwise, so the
+// same bits), stored un-normalised; the strip's maximum is returned (block max).
+__device__ double cost_pass(const Prob& p, int c0, int c1, double* red) {
+  const int m = p.m, n = p.n;
+  double mx = 0.0;
+  for (int j = c0; j < c1; ++j)
+    for (int i = threadIdx.x; i < m; i += NTT) {
+      double acc = 0.0;
+      for (int q = 0; q < p.d; ++q) {
+        const double t = __dsub_rn(p.X[i + (size_t)q * m], p.Y[j + (size_t)q * n]);
+        acc = __dadd_rn(acc, __dmul_rn(t, t));
+      }
+      const_cast<double*>(p.C)[i + (size_t)j * m] = acc;
+      mx = fmax(mx, acc);
+    }
+  mx = warp_max(mx);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  double v = 0.0;
+  for (int q = 0; q < NW; ++q) v = fmax(v, red[q]);
+  __syncthreads();
+  return v;  // exact and order-free
 }
 
-// Column pass of one problem over this CTA's strip (its groups are the next
-// ones in the ring): column sums with u, v = b / s, row partials r = K v ->
-// rowp[k], column-strip partials -> colp[k].
-// REREAD: the row update reads the stage from shared memory again instead of
-// keeping it in registers (for 16 rows per thread, which would not fit), and
-// the stage is refilled only after a block barrier that follows that read.
-template <int RPT, int CW, bool REREAD>
-__device__ bool column_pass(const Prob& p, const State& s, int k, const Ring& ring, unsigned& q, Issuer& is,
-                            const Prob* probs, const State* S, int np, int cta, int G, double* red, int& par) {
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+// First pass over the strip: K = exp(-C/eps) (sinkhorn_impl_vanilla.cpp:41
+// form) into shared memory (resident) or global memory (streamed), row
+// partials of K 1 -> rowp[0][k] (merged into u_1 = a / (K 1)), and whether a
+// mass of the strip's columns or (member 0) of the rows is not positive.
+template <int RPT>
+__device__ double init_pass(const Prob& p, int k, int c0, int c1, double cmax, double* Kres, double* red, int& par) {
+  const int tid = threadIdx.x;
   const int m = p.m;
-  const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
-  const double* ucur = s.par ? p.u1 : p.u0;
-  double u[RPT], r[RPT];
+  double r[RPT];
   bool valid[RPT];
 #pragma unroll
   for (int t = 0; t < RPT; ++t) {
     valid[t] = tid + t * NTT < m;
-    u[t] = valid[t] ? __ldcg(ucur + tid + t * NTT) : 0.0;
     r[t] = 0.0;
   }
-  double errc = 0.0, bad = 0.0;
-  for (int jb = c0; jb < c1; jb += CW) {
-    const unsigned seq = q;
-    if (!ring.wait(seq)) return false;
-    const double* buf = ring.slot(seq) + tid;
-    const int nc = min(CW, c1 - jb);
-    double kv[REREAD ? 1 : RPT][CW], sum[CW];
+  const bool res = (p.mode & MODE_RESIDENT) != 0;
+#pragma unroll 2
+  for (int j = c0; j < c1; ++j) {
+    const double* cj = p.C + (size_t)j * m;
+    double* kj = res ? Kres + (size_t)(j - c0) * p.ldk : p.K + (size_t)j * p.ldk;
 #pragma unroll
-    for (int c = 0; c < CW; ++c) {
-      sum[c] = 0.0;
-#pragma unroll
-      for (int t = 0; t < RPT; ++t) {
-        const double x = (c < nc && valid[t]) ? buf[(size_t)c * p.ldk + t * NTT] : 0.0;
-        if (!REREAD) kv[t][c] = x;
-        sum[c] = fma(x, u[t], sum[c]);
+    for (int t = 0; t < RPT; ++t)
+      if (valid[t]) {
+        double c = cj[tid + t * NTT];
+        if (p.X) {  // C /= max C
+          c = c / cmax;
+          const_cast<double*>(cj)[tid + t * NTT] = c;
+        }
+        const double x = exp(-c / p.eps);
+        kj[tid + t * NTT] = x;
+        r[t] += x;
       }
-    }
-    double v[CW];
-    {
-      block_sum_cols<CW, NW>(sum, red, par);  // (the stage is no longer read after this unless REREAD)
-      double s_l = 1.0;
-#pragma unroll
-      for (int c = 0; c < CW; ++c)
-        if (c == lane) s_l = sum[c];
-      const bool owner = lane < nc;
-      const double v_l = owner ? p.b[jb + lane] / s_l : 0.0;
-      if (w == 0 && owner) {
-        p.g[jb + lane] = v_l;
-        // log(v s) - log(b) with v = b / s is a rounding-level residual; its
-        // first-order form needs no logarithm
-        const double d = (v_l * s_l) / p.b[jb + lane] - 1.0;
-        errc += d * d;
-        if (!(v_l >= kScaleMin && v_l <= kScaleMax) || !(s_l >= 1e-300 && s_l <= 1e300)) bad = 1.0;
-      }
-#pragma unroll
-      for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);
-    }
-    if (!REREAD && tid == 0) issue_ahead(is, ring, seq + 1 + STAGES, probs, S, np, cta, G);
-    q = seq + 1;
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-      double acc = r[t];
-#pragma unroll
-      for (int c = 0; c < CW; ++c) {
-        const double x = REREAD ? ((c < nc && valid[t]) ? buf[(size_t)c * p.ldk + t * NTT] : 0.0)
-                                : kv[REREAD ? 0 : t][c];
-        acc = fma(x, v[c], acc);
-      }
-      r[t] = acc;
-    }
-    if (REREAD) {
-      __syncthreads();  // every thread is done with the stage
-      if (tid == 0) issue_ahead(is, ring, seq + 1 + STAGES, probs, S, np, cta, G);
-    }
   }
+  double bad = 0.0;
+  for (int j = c0 + tid; j < c1; j += NTT)
+    if (!(p.b[j] > 0.0)) bad = 1.0;
+  if (k == 0)
+    for (int i = tid; i < m; i += NTT)
+      if (!(p.a[i] > 0.0)) bad = 1.0;
+  if (!res) asm volatile("fence.proxy.async.global;" ::: "memory");  // K is read next by bulk copies
 #pragma unroll
   for (int t = 0; t < RPT; ++t)
     if (valid[t]) p.rowp[(size_t)k * m + tid + t * NTT] = r[t];
-  double tt[2] = {errc, bad};
-  block_sum_cols<2, NW>(tt, red, par);
-  if (tid == 0) {
-    p.colp[(size_t)k * 4 + 0] = tt[0];
-    p.colp[(size_t)k * 4 + 1] = tt[1];
-  }
-  return true;
+  double tt[1] = {bad};
+  block_sum_cols<1, NW>(tt, red, par);
+  return tt[0];
 }
 
-// Final pass over this CTA's strip: g = eps log v, P, loss and marginal partials.
+// Column pass, warp per column (m <= 32 RPL <= 512, resident strip): warp w
+// takes the strip's columns w, w + NW, ...; lanes own rows lane + 32 j.
+// Column sum with u (from su), v = b / s, row partials r += K v.  The warps'
+// row partials are added in a fixed tree; the CTA's go to rowp[buf][k].
+template <int RPL>
+__device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, int c1, const double* Ks, const Shared& sh, int& par,
+                          double& errc, double& bad) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int m = p.m;
+  const long long ldk = p.ldk;
+  double u[RPL], r[RPL];
+#pragma unroll
+  for (int j = 0; j < RPL; ++j) {
+    const int i = lane + 32 * j;
+    u[j] = i < m ? sh.su[i] : 0.0;
+    r[j] = 0.0;
+  }
+  double e = 0.0, bd = 0.0;
+  const int nc = c1 - c0;
+  auto column = [&](int c, double (&kv)[RPL], double& s) {
+    const double* col = Ks + (size_t)c * ldk;
+    s = 0.0;
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) {
+      const int i = lane + 32 * j;
+      kv[j] = i < m ? col[i] : 0.0;
+      s = fma(kv[j], u[j], s);
+    }
+  };
+  auto finish = [&](int c, const double (&kv)[RPL], double s) {
+    s = warp_sum(s);  // the same bits in every lane
+    const double bj = p.b[c0 + c];
+    const double v = bj / s;
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) r[j] = fma(kv[j], v, r[j]);
+    if (lane == 0) {
+      p.g[c0 + c] = v;
+      const double d = (v * s) / bj - 1.0;  // first-order form of log(v s) - log b
+      e += d * d;
+      if (!(v >= kScaleMin && v <= kScaleMax) || !(s >= 1e-300 && s <= 1e300)) bd = 1.0;
+    }
+  };
+  int c = w;
+  if (RPL <= 8)
+    for (; c + NW < nc; c += 2 * NW) {  // two columns in flight
+      double k1[RPL], k2[RPL], s1, s2;
+      column(c, k1, s1);
+      column(c + NW, k2, s2);
+      finish(c, k1, s1);
+      finish(c + NW, k2, s2);
+    }
+#pragma unroll 1
+  for (; c < nc; c += NW) {
+    double k1[RPL], s1;
+    column(c, k1, s1);
+    finish(c, k1, s1);
+  }
+  // fixed tree over the warps: w + h is added into w for h = 8, 4, 2, 1
+  double* tree = sh.area + kResident;
+#pragma unroll 1
+  for (int h = NW / 2; h >= 1; h >>= 1) {
+    if (w >= h && w < 2 * h)
+#pragma unroll
+      for (int j = 0; j < RPL; ++j) tree[((w - h) * RPL + j) * 32 + lane] = r[j];
+    __syncthreads();
+    if (w < h)
+#pragma unroll
+      for (int j = 0; j < RPL; ++j) r[j] += tree[(w * RPL + j) * 32 + lane];
+    __syncthreads();
+  }
+  if (w == 0)
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) {
+      const int i = lane + 32 * j;
+      if (i < m) p.rowp[((size_t)buf * p.gp + k) * m + i] = r[j];
+    }
+  double tt[2] = {e, bd};
+  block_sum_cols<2, NW>(tt, sh.red, par);
+  errc = tt[0];
+  bad = tt[1];
+}
+
+// One group of CW columns, thread per row (RPT rows per thread): column sums
+// with u, v = b / s (warp 0, lane c owns column jb + c), r += K v.  `buf`
+// points at column jb's row 0 (+ tid), leading dimension ldk.
+template <int RPT, int CW, bool REREAD>
+__device__ __forceinline__ void block_group(const Prob& p, const double* buf, int jb, int nc, const double (&u)[RPT],
+                                            double (&r)[RPT], const bool (&valid)[RPT], double* red, int& par,
+                                            double& e, double& bd, const Ring* ring, unsigned seq) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const long long ldk = p.ldk;
+  double kv[REREAD ? 1 : RPT][CW], sum[CW];
+#pragma unroll
+  for (int c = 0; c < CW; ++c) {
+    sum[c] = 0.0;
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) {
+      const double x = (c < nc && valid[t]) ? buf[(size_t)c * ldk + t * NTT] : 0.0;
+      if (!REREAD) kv[t][c] = x;
+      sum[c] = fma(x, u[t], sum[c]);
+    }
+  }
+  block_sum_cols<CW, NW>(sum, red, par);
+  double s_l = 1.0;
+#pragma unroll
+  for (int c = 0; c < CW; ++c)
+    if (c == lane) s_l = sum[c];
+  const bool owner = lane < nc;
+  const double v_l = owner ? p.b[jb + lane] / s_l : 0.0;
+  if (w == 0 && owner) {
+    p.g[jb + lane] = v_l;
+    const double d = (v_l * s_l) / p.b[jb + lane] - 1.0;  // first-order form of log(v s) - log b
+    e += d * d;
+    if (!(v_l >= kScaleMin && v_l <= kScaleMax) || !(s_l >= 1e-300 && s_l <= 1e300)) bd = 1.0;
+  }
+  double v[CW];
+#pragma unroll
+  for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);
+  // streamed, registers hold the stage: every thread has read it (block_sum_cols)
+  if (!REREAD && ring && tid == 0) ring->issue(seq + STAGES);
+#pragma unroll
+  for (int t = 0; t < RPT; ++t) {
+    double acc = r[t];
+#pragma unroll
+    for (int c = 0; c < CW; ++c) {
+      const double x = REREAD ? ((c < nc && valid[t]) ? buf[(size_t)c * ldk + t * NTT] : 0.0) : kv[REREAD ? 0 : t][c];
+      acc = fma(x, v[c], acc);
+    }
+    r[t] = acc;
+  }
+  if (REREAD && ring) {
+    __syncthreads();  // every thread is done with the stage
+    if (tid == 0) ring->issue(seq + STAGES);
+  }
+}
+
+// Final pass over the strip with u in shared memory (area): g = eps log v,
+// P, loss and column-marginal partials -> colp[buf][k], row sums -> rowp[buf][k].
 template <int RPT, int CW>
-__device__ void final_pass(const Prob& p, const State& s, int k, double* red, int& par) {
+__device__ void final_pass(const Prob& p, int k, int buf, int c0, int c1, const double* us, double* red, int& par) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int m = p.m;
   const double eps = p.eps;
-  const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
-  const double* ucur = s.par ? p.u1 : p.u0;
   double f[RPT], rs[RPT];
   bool valid[RPT];
 #pragma unroll
   for (int t = 0; t < RPT; ++t) {
     valid[t] = tid + t * NTT < m;
-    f[t] = valid[t] ? eps * log(__ldcg(ucur + tid + t * NTT)) : 0.0;
+    f[t] = valid[t] ? eps * log(us[tid + t * NTT]) : 0.0;
     rs[t] = 0.0;
   }
   double s1 = 0.0, s2 = 0.0, l1c = 0.0, l2c = 0.0;
@@ -303,100 +456,17 @@ __device__ void final_pass(const Prob& p, const State& s, int k, double* red, in
   }
 #pragma unroll
   for (int t = 0; t < RPT; ++t)
-    if (valid[t]) p.rowp[(size_t)k * m + tid + t * NTT] = rs[t];
+    if (valid[t]) p.rowp[((size_t)buf * p.gp + k) * m + tid + t * NTT] = rs[t];
   double tt[4] = {s1, s2, l1c, l2c};
   block_sum_cols<4, NW>(tt, red, par);
   if (tid == 0)
-    for (int i = 0; i < 4; ++i) p.colp[(size_t)k * 4 + i] = tt[i];
+    for (int i = 0; i < 4; ++i) p.colp[((size_t)buf * p.gp + k) * 4 + i] = tt[i];
 }
 
-// Cost from points over this CTA's strip: C_ij = sum_k (x_ik - y_jk)^2 in
-// ascending k, each step rounded separately (the same operations and order as
-// a host that computes the differences, squares and sums elementwise, so the
-// same bits), stored un-normalised; the strip's maximum -> colp[k][2].
-__device__ void cost_pass(const Prob& p, int k, double* red, int& par) {
-  const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
-  const int m = p.m, n = p.n;
-  double mx = 0.0;
-  for (int j = c0; j < c1; ++j)
-    for (int i = threadIdx.x; i < m; i += NTT) {
-      double acc = 0.0;
-      for (int q = 0; q < p.d; ++q) {
-        const double t = __dsub_rn(p.X[i + (size_t)q * m], p.Y[j + (size_t)q * n]);
-        acc = __dadd_rn(acc, __dmul_rn(t, t));
-      }
-      const_cast<double*>(p.C)[i + (size_t)j * m] = acc;
-      mx = fmax(mx, acc);
-    }
-  // block maximum (exact, order-free)
-  mx = warp_max(mx);
-  __syncthreads();  // red is free
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double v = 0.0;
-    for (int q = 0; q < NW; ++q) v = fmax(v, red[q]);
-    p.colp[(size_t)k * 4 + 2] = v;
-  }
-  __syncthreads();
-}
-
-// First pass of a problem over this CTA's strip: K = exp(-C/eps)
-// (sinkhorn_impl_vanilla.cpp:41 form) into its buffer, row partials of K 1
-// -> rowp[k] (the merge turns them into u_1 = a / (K 1)), and whether a mass
-// of the strip's columns or (member 0) of the rows is not positive -> colp[k][1].
-template <int RPT>
-__device__ void init_pass(const Prob& p, int k, double cmax, double* red, int& par) {
-  const int tid = threadIdx.x;
-  const int c0 = strip_begin(p, k), c1 = strip_begin(p, k + 1);
-  const int m = p.m;
-  double r[RPT];
-  bool valid[RPT];
-#pragma unroll
-  for (int t = 0; t < RPT; ++t) {
-    valid[t] = tid + t * NTT < m;
-    r[t] = 0.0;
-  }
-#pragma unroll 2
-  for (int j = c0; j < c1; ++j) {
-    const double* cj = p.C + (size_t)j * m;
-    double* kj = p.K + (size_t)j * p.ldk;
-#pragma unroll
-    for (int t = 0; t < RPT; ++t)
-      if (valid[t]) {
-        double c = cj[tid + t * NTT];
-        if (p.X) {  // C /= max C
-          c = c / cmax;
-          const_cast<double*>(cj)[tid + t * NTT] = c;
-        }
-        const double x = exp(-c / p.eps);
-        kj[tid + t * NTT] = x;
-        r[t] += x;
-      }
-  }
-  double bad = 0.0;
-  for (int j = c0 + tid; j < c1; j += NTT)
-    if (!(p.b[j] > 0.0)) bad = 1.0;
-  if (k == 0)
-    for (int i = tid; i < m; i += NTT)
-      if (!(p.a[i] > 0.0)) bad = 1.0;
-  asm volatile("fence.proxy.async.global;" ::: "memory");  // K is read next by bulk copies
-#pragma unroll
-  for (int t = 0; t < RPT; ++t)
-    if (valid[t]) p.rowp[(size_t)k * m + tid + t * NTT] = r[t];
-  double tt[1] = {bad};
-  block_sum_cols<1, NW>(tt, red, par);
-  if (tid == 0) {
-    p.colp[(size_t)k * 4 + 0] = 0.0;
-    p.colp[(size_t)k * 4 + 1] = tt[0];
-  }
-}
-
-// Row totals of merge unit u (rows u*64 .. u*64+63): warp w sums rows
-// 4w .. 4w+3 over the gp team partials, lane l taking members l, l+32, ...
-// in order, then a fixed butterfly across the lanes.  Lane r < 4 of the warp
-// receives the total of its row r (i = u*64 + 4w + r); rows past m give 0.
-__device__ __forceinline__ double merge_unit(const double* rowp, int gp, int m, int u) {
+// Row totals of merge unit u (rows u*64 .. u*64+63) over the team's partials
+// `rp` ([gp][m]): warp w sums rows 4w .. 4w+3, lane l taking members l, l+32,
+// ... in order, then a fixed butterfly.  Lane r < 4 receives row u*64+4w+r.
+__device__ __forceinline__ double merge_unit(const double* rp, int gp, int m, int u) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i0 = u * kUnit + 4 * w;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -405,7 +475,7 @@ __device__ __forceinline__ double merge_unit(const double* rowp, int gp, int m, 
   for (int j = 0; j < kMaxTeam / 32; ++j) {
     const int k = lane + 32 * j;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[j][r] = (k < gp && i0 + r < m) ? __ldcg(rowp + (size_t)k * m + i0 + r) : 0.0;
+    for (int r = 0; r < 4; ++r) v[j][r] = (k < gp && i0 + r < m) ? __ldcg(rp + (size_t)k * m + i0 + r) : 0.0;
   }
 #pragma unroll
   for (int j = 0; j < kMaxTeam / 32; ++j)
@@ -420,278 +490,494 @@ __device__ __forceinline__ double merge_unit(const double* rowp, int gp, int m, 
   return mine;
 }
 
-// Service loop.  probs[0, *pub) are the published problems (pub[0]: count,
-// pub[1]: stop flag; host-mapped memory for a server, device memory for a
-// batch call); done[q] is set (system scope) once problem q's results are in
-// probs[q].res.  dctl: [0] barrier count, [2] error bits, [3..5] values CTA 0
-// broadcasts to the grid each iteration.  The launch ends when no problem
-// runs and either the stop flag is set or nothing new was published for
-// idle_ns.  prof (may be null): CTA 0's nanoseconds in [1] column passes,
-// [2] the first barrier, [3] merges, [4] the second barrier and decisions,
-// [6] iterations; [8 + 2 it], [9 + 2 it]: column-pass time and running
-// problems of iteration it < 4096; [8 + 8192 + cta]: each CTA's column time.
-__global__ void __launch_bounds__(NTT, 1) batch_kernel(const Prob* probs, const volatile unsigned* pub,
-                                                        volatile unsigned* done, unsigned* dctl, double* prof,
-                                                        unsigned long long idle_ns) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  double* ringbuf = reinterpret_cast<double*>(smem);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ringbuf + (size_t)STAGES * kSlot);
-  double* red = reinterpret_cast<double*>(smem + (size_t)STAGES * kSlot * 8 + 64);
-  State* S = reinterpret_cast<State*>(red + 2 * NW * 16);
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, cta = blockIdx.x, G = gridDim.x;
-  int par = 0;
-  unsigned nbar = 0;
-  auto gsync = [&]() -> bool { ++nbar; return grid_sync(dctl, dctl + 2, nbar * (unsigned)G); };
-  const bool timing = prof && cta == 0 && tid == 0;
-  double pt[7] = {0, 0, 0, 0, 0, 0, 0};
-  double my_col_ns = 0.0;
-  unsigned long long tl = timing ? globaltimer_ns() : 0ull;
-  auto lap = [&](int slot) {
-    if (timing) {
-      const unsigned long long t = globaltimer_ns();
-      pt[slot] += (double)(t - tl);
-      tl = t;
-    }
-  };
-  if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(bar + s, 1);
-    fence_mbar_init();
+// Row total of row i over the team's partials rp ([gp][m]), members in order.
+__device__ __forceinline__ double row_total(const double* rp, int gp, int m, int i) {
+  double acc = 0.0;
+  int k = 0;
+  for (; k + 4 <= gp; k += 4) {
+    const double x0 = __ldcg(rp + (size_t)k * m + i), x1 = __ldcg(rp + (size_t)(k + 1) * m + i);
+    const double x2 = __ldcg(rp + (size_t)(k + 2) * m + i), x3 = __ldcg(rp + (size_t)(k + 3) * m + i);
+    acc += x0;
+    acc += x1;
+    acc += x2;
+    acc += x3;
   }
-  // the published problems at start: unfinished ones run, finished ones stay retired
-  unsigned long long last_busy = globaltimer_ns();
-  if (cta == 0 && tid == 0) dctl[3] = min(pub[0], (unsigned)kMaxProbs);
-  if (!gsync()) return;
-  int np = (int)__ldcg(dctl + 3);
-  for (int q = tid; q < np; q += NTT) S[q] = State{done[q] ? ST_RETIRED : ST_RUN, 0, 0, probs[q].X ? 2 : 1, 1000.0, 1.0};
-  __syncthreads();
-
-  const Ring ring{ringbuf, bar, l2_policy_evict_first()};
-  unsigned q = 0;
-  Issuer is{{-1, 0}, 0};
-  while (true) {
-    // ---- column pass over my strips: first passes, iterations, final passes
-    const unsigned long long tcol0 = (prof && tid == 0) ? globaltimer_ns() : 0ull;
-    if (tid == 0) {
-      is.c = Cursor{-1, 0};
-      next_group(is.c, probs, S, np, cta, G);
-      is.seq = q;
-      issue_ahead(is, ring, q + STAGES, probs, S, np, cta, G);
-    }
-    bool ok = true;
-    for (int pi = 0; pi < np && ok; ++pi) {
-      const int st = S[pi].st;
-      if (st != ST_RUN && st != ST_FIN) continue;
-      const Prob& p = probs[pi];
-      const int k = team_index(p, cta, G);
-      if (k < 0) continue;
-      if (st == ST_FIN) {
-        switch (p.cls) {
-          case 0: final_pass<1, 16>(p, S[pi], k, red, par); break;
-          case 1: final_pass<2, 8>(p, S[pi], k, red, par); break;
-          case 2: final_pass<4, 4>(p, S[pi], k, red, par); break;
-          case 3: final_pass<8, 2>(p, S[pi], k, red, par); break;
-          default: final_pass<16, 1>(p, S[pi], k, red, par); break;
-        }
-      } else if (S[pi].init == 2) {
-        cost_pass(p, k, red, par);
-      } else if (S[pi].init) {
-        const double cm = S[pi].cmax;
-        switch (p.cls) {
-          case 0: init_pass<1>(p, k, cm, red, par); break;
-          case 1: init_pass<2>(p, k, cm, red, par); break;
-          case 2: init_pass<4>(p, k, cm, red, par); break;
-          case 3: init_pass<8>(p, k, cm, red, par); break;
-          default: init_pass<16>(p, k, cm, red, par); break;
-        }
-      } else {
-        switch (p.cls) {
-          case 0: ok = column_pass<1, 16, false>(p, S[pi], k, ring, q, is, probs, S, np, cta, G, red, par); break;
-          case 1: ok = column_pass<2, 8, false>(p, S[pi], k, ring, q, is, probs, S, np, cta, G, red, par); break;
-          case 2: ok = column_pass<4, 4, false>(p, S[pi], k, ring, q, is, probs, S, np, cta, G, red, par); break;
-          case 3: ok = column_pass<8, 2, false>(p, S[pi], k, ring, q, is, probs, S, np, cta, G, red, par); break;
-          default: ok = column_pass<16, 1, true>(p, S[pi], k, ring, q, is, probs, S, np, cta, G, red, par); break;
-        }
-      }
-    }
-    if (!ok) {
-      if (tid == 0) atomicOr(dctl + 2, KERR_MBAR_TIMEOUT);
-      return;
-    }
-    if (prof && tid == 0) my_col_ns += (double)(globaltimer_ns() - tcol0);
-    if (timing && (int)pt[6] < 4096) prof[8 + 2 * (int)pt[6]] = (double)(globaltimer_ns() - tl);
-    lap(1);
-    if (!gsync()) return;
-    lap(2);
-    // ---- row merges: u_next = a / (sum over the team's partials) for the
-    // running problems, f and the row marginals for the finishing ones
-    for (int pi = 0; pi < np; ++pi) {
-      const int st = S[pi].st;
-      if ((st != ST_RUN && st != ST_FIN) || S[pi].init == 2) continue;
-      const Prob& p = probs[pi];
-      const double* ucur = S[pi].par ? p.u1 : p.u0;
-      double* unext = S[pi].par ? p.u0 : p.u1;
-      for (int u = (cta - p.unit0 + G) % G; u < p.nunits; u += G) {
-        const double tot = merge_unit(p.rowp, p.gp, p.m, u);
-        const int i = u * kUnit + 4 * w + lane;
-        double t[2] = {0.0, 0.0};
-        if (lane < 4 && i < p.m) {
-          const double ai = p.a[i];
-          if (st == ST_FIN) {
-            p.f[i] = p.eps * log(__ldcg(ucur + i));
-            const double d = tot - ai;
-            t[0] = fabs(d);
-            t[1] = d * d;
-          } else {
-            const double un = ai / tot;
-            unext[i] = un;
-            if (!S[pi].init) {
-              const double d = log((__ldcg(ucur + i) * tot) / ai);
-              t[0] = d * d;
-            }
-            if (!(un >= kScaleMin && un <= kScaleMax) || !(tot >= 1e-300 && tot <= 1e300)) t[1] = 1.0;
-          }
-        }
-        block_sum_cols<2, NW>(t, red, par);
-        if (tid == 0) {
-          const int o = st == ST_FIN ? 2 : 0;
-          p.unitp[(size_t)u * 4 + o] = t[0];
-          p.unitp[(size_t)u * 4 + o + 1] = t[1];
-        }
-      }
-    }
-    if (cta == 0 && tid == 0) {
-      dctl[3] = min(pub[0], (unsigned)kMaxProbs);
-      dctl[4] = pub[1];
-      dctl[5] = (globaltimer_ns() - last_busy > idle_ns) ? 1u : 0u;
-    }
-    lap(3);
-    if (!gsync()) return;
-    const int np_new = max(np, (int)__ldcg(dctl + 3));
-    const bool stop = __ldcg(dctl + 4) != 0u, idle = __ldcg(dctl + 5) != 0u;
-    // ---- the same decisions in every CTA: warp w takes problems w, w+16, ...
-    int running = 0;
-    for (int pi = w; pi < np; pi += NW) {
-      State& s = S[pi];
-      if (s.st != ST_RUN && s.st != ST_FIN) continue;
-      const Prob& p = probs[pi];
-      const bool reporter = (p.off == cta) && lane == 0;
-      if (s.st == ST_FIN) {
-        double c[6] = {0, 0, 0, 0, 0, 0};
-        for (int k = lane; k < p.gp; k += 32)
-          for (int j = 0; j < 4; ++j) c[j] += __ldcg(p.colp + (size_t)k * 4 + j);
-        for (int u = lane; u < p.nunits; u += 32) {
-          c[4] += __ldcg(p.unitp + (size_t)u * 4 + 2);
-          c[5] += __ldcg(p.unitp + (size_t)u * 4 + 3);
-        }
-#pragma unroll
-        for (int j = 0; j < 6; ++j) c[j] = warp_sum(c[j]);
-        if (reporter) {
-          p.res[0] = c[0] + p.eps * c[1];  // accu(C % P) + reg * accu(P % (log(P) - 1))
-          p.res[1] = s.err;
-          p.res[2] = s.iter;
-          p.res[3] = (s.err <= p.tol) ? 0.0 : (s.iter == p.max_iter ? 1.0 : 2.0);
-          p.res[4] = c[4];
-          p.res[5] = c[2];
-          p.res[6] = sqrt(c[5]);
-          p.res[7] = sqrt(c[3]);
-          __threadfence_system();
-          done[pi] = 1u;
-        }
-        if (lane == 0) s.st = ST_RETIRED;
-        continue;
-      }
-      if (s.init == 2) {  // maximum of the cost over the team's strips
-        double mx = 0.0;
-        for (int k = lane; k < p.gp; k += 32) mx = fmax(mx, __ldcg(p.colp + (size_t)k * 4 + 2));
-        mx = warp_max(mx);
-        if (lane == 0) {
-          s.cmax = mx;
-          s.init = 1;
-          ++running;
-        }
-        continue;
-      }
-      double er = 0.0, ec = 0.0, bad = 0.0;
-      for (int u = lane; u < p.nunits; u += 32) {
-        er += __ldcg(p.unitp + (size_t)u * 4 + 0);
-        bad += __ldcg(p.unitp + (size_t)u * 4 + 1);
-      }
-      for (int k = lane; k < p.gp; k += 32) {
-        ec += __ldcg(p.colp + (size_t)k * 4 + 0);
-        bad += __ldcg(p.colp + (size_t)k * 4 + 1);
-      }
-      er = warp_sum(er);
-      ec = warp_sum(ec);
-      bad = warp_sum(bad);
-      if (lane != 0) continue;
-      if (bad != 0.0) {
-        if (reporter) {
-          p.res[3] = kUnsafeStatus;
-          __threadfence_system();
-          done[pi] = 1u;
-        }
-        s.st = ST_RETIRED;
-        continue;
-      }
-      ++running;
-      if (s.init) {  // u_1 = a / (K 1): no iteration counted
-        s.init = 0;
-        s.par ^= 1;
-        continue;
-      }
-      ++s.iter;
-      s.err = sqrt(er) + sqrt(ec);
-      if (s.iter < p.max_iter && s.err >= p.tol) s.par ^= 1;
-      else s.st = ST_FIN;
-    }
-    for (int pi = np + tid; pi < np_new; pi += NTT) S[pi] = State{ST_RUN, 0, 0, probs[pi].X ? 2 : 1, 1000.0, 1.0};
-    double t[1] = {(double)(running + (tid == 0 ? np_new - np : 0))};
-    block_sum_cols<1, NW>(t, red, par);  // (also orders the state updates before the next pass)
-    np = np_new;
-    if (timing && (int)pt[6] < 4096) prof[9 + 2 * (int)pt[6]] = t[0];
-    lap(4);
-    pt[6] += 1.0;
-    if (t[0] != 0.0) last_busy = globaltimer_ns();
-    else if (stop || idle) break;
-  }
-  if (timing)
-    for (int i = 0; i < 7; ++i) prof[i] = pt[i];
-  if (prof && tid == 0) prof[8 + 2 * 4096 + cta] = my_col_ns;
+  for (; k < gp; ++k) acc += __ldcg(rp + (size_t)k * m + i);
+  return acc;
 }
 
-int row_class(int m) { return m <= 512 ? 0 : m <= 1024 ? 1 : m <= 2048 ? 2 : m <= 4096 ? 3 : 4; }
+// The row update of one row: u_next = a / tot, the squared row error (not in
+// the init round) and the range check.
+__device__ __forceinline__ double row_update(double ai, double ucur, double tot, bool init, double& e, double& bd) {
+  const double un = ai / tot;
+  if (!init) {
+    const double d = log((ucur * tot) / ai);
+    e += d * d;
+  }
+  if (!(un >= kScaleMin && un <= kScaleMax) || !(tot >= 1e-300 && tot <= 1e300)) bd = 1.0;
+  return un;
+}
+
+// Sums of the team's partials part[gp][4] (columns j0, j1) in a fixed order,
+// computed by warp 0 and returned to every thread.
+__device__ __forceinline__ void team_sum2(const double* part, int gp, int j0, int j1, const Shared& sh, double& t0,
+                                          double& t1) {
+  if ((threadIdx.x >> 5) == 0) {
+    const int lane = threadIdx.x & 31;
+    double x0 = 0.0, x1 = 0.0;
+    for (int k = lane; k < gp; k += 32) {
+      x0 += __ldcg(part + (size_t)k * 4 + j0);
+      x1 += __ldcg(part + (size_t)k * 4 + j1);
+    }
+    x0 = warp_sum(x0);
+    x1 = warp_sum(x1);
+    if (lane == 0) {
+      sh.dec[0] = x0;
+      sh.dec[1] = x1;
+    }
+  }
+  __syncthreads();
+  t0 = sh.dec[0];
+  t1 = sh.dec[1];
+  __syncthreads();
+}
+
+// Solves problem pi as member k of its team.  RPT / CW: thread-per-row shape
+// of the row class; WARP: warp-per-column passes (resident, m <= 512); RES:
+// resident strip; REREAD: 16 rows per thread, the group is read from shared
+// memory twice instead of held in registers.  Rounds: 0 builds K and merges
+// u_1; round t >= 1 is iteration t (column pass, merge, decision).  Round
+// parity selects the partial buffers, so a member may run one round ahead of
+// another that is still reading.  Returns false after a failed wait.
+template <int RPT, int CW, bool WARP, bool RES, bool REREAD>
+__device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& sh, unsigned& q, unsigned* dctl,
+                      volatile unsigned* done, double* pw) {
+  const int tid = threadIdx.x;
+  const int m = p.m, gp = p.gp;
+  const int c0 = strip_begin(p.n, gp, k), c1 = strip_begin(p.n, gp, k + 1);
+  const bool redundant = RPT <= 8 && (p.mode & MODE_REDUNDANT) != 0;  // the host sets it for m <= 4096 only
+  const unsigned long long t_start = globaltimer_ns();
+  int par = 0;
+  unsigned nb = 0;
+  bool valid[RPT];
+#pragma unroll
+  for (int t = 0; t < RPT; ++t) valid[t] = tid + t * NTT < m;
+
+  // ---- round 0: cost from points, K, row sums of K
+  double cmax = 1.0;
+  bool forming = true;
+  if (p.X) {
+    const double mx = cost_pass(p, c0, c1, sh.red);
+    if (tid == 0) p.colp[((size_t)1 * gp + k) * 4 + 2] = mx;  // read before round 1 writes colp[1]
+    if (!team_sync(p, nb, true, dctl, sh, pw)) return false;
+    forming = false;
+    if (tid < 32) {
+      double v = 0.0;
+      for (int j = tid; j < gp; j += 32) v = fmax(v, __ldcg(p.colp + ((size_t)1 * gp + j) * 4 + 2));
+      v = warp_max(v);
+      if (tid == 0) sh.dec[2] = v;
+    }
+    __syncthreads();
+    cmax = sh.dec[2];
+  }
+  {
+    const double bad0 = init_pass<RPT>(p, k, c0, c1, cmax, sh.area, sh.red, par);
+    if (tid == 0) {
+      p.colp[(size_t)k * 4 + 0] = 0.0;
+      p.colp[(size_t)k * 4 + 1] = bad0;
+    }
+  }
+  if (!team_sync(p, nb, forming, dctl, sh, pw)) return false;
+
+  // stage ring of a streamed strip: its groups, prefetched across rounds
+  Ring ring{};
+  ring.buf = sh.area;
+  ring.bar = sh.bar;
+  ring.pol = (p.mode & MODE_KEEP_L2) ? l2_policy_evict_last() : l2_policy_evict_first();
+  ring.K = p.K;
+  ring.ldk = p.ldk;
+  ring.c0 = c0;
+  ring.c1 = c1;
+  ring.cw = CW;
+  ring.ngroups = (c1 - c0 + CW - 1) / CW;
+  ring.q0 = q;
+  unsigned issued = q;  // the same in every thread; thread 0 issues
+  auto drain = [&]() {
+    if (!RES)
+      for (; q < issued; ++q) ring.wait(q);
+    __syncthreads();
+  };
+
+  // u of the current round: registers (thread per row), su (warp mode) or
+  // ug[round parity] (split merges); un: the merged u of the next round
+  double u[RPT];
+#pragma unroll
+  for (int t = 0; t < RPT; ++t) u[t] = 0.0;
+  int rd = 0, iter = 0;
+  double err = 1000.0;
+  bool unsafe = false;
+  while (true) {
+    const int buf = rd & 1;
+    const double* rp = p.rowp + (size_t)buf * gp * m;
+    const bool init = rd == 0;
+    // ---- merge of round rd: un = a / (row totals), row error with u
+    double er = 0.0, rbad = 0.0;
+    double un[RPT];
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) un[t] = 0.0;
+    if (redundant) {
+      double e = 0.0, bd = 0.0;
+      if (WARP) {
+        if (tid < m) un[0] = row_update(p.a[tid], sh.su[tid], row_total(rp, gp, m, tid), init, e, bd);
+      } else {
+#pragma unroll
+        for (int t = 0; t < RPT; ++t)
+          if (valid[t]) {
+            const int i = tid + t * NTT;
+            un[t] = row_update(p.a[i], u[t], row_total(rp, gp, m, i), init, e, bd);
+          }
+      }
+      double tt[2] = {e, bd};
+      block_sum_cols<2, NW>(tt, sh.red, par);
+      er = tt[0];
+      rbad = tt[1];
+    } else {
+      const double* ucur = p.ug + (size_t)buf * m;
+      double* unext = p.ug + (size_t)(buf ^ 1) * m;
+      double e = 0.0, bd = 0.0;
+      for (int un_ = k; un_ < p.nunits; un_ += gp) {
+        const double tot = merge_unit(rp, gp, m, un_);
+        const int i = un_ * kUnit + 4 * (tid >> 5) + (tid & 31);
+        if ((tid & 31) < 4 && i < m) unext[i] = row_update(p.a[i], init ? 1.0 : __ldcg(ucur + i), tot, init, e, bd);
+      }
+      double tt[2] = {e, bd};
+      block_sum_cols<2, NW>(tt, sh.red, par);
+      if (tid == 0) {
+        p.mrgp[((size_t)buf * gp + k) * 4 + 0] = tt[0];
+        p.mrgp[((size_t)buf * gp + k) * 4 + 1] = tt[1];
+      }
+      if (!team_sync(p, nb, false, dctl, sh, pw)) {
+        drain();
+        return false;
+      }
+      team_sum2(p.mrgp + (size_t)buf * gp * 4, gp, 0, 1, sh, er, rbad);
+    }
+    // ---- decision of round rd (the same inputs and order in every member)
+    double ec, cbad;
+    team_sum2(p.colp + (size_t)buf * gp * 4, gp, 0, 1, sh, ec, cbad);
+    if (k == 0 && tid == 0) atomicAdd(dctl + DC_PROGRESS, 1u);
+    if (rbad != 0.0 || cbad != 0.0) {
+      unsafe = true;
+      break;
+    }
+    if (!init) {
+      iter = rd;
+      err = sqrt(er) + sqrt(ec);
+      if (!(iter < p.max_iter && err >= p.tol)) break;  // u, v of round rd are the final ones
+    }
+    // ---- the merged u becomes current
+    ++rd;
+    const int nbuf = rd & 1;
+    if (redundant) {
+      if (WARP) {
+        if (tid < m) sh.su[tid] = un[0];
+        __syncthreads();
+      } else {
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) u[t] = un[t];
+      }
+    } else {
+      const double* ucur = p.ug + (size_t)nbuf * m;
+      if (WARP) {
+        for (int i = tid; i < m; i += NTT) sh.su[i] = __ldcg(ucur + i);
+        __syncthreads();
+      } else {
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) u[t] = valid[t] ? __ldcg(ucur + tid + t * NTT) : 0.0;
+      }
+    }
+    // ---- column pass of round rd: v = b / (K^T u), row partials of K v
+    double ecol = 0.0, bcol = 0.0;
+    if constexpr (WARP) {
+      if (m <= 64) warp_pass<2>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
+      else if (m <= 128) warp_pass<4>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
+      else if (m <= 256) warp_pass<8>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
+      else warp_pass<16>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
+    } else {
+      double r[RPT];
+#pragma unroll
+      for (int t = 0; t < RPT; ++t) r[t] = 0.0;
+      double e = 0.0, bd = 0.0;
+      if constexpr (RES) {
+        for (int jb = c0; jb < c1; jb += CW)
+          block_group<RPT, CW, REREAD>(p, sh.area + (size_t)(jb - c0) * p.ldk + tid, jb, min(CW, c1 - jb), u, r,
+                                       valid, sh.red, par, e, bd, nullptr, 0u);
+      } else {
+        if (tid == 0)
+          for (unsigned s2 = issued; s2 < q + STAGES; ++s2) ring.issue(s2);
+        issued = max(issued, q + STAGES);
+        for (int gi = 0; gi < ring.ngroups; ++gi) {
+          const unsigned seq = q;
+          if (!ring.wait(seq)) {
+            atomicOr(dctl + DC_ERR, KERR_MBAR_TIMEOUT);
+            drain();
+            return false;
+          }
+          const int jb = ring.group_begin(seq);
+          block_group<RPT, CW, REREAD>(p, ring.slot(seq) + tid, jb, min(CW, c1 - jb), u, r, valid, sh.red, par, e,
+                                       bd, &ring, seq);
+          q = seq + 1;
+          issued = seq + STAGES + 1;  // block_group issued stage seq + STAGES
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < RPT; ++t)
+        if (valid[t]) p.rowp[((size_t)nbuf * gp + k) * m + tid + t * NTT] = r[t];
+      double tt[2] = {e, bd};
+      block_sum_cols<2, NW>(tt, sh.red, par);
+      ecol = tt[0];
+      bcol = tt[1];
+    }
+    if (tid == 0) {
+      p.colp[((size_t)nbuf * gp + k) * 4 + 0] = ecol;
+      p.colp[((size_t)nbuf * gp + k) * 4 + 1] = bcol;
+    }
+    if (!team_sync(p, nb, false, dctl, sh, pw)) {
+      drain();
+      return false;
+    }
+  }
+  drain();
+
+  if (unsafe) {
+    if (k == 0 && tid == 0) {
+      p.res[3] = kUnsafeStatus;
+      __threadfence_system();
+      done[pi] = 1u;
+    }
+    return true;
+  }
+
+  // ---- final round: u of the last column pass into the area (K is no longer
+  // read), then P, g, loss and marginal partials
+  double* us = sh.area;
+  if (rd == 0) {
+    // no iteration ran (cannot happen with max_iter >= 1): u = u_1
+    for (int i = tid; i < m; i += NTT) us[i] = 0.0;
+  } else if (redundant || !WARP) {
+    if (WARP) {
+      for (int i = tid; i < m; i += NTT) us[i] = sh.su[i];
+    } else if (redundant) {
+#pragma unroll
+      for (int t = 0; t < RPT; ++t)
+        if (valid[t]) us[tid + t * NTT] = u[t];
+    } else {
+      const double* ucur = p.ug + (size_t)(rd & 1) * m;
+      for (int i = tid; i < m; i += NTT) us[i] = __ldcg(ucur + i);
+    }
+  } else {
+    for (int i = tid; i < m; i += NTT) us[i] = sh.su[i];
+  }
+  __syncthreads();
+  const int fbuf = (rd + 1) & 1;
+  final_pass<RPT, 16 / RPT>(p, k, fbuf, c0, c1, us, sh.red, par);
+  if (!team_sync(p, nb, false, dctl, sh, pw)) return false;
+  if (k == 0) {
+    const double* rp = p.rowp + (size_t)fbuf * gp * m;
+    double l1 = 0.0, l2 = 0.0;
+    for (int i = tid; i < m; i += NTT) {
+      const double d = row_total(rp, gp, m, i) - p.a[i];
+      l1 += fabs(d);
+      l2 += d * d;
+      p.f[i] = p.eps * log(us[i]);
+    }
+    double tt[2] = {l1, l2};
+    block_sum_cols<2, NW>(tt, sh.red, par);
+    double s1, s2, lc1, lc2;
+    team_sum2(p.colp + (size_t)fbuf * gp * 4, gp, 0, 1, sh, s1, s2);
+    team_sum2(p.colp + (size_t)fbuf * gp * 4, gp, 2, 3, sh, lc1, lc2);
+    if (tid == 0) {
+      p.res[0] = s1 + p.eps * s2;  // accu(C % P) + reg * accu(P % (log(P) - 1))
+      p.res[1] = err;
+      p.res[2] = iter;
+      p.res[3] = (err <= p.tol) ? 0.0 : (iter == p.max_iter ? 1.0 : 2.0);
+      p.res[4] = tt[0];
+      p.res[5] = lc1;
+      p.res[6] = sqrt(tt[1]);
+      p.res[7] = sqrt(lc2);
+      p.res[8] = (double)(globaltimer_ns() - t_start);
+      __threadfence_system();
+      done[pi] = 1u;
+    }
+  }
+  return true;
+}
+
+// Claim of the next member slot (thread 0): the oldest published problem
+// whose team is incomplete.  Returns the problem and member index, or pi = -1
+// when the launch is closing (or on an error).  The published count is taken
+// from pub[0] until the launch closes (stop flag, or idle_ns with nothing to
+// claim and no team running); after that it is frozen, so a member never
+// waits for CTAs that have left.
+__device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned* dctl, unsigned long long idle_ns,
+                      int& pi, int& k) {
+  pi = -1;
+  k = -1;
+  const unsigned long long t_idle = globaltimer_ns();
+  while (true) {
+    if (*(volatile unsigned*)(dctl + DC_ERR) != 0u) return;
+    const unsigned W = *(volatile unsigned*)(dctl + DC_AVAIL);
+    const unsigned npx = W & ~kClosed;
+    if (!(W & kClosed)) {
+      const unsigned p0 = min(pub[0], (unsigned)kMaxProbs);
+      if (p0 > npx) {
+        atomicCAS(dctl + DC_AVAIL, W, p0);
+        continue;
+      }
+    }
+    for (unsigned h = *(volatile unsigned*)(dctl + DC_HEAD); h < npx; ++h) {
+      const int gp = __ldcg(&probs[h].gp);
+      unsigned* ctl = reinterpret_cast<unsigned*>(__ldcg(reinterpret_cast<const unsigned long long*>(&probs[h].ctl)));
+      const unsigned c = atomicAdd(ctl, 1u);
+      if ((int)c < gp) {
+        if ((int)c == gp - 1) atomicMax(dctl + DC_HEAD, h + 1);
+        pi = (int)h;
+        k = (int)c;
+        return;
+      }
+    }
+    if (W & kClosed) return;
+    const bool idle = globaltimer_ns() - t_idle > idle_ns && *(volatile unsigned*)(dctl + DC_ACTIVE) == 0u;
+    if (pub[1] != 0u || idle) {
+      atomicCAS(dctl + DC_AVAIL, W, W | kClosed);
+      continue;
+    }
+    __nanosleep(1000);
+  }
+}
+
+int __host__ __device__ row_class(int m) { return m <= 512 ? 0 : m <= 1024 ? 1 : m <= 2048 ? 2 : m <= 4096 ? 3 : 4; }
+
+// Service loop: CTAs claim member slots of the published problems
+// probs[0, pub[0]) (pub[1]: stop flag; host-mapped memory for a server,
+// device memory for a batch call) until the launch closes.  done[q] is set
+// (system scope) once problem q's results are in probs[q].res.  dctl: see
+// DC_*.  prof (may be null): per CTA [4 c + 0] busy ns, [1] team-wait ns,
+// [2] claim ns, [3] member slots solved.
+__global__ void __launch_bounds__(NTT, 1) service_kernel(const Prob* probs, const volatile unsigned* pub,
+                                                          volatile unsigned* done, unsigned* dctl, double* prof,
+                                                          unsigned long long idle_ns) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  Shared sh;
+  sh.area = reinterpret_cast<double*>(smem);
+  sh.bar = reinterpret_cast<uint64_t*>(smem + (size_t)kArea * 8);
+  sh.su = reinterpret_cast<double*>(smem + (size_t)kArea * 8 + 64);
+  sh.red = sh.su + kWarpRows;
+  sh.dec = sh.red + 2 * NW * 16;
+  sh.flag = reinterpret_cast<int*>(sh.dec + 8);
+  Prob* sp = reinterpret_cast<Prob*>(sh.flag + 4);
+  const int tid = threadIdx.x, cta = blockIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(sh.bar + s, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned q = 0;
+  double t_busy = 0.0, t_wait = 0.0, t_claim = 0.0, slots = 0.0;
+  double* pw = prof ? &t_wait : nullptr;
+  while (true) {
+    const unsigned long long t0 = globaltimer_ns();
+    if (tid == 0) {
+      int pi, k;
+      claim(probs, pub, dctl, idle_ns, pi, k);
+      sh.flag[1] = pi;
+      sh.flag[2] = k;
+      if (pi >= 0) {
+        atomicAdd(dctl + DC_ACTIVE, 1u);
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(probs + pi);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(sp);
+        for (int w = 0; w < (int)(sizeof(Prob) / 8); ++w) dst[w] = __ldcg(src + w);
+      }
+    }
+    __syncthreads();
+    const int pi = sh.flag[1], k = sh.flag[2];
+    const unsigned long long t1 = globaltimer_ns();
+    t_claim += (double)(t1 - t0);
+    if (pi < 0) break;
+    const Prob& p = *sp;
+    bool ok;
+    if (p.mode & MODE_RESIDENT) {
+      if (p.mode & MODE_WARP) {
+        ok = solve<1, 16, true, true, false>(p, pi, k, sh, q, dctl, done, pw);
+      } else {
+        switch (row_class(p.m)) {
+          case 0: ok = solve<1, 16, false, true, false>(p, pi, k, sh, q, dctl, done, pw); break;
+          case 1: ok = solve<2, 8, false, true, false>(p, pi, k, sh, q, dctl, done, pw); break;
+          case 2: ok = solve<4, 4, false, true, false>(p, pi, k, sh, q, dctl, done, pw); break;
+          case 3: ok = solve<8, 2, false, true, false>(p, pi, k, sh, q, dctl, done, pw); break;
+          default: ok = solve<16, 1, false, true, true>(p, pi, k, sh, q, dctl, done, pw); break;
+        }
+      }
+    } else {
+      switch (row_class(p.m)) {
+        case 0: ok = solve<1, 16, false, false, false>(p, pi, k, sh, q, dctl, done, pw); break;
+        case 1: ok = solve<2, 8, false, false, false>(p, pi, k, sh, q, dctl, done, pw); break;
+        case 2: ok = solve<4, 4, false, false, false>(p, pi, k, sh, q, dctl, done, pw); break;
+        case 3: ok = solve<8, 2, false, false, false>(p, pi, k, sh, q, dctl, done, pw); break;
+        default: ok = solve<16, 1, false, false, true>(p, pi, k, sh, q, dctl, done, pw); break;
+      }
+    }
+    __syncthreads();  // sp and flags are rewritten by the next claim
+    if (tid == 0) atomicSub(dctl + DC_ACTIVE, 1u);
+    t_busy += (double)(globaltimer_ns() - t1);
+    slots += 1.0;
+    if (!ok) break;
+  }
+  if (prof && tid == 0) {
+    prof[4 * cta + 0] = t_busy - t_wait;
+    prof[4 * cta + 1] = t_wait;
+    prof[4 * cta + 2] = t_claim;
+    prof[4 * cta + 3] = slots;
+  }
+}
 
 }  // namespace batch
 
-// Per-launch bounds: problem count (shared-memory state) and total elements
-// (the K build of one launch must stay well inside the bounded barrier wait).
-constexpr long long kLaunchMaxElems = 1LL << 30;
-// Problems with more than this many elements go through the per-call path:
-// its grid-wide sweep streams them at the bandwidth bound with less
-// per-iteration overhead than a lockstep iteration.
-constexpr long long kBatchMaxElems = 4LL << 20;
+// Per-launch bound on the elements of the streamed problems' K and the
+// points-built costs (device memory of one launch).
+constexpr long long kLaunchMaxElems = 1LL << 31;
 
-enum { SBT_DESC = 200, SBT_K, SBT_WORK, SBT_CTRL, SBT_PROF, SBT_RES, SBT_HOSTIO = 210 };
+enum { SBT_DESC = 200, SBT_K, SBT_WORK, SBT_CTRL, SBT_PROF, SBT_RES, SBT_PCTL, SBT_HOSTIO = 210 };
 
-// Placement of problem q on the grid: team size, offset, merge units and the
-// row class (all functions of the problem and of the running placement
-// pointers), and the sizes of its work arrays.
-void place(const rwig_problem& q, int G, int& ptr, int& unit0, batch::Prob& d, long long& kdoubles,
-           long long& wdoubles) {
+// Placement of problem q: team size, strip mode, merge mode (functions of the
+// problem, the SM count and the engine options batch.strip_kb,
+// batch.max_team, batch.redundant_rows and batch.l2_keep_mb) and the sizes of
+// its K and work arrays.
+void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, long long& wdoubles) {
   using namespace batch;
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
+  d = Prob{};
   d.m = q.M;
   d.n = q.N;
   d.ldk = ((q.M + 1) / 2) * 2;
-  d.gp = (int)std::min<long long>(
-      std::min(G, q.N), std::max<long long>(1, ((long long)d.ldk * q.N * 8 + kStripBytes - 1) / kStripBytes));
-  d.off = ptr;
-  ptr = (ptr + d.gp) % G;
+  const long long strip_target = (long long)(option("batch.strip_kb", 184.0) * 1024.0 / 8.0);
+  const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
+  const int gp_res = (int)((q.N + cols - 1) / cols);
+  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)G)));
+  int mode = 0;
+  if (gp_res <= maxteam) {
+    mode |= MODE_RESIDENT;
+    d.gp = gp_res;
+    if (q.M <= kWarpRows) mode |= MODE_WARP;
+  } else {
+    d.gp = std::min(maxteam, q.N);
+    if ((double)d.ldk * q.N * 8.0 <= option("batch.l2_keep_mb", 48.0) * 1048576.0) mode |= MODE_KEEP_L2;
+  }
+  const long long red_rows = (long long)option("batch.redundant_rows", 16384.0);
+  if (q.M <= 4096 && (d.gp == 1 || (long long)d.gp * q.M <= red_rows)) mode |= MODE_REDUNDANT;
+  d.mode = mode;
   d.nunits = (q.M + kUnit - 1) / kUnit;
-  d.unit0 = unit0;
-  unit0 = (unit0 + d.nunits) % G;
   d.max_iter = q.max_iter;
-  d.cls = row_class(q.M);
   d.eps = q.reg;
   d.tol = q.zero_tol;
   d.a = q.a;
@@ -703,37 +989,39 @@ void place(const rwig_problem& q, int G, int& ptr, int& unit0, batch::Prob& d, l
   d.P = q.P;
   d.f = q.f;
   d.g = q.g;
-  kdoubles = al(d.ldk * q.N);
-  wdoubles = 2 * al(q.M) + al((long long)d.gp * q.M) + al(4LL * d.gp) + al(4LL * d.nunits) + 32 +
+  kdoubles = (mode & MODE_RESIDENT) ? 0 : al(d.ldk * q.N);
+  wdoubles = al(2LL * d.gp * q.M) + 2 * al(8LL * d.gp) + al(2LL * q.M) + 32 +
              (q.C ? 0 : al((long long)q.M * q.N));  // the cost built from points
 }
 
-// Points the work arrays of d into w (wdoubles doubles) and K into k.
-void bind(batch::Prob& d, double* k, double* w, double* res) {
+// Points the work arrays of d into w (wdoubles doubles), K into k, the
+// results into res and the control words into ctl (4, zeroed by the caller).
+void bind(batch::Prob& d, double* k, double* w, double* res, unsigned* ctl) {
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   d.K = k;
-  d.u0 = w;
-  d.u1 = w + al(d.m);
-  d.rowp = d.u1 + al(d.m);
-  d.colp = d.rowp + al((long long)d.gp * d.m);
-  d.unitp = d.colp + al(4LL * d.gp);
+  d.rowp = w;
+  d.colp = d.rowp + al(2LL * d.gp * d.m);
+  d.mrgp = d.colp + al(8LL * d.gp);
+  d.ug = d.mrgp + al(8LL * d.gp);
   d.res = res;
-  if (d.X) d.C = d.unitp + al(4LL * d.nunits) + 32;
+  d.ctl = ctl;
+  if (d.X) d.C = d.ug + al(2LL * d.m) + 32;
 }
 
 int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, const unsigned* pub, unsigned* done,
-                   unsigned* dctl, double* dprof, unsigned long long idle_ns) {
+                   unsigned* dctl, double* dprof, unsigned long long idle_ns, unsigned avail0) {
   using namespace batch;
   static bool attr = false;
   if (!attr) {
     RWIG_CUDA_TRY(
-        cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes()));
+        cudaFuncSetAttribute(service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes()));
     attr = true;
   }
   int nblk = 0;
-  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, batch_kernel, NTT, smem_bytes()));
+  RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, service_kernel, NTT, smem_bytes()));
   if (nblk < 1) return set_error(RWIG_E_UNSUPPORTED, "batched Sinkhorn kernel does not fit on an SM");
-  RWIG_CUDA_TRY(cudaMemsetAsync(dctl, 0, sizeof(unsigned) * 8, st));
+  const unsigned h0[8] = {avail0, 0, 0, 0, 0, 0, 0, 0};
+  RWIG_CUDA_TRY(cudaMemcpyAsync(dctl, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
   const Prob* dp = dprob;
   const volatile unsigned* pb = pub;
   volatile unsigned* dn = done;
@@ -741,67 +1029,52 @@ int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, cons
   double* pr = dprof;
   unsigned long long idle = idle_ns;
   void* args[] = {(void*)&dp, (void*)&pb, (void*)&dn, (void*)&ctl, (void*)&pr, (void*)&idle};
-  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)batch_kernel, dim3(ctx->sm_count), dim3(NTT), args,
+  RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)service_kernel, dim3(ctx->sm_count), dim3(NTT), args,
                                             smem_bytes(), st));
   return 0;
 }
 
-// Prints the optional per-phase profile of the last launch (rwig_set_option
-// "batch.profile").
-int print_profile(Context* ctx, const double* dprof, int np) {
+// Prints the optional per-CTA profile of the last launch (rwig_set_option
+// "batch.profile"): busy, team-wait and claim time, member slots.
+int print_profile(Context* ctx, const double* dprof, int np, float kernel_ms) {
   const int G = ctx->sm_count;
-  std::vector<double> hpv(8 + 2 * 4096 + 256);
-  RWIG_CUDA_TRY(cudaMemcpy(hpv.data(), dprof, sizeof(double) * hpv.size(), cudaMemcpyDeviceToHost));
-  const double* h = hpv.data();
-  double mx = 0.0, mn = 1e300, sm = 0.0;
-  for (int c = 0; c < G; ++c) {
-    mx = std::max(mx, h[8 + 2 * 4096 + c]);
-    mn = std::min(mn, h[8 + 2 * 4096 + c]);
-    sm += h[8 + 2 * 4096 + c];
-  }
-  const int nit = std::min(4096, (int)h[6]);
-  std::vector<double> tsum(6, 0.0);
-  std::vector<int> tcnt(6, 0);
-  for (int it = 0; it < nit; ++it) {
-    const int r = (int)h[9 + 2 * it];
-    const int b = r <= 1 ? 0 : r <= 2 ? 1 : r <= 4 ? 2 : r <= 16 ? 3 : r <= 64 ? 4 : 5;
-    tsum[b] += h[8 + 2 * it];
-    ++tcnt[b];
-  }
+  std::vector<double> h(4 * (size_t)G);
+  RWIG_CUDA_TRY(cudaMemcpy(h.data(), dprof, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+  double s[4] = {0, 0, 0, 0}, mx[4] = {0, 0, 0, 0};
+  for (int c = 0; c < G; ++c)
+    for (int j = 0; j < 4; ++j) {
+      s[j] += h[4 * c + j];
+      mx[j] = std::max(mx[j], h[4 * c + j]);
+    }
   std::fprintf(stderr,
-               "batch_kernel profile (CTA 0, ms): column passes %.3f | barrier 1 %.3f | merges %.3f | barrier 2 + "
-               "decisions %.3f | iterations %.0f | problems %d\n  column pass per CTA (ms): max %.3f mean %.3f min "
-               "%.3f\n  column pass by running problems (iterations, us):",
-               h[1] * 1e-6, h[2] * 1e-6, h[3] * 1e-6, h[4] * 1e-6, h[6], np, mx * 1e-6, sm / G * 1e-6, mn * 1e-6);
-  const char* lab[6] = {"<=1", "2", "3-4", "5-16", "17-64", ">64"};
-  for (int b = 0; b < 6; ++b) std::fprintf(stderr, " %s: %d, %.1f |", lab[b], tcnt[b], tcnt[b] ? tsum[b] / tcnt[b] * 1e-3 : 0.0);
-  std::fprintf(stderr, "\n");
+               "service_kernel profile: %d problems, kernel %.3f ms | per CTA mean (max) ms: busy %.3f (%.3f), "
+               "team waits %.3f (%.3f), claim/idle %.3f (%.3f) | member slots %.0f\n",
+               np, kernel_ms, s[0] / G * 1e-6, mx[0] * 1e-6, s[1] / G * 1e-6, mx[1] * 1e-6, s[2] / G * 1e-6,
+               mx[2] * 1e-6, s[3]);
   return 0;
 }
 
-// One launch over problems `idx` (all eligible for the kernel), every one
-// published up front with the stop flag set.
+// One launch over problems `idx` (all eligible for the kernel), published up
+// front in descending size (the claim order) with the launch closed.
 static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs, const std::vector<int>& idx,
                         rwig_result* out, std::vector<int>& percall, int* launches) {
   using namespace batch;
   const int np = (int)idx.size();
   const int G = ctx->sm_count;
   if (G > kMaxTeam) return set_error(RWIG_E_UNSUPPORTED, "more SMs than the batched kernel's team limit");
-  std::vector<Prob> hp(np);
-  std::vector<long long> koff(np), woff(np);
-  long long kd = 0, wd = 0;
-  int ptr = 0, unit0 = 0;
-  // team placement, largest problems first; the problem order stays as given
-  std::vector<int> ord(np);
+  std::vector<int> ord(np);  // descriptor slot -> position in idx
   std::iota(ord.begin(), ord.end(), 0);
   std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
     return (long long)probs[idx[x]].M * probs[idx[x]].N > (long long)probs[idx[y]].M * probs[idx[y]].N;
   });
-  for (int t : ord) {
+  std::vector<Prob> hp(np);
+  std::vector<long long> koff(np), woff(np);
+  long long kd = 0, wd = 0;
+  for (int s = 0; s < np; ++s) {
     long long k1, w1;
-    place(probs[idx[t]], G, ptr, unit0, hp[t], k1, w1);
-    koff[t] = kd;
-    woff[t] = wd;
+    place(probs[idx[ord[s]]], G, hp[s], k1, w1);
+    koff[s] = kd;
+    woff[s] = wd;
     kd += k1;
     wd += w1;
   }
@@ -810,19 +1083,23 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   double* dW = (double*)scratch(ctx, SBT_WORK, sizeof(double) * std::max<long long>(wd, 32));
   double* dres = (double*)scratch(ctx, SBT_RES, sizeof(double) * 10 * np);
   unsigned* ctrl = (unsigned*)scratch(ctx, SBT_CTRL, sizeof(unsigned) * (8 + 2 + kMaxProbs));
+  unsigned* pctl = (unsigned*)scratch(ctx, SBT_PCTL, sizeof(unsigned) * 4 * kMaxProbs);
   const bool profile = option("batch.profile", 0.0) != 0.0;
-  double* dprof = profile ? (double*)scratch(ctx, SBT_PROF, sizeof(double) * (8 + 2 * 4096 + 256)) : nullptr;
-  if (!dprob || !dK || !dW || !dres || !ctrl || (profile && !dprof)) return RWIG_E_NOMEM;
-  for (int t = 0; t < np; ++t) bind(hp[t], dK + koff[t], dW + woff[t], dres + 10 * (size_t)t);
+  double* dprof = profile ? (double*)scratch(ctx, SBT_PROF, sizeof(double) * 4 * G) : nullptr;
+  if (!dprob || !dK || !dW || !dres || !ctrl || !pctl || (profile && !dprof)) return RWIG_E_NOMEM;
+  for (int s = 0; s < np; ++s) bind(hp[s], dK + koff[s], dW + woff[s], dres + 10 * (size_t)s, pctl + 4 * s);
   unsigned* pub = ctrl + 8;
   unsigned* done = ctrl + 10;
   const unsigned hpub[2] = {(unsigned)np, 1u};
   RWIG_CUDA_TRY(cudaMemcpyAsync(dprob, hp.data(), sizeof(Prob) * np, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(pub, hpub, sizeof(hpub), cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned) * kMaxProbs, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(pctl, 0, sizeof(unsigned) * 4 * np, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(dres, 0, sizeof(double) * 10 * np, st));
-  const int rc = launch_service(ctx, st, dprob, pub, done, ctrl, dprof, 0ull);
+  if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
+  const int rc = launch_service(ctx, st, dprob, pub, done, ctrl, dprof, 0ull, (unsigned)np | kClosed);
   if (rc) return rc;
+  if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   ++*launches;
   std::vector<double> hres(10 * (size_t)np);
   RWIG_CUDA_TRY(cudaMemcpyAsync(hres.data(), dres, sizeof(double) * 10 * np, cudaMemcpyDeviceToHost, st));
@@ -831,14 +1108,17 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   if (hctl[2]) return set_error(RWIG_E_TIMEOUT, "a bounded wait in the batched Sinkhorn kernel expired");
   if (profile) {
-    const int rc2 = print_profile(ctx, dprof, np);
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, ctx->evk, ctx->ev1);
+    const int rc2 = print_profile(ctx, dprof, np, kms);
     if (rc2) return rc2;
   }
-  for (int t = 0; t < np; ++t) {
-    rwig_result& o = out[idx[t]];
-    const double* r = hres.data() + 10 * (size_t)t;
+  for (int s = 0; s < np; ++s) {
+    const int i = idx[ord[s]];
+    rwig_result& o = out[i];
+    const double* r = hres.data() + 10 * (size_t)s;
     if (r[3] == kUnsafeStatus) {
-      if (probs[idx[t]].C) percall.push_back(idx[t]);
+      if (probs[i].C) percall.push_back(i);
       else o.status = RWIG_E_UNSUPPORTED;  // outside the scaling form; the per-call path takes C
       continue;
     }
@@ -848,6 +1128,7 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
     o.status = (int)r[3];
     o.marg_l1_row = r[4];
     o.marg_l1_col = r[5];
+    o.device_us = r[8] * 1e-3;
     o.path = 0;
   }
   return 0;
@@ -872,7 +1153,8 @@ int batch_device(Context* ctx, cudaStream_t st, const rwig_problem* probs, int c
       out[i].status = RWIG_E_UNSUPPORTED;  // the per-call path takes a cost matrix
       continue;
     }
-    if (q.M <= kMaxRows && q.max_iter >= 1 && (pts || (long long)q.M * q.N <= kBatchMaxElems))
+    if (q.M <= kMaxRows && q.max_iter >= 1 &&
+        (pts || (double)q.M * q.N <= option("batch.max_elems", (double)(1LL << 26))))
       eligible.push_back(i);
     else
       percall.push_back(i);
@@ -1039,8 +1321,9 @@ struct rwig_server {
   double* hres = nullptr;                   // mapped: 10 results per slot
   double* dres = nullptr;
   unsigned* dctl = nullptr;                 // device control words
+  unsigned* dpctl = nullptr;                // device, 4 control words per slot
   unsigned hctl_err = 0;
-  int nslots = 0, npub = 0, ptr = 0, unit0 = 0, next_ticket = 0;
+  int nslots = 0, npub = 0, next_ticket = 0;
   bool launched = false;
   double budget = 0.0, inflight = 0.0;
   unsigned long long idle_ns = 0;
@@ -1079,7 +1362,7 @@ int ensure_running(rwig_server* s) {
   for (int i = 0; i < s->npub; ++i)
     if (!s->hdone[i]) pending = true;
   if (!pending) return 0;
-  const int rc = launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns);
+  const int rc = launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns, 0u);
   if (rc) return rc;
   s->launched = true;
   return 0;
@@ -1128,6 +1411,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
   if ((e = cudaMalloc(&s->dprob, sizeof(batch::Prob) * batch::kMaxProbs)) != cudaSuccess) return fail(e, "descriptors");
   if ((e = cudaMalloc(&s->dctl, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * 4 * batch::kMaxProbs)) != cudaSuccess) return fail(e, "slot control");
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
   if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
     return fail(e, "done");
@@ -1169,8 +1453,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   }
   Prob d{};
   long long kd = 0, wd = 0;
-  int ptr = s->ptr, unit0 = s->unit0;
-  place(*q, s->ctx->sm_count, ptr, unit0, d, kd, wd);
+  place(*q, s->ctx->sm_count, d, kd, wd);
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   const long long M = q->M, N = q->N;
   const long long cd = pts ? al(M * q->d) + al(N * q->d) : al(M * N);  // C, or the points
@@ -1207,12 +1490,11 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   d.f = df;
   d.g = dg;
   d.P = dP;
-  bind(d, dk, dw, s->dres + 10 * (size_t)slot);
+  bind(d, dk, dw, s->dres + 10 * (size_t)slot, s->dpctl + 4 * (size_t)slot);
+  RWIG_CUDA_TRY(cudaMemsetAsync(s->dpctl + 4 * (size_t)slot, 0, sizeof(unsigned) * 4, s->cs));
   s->staged[slot] = d;  // the copy source must outlive the asynchronous copy
   RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &s->staged[slot], sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
   RWIG_CUDA_TRY(cudaEventRecord(s->slots[slot].ev, s->cs));
-  s->ptr = ptr;
-  s->unit0 = unit0;
   auto& sl = s->slots[slot];
   sl.ticket = s->next_ticket++;
   sl.mem = mem;
@@ -1259,6 +1541,7 @@ extern "C" int rwig_server_poll(rwig_server* s, int ticket, rwig_result* out) {
     out->status = (int)r[3];
     out->marg_l1_row = r[4];
     out->marg_l1_col = r[5];
+    out->device_us = r[8] * 1e-3;
     RWIG_CUDA_TRY(cudaMemcpyAsync(sl.hf, sl.df, sizeof(double) * sl.M, cudaMemcpyDeviceToHost, s->cs));
     RWIG_CUDA_TRY(cudaMemcpyAsync(sl.hg, sl.dg, sizeof(double) * sl.N, cudaMemcpyDeviceToHost, s->cs));
     if (sl.hP)
@@ -1287,6 +1570,7 @@ extern "C" int rwig_server_destroy(rwig_server* s) {
     if (s->cs) cudaStreamSynchronize(s->cs);
     if (s->dprob) cudaFree(s->dprob);
     if (s->dctl) cudaFree(s->dctl);
+    if (s->dpctl) cudaFree(s->dpctl);
     if (s->hpub) cudaFreeHost(s->hpub);
     if (s->hdone) cudaFreeHost(s->hdone);
     if (s->hres) cudaFreeHost(s->hres);
