@@ -74,8 +74,8 @@ def test_in_mix_equals_alone_and_oracle():
 
 def test_memory_budget_and_idle_restart():
     q = _prob(0, 400, 300, 0.05, 2)
-    big = _prob(1, 1000, 1000, 0.05, 2)
-    with rw.Server(mem_budget_bytes=12e6, idle_ms=1.0) as srv:  # holds the small one (~2 MB), not the big one (~17 MB)
+    big = _prob(1, 1500, 1500, 0.05, 2)
+    with rw.Server(mem_budget_bytes=12e6, idle_ms=1.0) as srv:  # holds the small one (~1 MB), not the big one (~19 MB)
         t1 = srv.submit(q["a"], q["b"], q["C"], q["reg"], 2000, 1e-9)
         assert t1 is not None
         assert srv.submit(big["a"], big["b"], big["C"], big["reg"], 2000, 1e-9) is None  # over the budget
