@@ -518,6 +518,27 @@ __device__ __forceinline__ double row_update(double ai, double ucur, double tot,
   return un;
 }
 
+// Sums of the team's partials part[gp][4] (all four columns) in a fixed
+// order, computed by warp 0 and returned to every thread.
+__device__ __forceinline__ void team_sum4(const double* part, int gp, const Shared& sh, double (&t)[4]) {
+  if ((threadIdx.x >> 5) == 0) {
+    const int lane = threadIdx.x & 31;
+    double x[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = lane; k < gp; k += 32)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[j] += __ldcg(part + (size_t)k * 4 + j);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      x[j] = warp_sum(x[j]);
+      if (lane == 0) sh.dec[j] = x[j];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 4; ++j) t[j] = sh.dec[j];
+  __syncthreads();
+}
+
 // Sums of the team's partials part[gp][4] (columns j0, j1) in a fixed order,
 // computed by warp 0 and returned to every thread.
 __device__ __forceinline__ void team_sum2(const double* part, int gp, int j0, int j1, const Shared& sh, double& t0,
@@ -621,11 +642,16 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
     const double* rp = p.rowp + (size_t)buf * gp * m;
     const bool init = rd == 0;
     // ---- merge of round rd: un = a / (row totals), row error with u
-    double er = 0.0, rbad = 0.0;
+    double er = 0.0, rbad = 0.0, ec = 0.0, cbad = 0.0;
     double un[RPT];
 #pragma unroll
     for (int t = 0; t < RPT; ++t) un[t] = 0.0;
     if (redundant) {
+      // the column partials of the team ride along in the merge's reduction
+      // (thread t adds member t's), so the decision needs no further round trip
+      const double* cp = p.colp + (size_t)buf * gp * 4;
+      const double ce = tid < gp ? __ldcg(cp + (size_t)tid * 4 + 0) : 0.0;
+      const double cb = tid < gp ? __ldcg(cp + (size_t)tid * 4 + 1) : 0.0;
       double e = 0.0, bd = 0.0;
       if (WARP) {
         if (tid < m) un[0] = row_update(p.a[tid], sh.su[tid], row_total(rp, gp, m, tid), init, e, bd);
@@ -637,10 +663,12 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
             un[t] = row_update(p.a[i], u[t], row_total(rp, gp, m, i), init, e, bd);
           }
       }
-      double tt[2] = {e, bd};
-      block_sum_cols<2, NW>(tt, sh.red, par);
+      double tt[4] = {e, bd, ce, cb};
+      block_sum_cols<4, NW>(tt, sh.red, par);
       er = tt[0];
       rbad = tt[1];
+      ec = tt[2];
+      cbad = tt[3];
     } else {
       const double* ucur = p.ug + (size_t)buf * m;
       double* unext = p.ug + (size_t)(buf ^ 1) * m;
@@ -652,19 +680,25 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       }
       double tt[2] = {e, bd};
       block_sum_cols<2, NW>(tt, sh.red, par);
-      if (tid == 0) {
-        p.mrgp[((size_t)buf * gp + k) * 4 + 0] = tt[0];
-        p.mrgp[((size_t)buf * gp + k) * 4 + 1] = tt[1];
+      if (tid == 0) {  // with this member's column partials
+        double* mp = p.mrgp + ((size_t)buf * gp + k) * 4;
+        mp[0] = tt[0];
+        mp[1] = tt[1];
+        mp[2] = p.colp[((size_t)buf * gp + k) * 4 + 0];
+        mp[3] = p.colp[((size_t)buf * gp + k) * 4 + 1];
       }
       if (!team_sync(p, nb, false, dctl, sh, pw)) {
         drain();
         return false;
       }
-      team_sum2(p.mrgp + (size_t)buf * gp * 4, gp, 0, 1, sh, er, rbad);
+      double t4[4];
+      team_sum4(p.mrgp + (size_t)buf * gp * 4, gp, sh, t4);
+      er = t4[0];
+      rbad = t4[1];
+      ec = t4[2];
+      cbad = t4[3];
     }
     // ---- decision of round rd (the same inputs and order in every member)
-    double ec, cbad;
-    team_sum2(p.colp + (size_t)buf * gp * 4, gp, 0, 1, sh, ec, cbad);
     if (k == 0 && tid == 0) atomicAdd(dctl + DC_PROGRESS, 1u);
     if (rbad != 0.0 || cbad != 0.0) {
       unsafe = true;
@@ -964,14 +998,18 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
   const int gp_res = (int)((q.N + cols - 1) / cols);
   const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)G)));
+  const int res_team = std::min(maxteam, (int)option("batch.resident_team", (double)G));
   int mode = 0;
-  if (gp_res <= maxteam) {
+  if (gp_res <= res_team || (q.M <= kWarpRows && gp_res <= maxteam)) {
     mode |= MODE_RESIDENT;
     d.gp = gp_res;
     if (q.M <= kWarpRows) mode |= MODE_WARP;
   } else {
-    d.gp = std::min(maxteam, q.N);
-    if ((double)d.ldk * q.N * 8.0 <= option("batch.l2_keep_mb", 48.0) * 1048576.0) mode |= MODE_KEEP_L2;
+    // streamed strips of about batch.stream_strip_kb each
+    const double kbytes = (double)d.ldk * q.N * 8.0;
+    const double sst = std::max(64.0, option("batch.stream_strip_kb", 1e9)) * 1024.0;
+    d.gp = (int)std::min<double>(std::min(maxteam, q.N), std::max(1.0, std::ceil(kbytes / sst)));
+    if (kbytes <= option("batch.l2_keep_mb", 48.0) * 1048576.0) mode |= MODE_KEEP_L2;
   }
   const long long red_rows = (long long)option("batch.redundant_rows", 16384.0);
   if (q.M <= 4096 && (d.gp == 1 || (long long)d.gp * q.M <= red_rows)) mode |= MODE_REDUNDANT;
