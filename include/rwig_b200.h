@@ -76,7 +76,11 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "batch.strip_kb": target K strip per team member of a batched problem,
  *       at most 184 (default); strips up to that stay in shared memory;
  *   "batch.max_team": largest team of CTAs per batched problem (default:
- *       the SM count);
+ *       half the SM count);
+ *   "batch.resident_team": problems with M > 512 keep their K strips in
+ *       shared memory when that takes at most this many CTAs (default 16),
+ *       else stream strips of about "batch.stream_strip_kb" (default 1024)
+ *       from memory every iteration;
  *   "batch.redundant_rows": teams with gp * M up to this (and M <= 4096)
  *       merge row sums redundantly in every member, one team barrier per
  *       iteration (default 16384);

@@ -95,7 +95,7 @@ struct Prob {
   double* mrgp;      // [2][gp][4] merge partials (split merges)
   double* ug;        // [2][m] u (split merges)
   unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals
-  double* res;       // [10]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, -
+  double* res;       // [10]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, formation ns
   int m, n, max_iter, gp, mode, nunits;
   double eps, tol;
 };
@@ -587,10 +587,13 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
   // ---- round 0: cost from points, K, row sums of K
   double cmax = 1.0;
   bool forming = true;
+  unsigned long long t_form = 0;  // time waiting for the team to form
   if (p.X) {
     const double mx = cost_pass(p, c0, c1, sh.red);
     if (tid == 0) p.colp[((size_t)1 * gp + k) * 4 + 2] = mx;  // read before round 1 writes colp[1]
+    const unsigned long long tf = globaltimer_ns();
     if (!team_sync(p, nb, true, dctl, sh, pw)) return false;
+    t_form = globaltimer_ns() - tf;
     forming = false;
     if (tid < 32) {
       double v = 0.0;
@@ -608,7 +611,11 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       p.colp[(size_t)k * 4 + 1] = bad0;
     }
   }
-  if (!team_sync(p, nb, forming, dctl, sh, pw)) return false;
+  {
+    const unsigned long long tf = globaltimer_ns();
+    if (!team_sync(p, nb, forming, dctl, sh, pw)) return false;
+    if (forming) t_form = globaltimer_ns() - tf;
+  }
 
   // stage ring of a streamed strip: its groups, prefetched across rounds
   Ring ring{};
@@ -840,6 +847,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       p.res[6] = sqrt(tt[1]);
       p.res[7] = sqrt(lc2);
       p.res[8] = (double)(globaltimer_ns() - t_start);
+      p.res[9] = (double)t_form;
       __threadfence_system();
       done[pi] = 1u;
     }
@@ -997,8 +1005,8 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   const long long strip_target = (long long)(option("batch.strip_kb", 184.0) * 1024.0 / 8.0);
   const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
   const int gp_res = (int)((q.N + cols - 1) / cols);
-  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)G)));
-  const int res_team = std::min(maxteam, (int)option("batch.resident_team", (double)G));
+  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)(G / 2))));
+  const int res_team = std::min(maxteam, (int)option("batch.resident_team", 16.0));
   int mode = 0;
   if (gp_res <= res_team || (q.M <= kWarpRows && gp_res <= maxteam)) {
     mode |= MODE_RESIDENT;
@@ -1007,7 +1015,7 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   } else {
     // streamed strips of about batch.stream_strip_kb each
     const double kbytes = (double)d.ldk * q.N * 8.0;
-    const double sst = std::max(64.0, option("batch.stream_strip_kb", 1e9)) * 1024.0;
+    const double sst = std::max(64.0, option("batch.stream_strip_kb", 1024.0)) * 1024.0;
     d.gp = (int)std::min<double>(std::min(maxteam, q.N), std::max(1.0, std::ceil(kbytes / sst)));
     if (kbytes <= option("batch.l2_keep_mb", 48.0) * 1048576.0) mode |= MODE_KEEP_L2;
   }
@@ -1150,6 +1158,28 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
     cudaEventElapsedTime(&kms, ctx->evk, ctx->ev1);
     const int rc2 = print_profile(ctx, dprof, np, kms);
     if (rc2) return rc2;
+    // per placement class: problems, member-iterations, solve and formation time, K bytes per member-us
+    struct Agg { int n = 0; double mi = 0, dev = 0, form = 0, bytes = 0, mus = 0; };
+    Agg agg[4];
+    for (int s2 = 0; s2 < np; ++s2) {
+      const Prob& d = hp[s2];
+      const double* r = hres.data() + 10 * (size_t)s2;
+      const int c = ((d.mode & MODE_RESIDENT) ? 0 : 2) + (d.m > kWarpRows ? 1 : 0);
+      agg[c].n += 1;
+      agg[c].mi += r[2] * d.gp;
+      agg[c].dev += r[8] * 1e-6;
+      agg[c].form += r[9] * 1e-6;
+      agg[c].bytes += r[2] * (double)d.ldk * d.n * 8.0;
+      agg[c].mus += (r[8] - r[9]) * 1e-3 * d.gp;
+    }
+    const char* lab[4] = {"resident m<=512", "resident m>512", "streamed m<=512", "streamed m>512"};
+    for (int c = 0; c < 4; ++c)
+      if (agg[c].n)
+        std::fprintf(stderr,
+                     "  %-16s problems %3d | member-iterations %9.0f | solve ms (sum) %9.2f | formation ms (sum) "
+                     "%8.2f | member-us per member-iteration %6.2f | GB/s per member %6.1f\n",
+                     lab[c], agg[c].n, agg[c].mi, agg[c].dev, agg[c].form,
+                     agg[c].mi > 0 ? agg[c].mus / agg[c].mi : 0.0, agg[c].mus > 0 ? agg[c].bytes / agg[c].mus * 1e-3 : 0.0);
   }
   for (int s = 0; s < np; ++s) {
     const int i = idx[ord[s]];
