@@ -273,11 +273,13 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int m = p.m;
   const long long ldk = p.ldk;
-  double u[RPL], r[RPL];
+  // u in registers, or (16 rows per lane) read from su at each use
+  constexpr bool kUReg = RPL <= 8;
+  double u[kUReg ? RPL : 1], r[RPL];
 #pragma unroll
   for (int j = 0; j < RPL; ++j) {
     const int i = lane + 32 * j;
-    u[j] = i < m ? sh.su[i] : 0.0;
+    if (kUReg) u[kUReg ? j : 0] = i < m ? sh.su[i] : 0.0;
     r[j] = 0.0;
   }
   double e = 0.0, bd = 0.0;
@@ -289,7 +291,7 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
     for (int j = 0; j < RPL; ++j) {
       const int i = lane + 32 * j;
       kv[j] = i < m ? col[i] : 0.0;
-      s = fma(kv[j], u[j], s);
+      s = fma(kv[j], kUReg ? u[kUReg ? j : 0] : (i < m ? sh.su[i] : 0.0), s);
     }
   };
   auto finish = [&](int c, const double (&kv)[RPL], double s) {
@@ -354,6 +356,7 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
                                             double& e, double& bd, const Ring* ring, unsigned seq) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const long long ldk = p.ldk;
+  const double bl = lane < nc ? p.b[jb + lane] : 1.0;  // issued before the reduction's barrier
   double kv[REREAD ? 1 : RPT][CW], sum[CW];
 #pragma unroll
   for (int c = 0; c < CW; ++c) {
@@ -371,10 +374,10 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
   for (int c = 0; c < CW; ++c)
     if (c == lane) s_l = sum[c];
   const bool owner = lane < nc;
-  const double v_l = owner ? p.b[jb + lane] / s_l : 0.0;
+  const double v_l = owner ? bl / s_l : 0.0;
   if (w == 0 && owner) {
     p.g[jb + lane] = v_l;
-    const double d = (v_l * s_l) / p.b[jb + lane] - 1.0;  // first-order form of log(v s) - log b
+    const double d = (v_l * s_l) / bl - 1.0;  // first-order form of log(v s) - log b
     e += d * d;
     if (!(v_l >= kScaleMin && v_l <= kScaleMax) || !(s_l >= 1e-300 && s_l <= 1e300)) bd = 1.0;
   }
@@ -491,18 +494,18 @@ __device__ __forceinline__ double merge_unit(const double* rp, int gp, int m, in
 }
 
 // Row total of row i over the team's partials rp ([gp][m]), members in order.
+// Loads go out in batches of 8 (one memory round trip per batch); the sum
+// is sequential in member order.
 __device__ __forceinline__ double row_total(const double* rp, int gp, int m, int i) {
   double acc = 0.0;
-  int k = 0;
-  for (; k + 4 <= gp; k += 4) {
-    const double x0 = __ldcg(rp + (size_t)k * m + i), x1 = __ldcg(rp + (size_t)(k + 1) * m + i);
-    const double x2 = __ldcg(rp + (size_t)(k + 2) * m + i), x3 = __ldcg(rp + (size_t)(k + 3) * m + i);
-    acc += x0;
-    acc += x1;
-    acc += x2;
-    acc += x3;
+  for (int k = 0; k < gp; k += 8) {
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = k + j < gp ? __ldcg(rp + (size_t)(k + j) * m + i) : 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (k + j < gp) acc += x[j];
   }
-  for (; k < gp; ++k) acc += __ldcg(rp + (size_t)k * m + i);
   return acc;
 }
 
