@@ -72,6 +72,7 @@ constexpr int kMaxTeam = 160;              // CTAs of a team (the grid is one CT
 constexpr double kScaleMin = 5.1e-283, kScaleMax = 1.95e282;  // e^-650, e^650
 constexpr double kUnsafeStatus = -100.0;
 constexpr unsigned kClosed = 0x80000000u;
+constexpr int kResStride = 16;  // doubles of results per problem
 
 enum : int { MODE_RESIDENT = 1, MODE_WARP = 2, MODE_REDUNDANT = 4, MODE_KEEP_L2 = 8 };
 
@@ -95,7 +96,8 @@ struct Prob {
   double* mrgp;      // [2][gp][4] merge partials (split merges)
   double* ug;        // [2][m] u (split merges)
   unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals
-  double* res;       // [10]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, formation ns
+  double* res;       // [16]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, formation
+                     // ns, then member 0's ns in column passes, merges + decisions, team barriers
   int m, n, max_iter, gp, mode, nunits;
   double eps, tol;
 };
@@ -149,7 +151,7 @@ __device__ bool team_wait(unsigned* cnt, unsigned target, unsigned* dctl, bool f
 }
 
 // Team barrier (all threads).  Single-member teams need only the block barrier.
-__device__ __forceinline__ bool team_sync(const Prob& p, unsigned& nb, bool forming, unsigned* dctl, const Shared& sh,
+__device__ __forceinline__ bool team_sync(const Prob& p, unsigned& nb, bool forming, unsigned* dctl, const Shared sh,
                                           double* prof_wait) {
   __syncthreads();
   if (p.gp == 1) return true;
@@ -193,16 +195,19 @@ struct Ring {
 // a host that computes the differences, squares and sums elementwise, so the
 // same bits), stored un-normalised; the strip's maximum is returned (block max).
 __device__ double cost_pass(const Prob& p, int c0, int c1, double* red) {
-  const int m = p.m, n = p.n;
+  const int m = p.m, n = p.n, dim = p.d;
+  const double* const X = p.X;
+  const double* const Y = p.Y;
+  double* const C = const_cast<double*>(p.C);
   double mx = 0.0;
   for (int j = c0; j < c1; ++j)
     for (int i = threadIdx.x; i < m; i += NTT) {
       double acc = 0.0;
-      for (int q = 0; q < p.d; ++q) {
-        const double t = __dsub_rn(p.X[i + (size_t)q * m], p.Y[j + (size_t)q * n]);
+      for (int q = 0; q < dim; ++q) {
+        const double t = __dsub_rn(X[i + (size_t)q * m], Y[j + (size_t)q * n]);
         acc = __dadd_rn(acc, __dmul_rn(t, t));
       }
-      const_cast<double*>(p.C)[i + (size_t)j * m] = acc;
+      C[i + (size_t)j * m] = acc;
       mx = fmax(mx, acc);
     }
   mx = warp_max(mx);
@@ -231,19 +236,24 @@ __device__ double init_pass(const Prob& p, int k, int c0, int c1, double cmax, d
     r[t] = 0.0;
   }
   const bool res = (p.mode & MODE_RESIDENT) != 0;
+  double* const C = const_cast<double*>(p.C);
+  double* const Kg = p.K;
+  const long long ldk = p.ldk;
+  const bool pts = p.X != nullptr;
+  const double eps = p.eps;
 #pragma unroll 2
   for (int j = c0; j < c1; ++j) {
-    const double* cj = p.C + (size_t)j * m;
-    double* kj = res ? Kres + (size_t)(j - c0) * p.ldk : p.K + (size_t)j * p.ldk;
+    double* cj = C + (size_t)j * m;
+    double* kj = res ? Kres + (size_t)(j - c0) * ldk : Kg + (size_t)j * ldk;
 #pragma unroll
     for (int t = 0; t < RPT; ++t)
       if (valid[t]) {
         double c = cj[tid + t * NTT];
-        if (p.X) {  // C /= max C
+        if (pts) {  // C /= max C
           c = c / cmax;
-          const_cast<double*>(cj)[tid + t * NTT] = c;
+          cj[tid + t * NTT] = c;
         }
-        const double x = exp(-c / p.eps);
+        const double x = exp(-c / eps);
         kj[tid + t * NTT] = x;
         r[t] += x;
       }
@@ -268,18 +278,26 @@ __device__ double init_pass(const Prob& p, int k, int c0, int c1, double cmax, d
 // Column sum with u (from su), v = b / s, row partials r += K v.  The warps'
 // row partials are added in a fixed tree; the CTA's go to rowp[buf][k].
 template <int RPL>
-__device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, int c1, const double* Ks, const Shared& sh, int& par,
+__device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, int c1, const double* Ks, const Shared sh, int& par,
                           double& errc, double& bad) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  // every field used in the loops is read once here: stores through the
+  // plan pointers would otherwise force reloads of the descriptor
   const int m = p.m;
   const long long ldk = p.ldk;
+  const double* const bb = p.b + c0;
+  double* const gg = p.g + c0;
+  double* const rp_out = p.rowp + ((size_t)buf * p.gp + k) * m;
+  const double* const su = sh.su;
+  double* const tree = sh.area + kResident;
+  double* const red = sh.red;
   // u in registers, or (16 rows per lane) read from su at each use
   constexpr bool kUReg = RPL <= 8;
   double u[kUReg ? RPL : 1], r[RPL];
 #pragma unroll
   for (int j = 0; j < RPL; ++j) {
     const int i = lane + 32 * j;
-    if (kUReg) u[kUReg ? j : 0] = i < m ? sh.su[i] : 0.0;
+    if (kUReg) u[kUReg ? j : 0] = i < m ? su[i] : 0.0;
     r[j] = 0.0;
   }
   double e = 0.0, bd = 0.0;
@@ -291,17 +309,17 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
     for (int j = 0; j < RPL; ++j) {
       const int i = lane + 32 * j;
       kv[j] = i < m ? col[i] : 0.0;
-      s = fma(kv[j], kUReg ? u[kUReg ? j : 0] : (i < m ? sh.su[i] : 0.0), s);
+      s = fma(kv[j], kUReg ? u[kUReg ? j : 0] : (i < m ? su[i] : 0.0), s);
     }
   };
   auto finish = [&](int c, const double (&kv)[RPL], double s) {
+    const double bj = bb[c];
     s = warp_sum(s);  // the same bits in every lane
-    const double bj = p.b[c0 + c];
     const double v = bj / s;
 #pragma unroll
     for (int j = 0; j < RPL; ++j) r[j] = fma(kv[j], v, r[j]);
     if (lane == 0) {
-      p.g[c0 + c] = v;
+      gg[c] = v;
       const double d = (v * s) / bj - 1.0;  // first-order form of log(v s) - log b
       e += d * d;
       if (!(v >= kScaleMin && v <= kScaleMax) || !(s >= 1e-300 && s <= 1e300)) bd = 1.0;
@@ -323,7 +341,6 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
     finish(c, k1, s1);
   }
   // fixed tree over the warps: w + h is added into w for h = 8, 4, 2, 1
-  double* tree = sh.area + kResident;
 #pragma unroll 1
   for (int h = NW / 2; h >= 1; h >>= 1) {
     if (w >= h && w < 2 * h)
@@ -339,10 +356,10 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
 #pragma unroll
     for (int j = 0; j < RPL; ++j) {
       const int i = lane + 32 * j;
-      if (i < m) p.rowp[((size_t)buf * p.gp + k) * m + i] = r[j];
+      if (i < m) rp_out[i] = r[j];
     }
   double tt[2] = {e, bd};
-  block_sum_cols<2, NW>(tt, sh.red, par);
+  block_sum_cols<2, NW>(tt, red, par);
   errc = tt[0];
   bad = tt[1];
 }
@@ -356,6 +373,7 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
                                             double& e, double& bd, const Ring* ring, unsigned seq) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const long long ldk = p.ldk;
+  double* const gg = p.g;
   const double bl = lane < nc ? p.b[jb + lane] : 1.0;  // issued before the reduction's barrier
   double kv[REREAD ? 1 : RPT][CW], sum[CW];
 #pragma unroll
@@ -376,7 +394,7 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
   const bool owner = lane < nc;
   const double v_l = owner ? bl / s_l : 0.0;
   if (w == 0 && owner) {
-    p.g[jb + lane] = v_l;
+    gg[jb + lane] = v_l;
     const double d = (v_l * s_l) / bl - 1.0;  // first-order form of log(v s) - log b
     e += d * d;
     if (!(v_l >= kScaleMin && v_l <= kScaleMax) || !(s_l >= 1e-300 && s_l <= 1e300)) bd = 1.0;
@@ -418,24 +436,28 @@ __device__ void final_pass(const Prob& p, int k, int buf, int c0, int c1, const 
     rs[t] = 0.0;
   }
   double s1 = 0.0, s2 = 0.0, l1c = 0.0, l2c = 0.0;
+  const double* const C = p.C;
+  double* const Pp = p.P;
+  double* const gg = p.g;
+  const double* const bb = p.b;
   for (int jb = c0; jb < c1; jb += CW) {
     const int nc = min(CW, c1 - jb);
     double gj[CW], cs[CW];
 #pragma unroll
     for (int c = 0; c < CW; ++c) {
-      gj[c] = c < nc ? eps * log(p.g[jb + c]) : 0.0;
+      gj[c] = c < nc ? eps * log(gg[jb + c]) : 0.0;
       cs[c] = 0.0;
     }
 #pragma unroll
     for (int c = 0; c < CW; ++c) {
       if (c >= nc) continue;
-      const double* cj = p.C + (size_t)(jb + c) * m;
+      const double* cj = C + (size_t)(jb + c) * m;
 #pragma unroll
       for (int t = 0; t < RPT; ++t)
         if (valid[t]) {
           const double cij = cj[tid + t * NTT];
           const double pij = exp(-((cij - f[t]) - gj[c]) / eps);
-          if (p.P) p.P[(size_t)(jb + c) * m + tid + t * NTT] = pij;
+          if (Pp) Pp[(size_t)(jb + c) * m + tid + t * NTT] = pij;
           s1 += cij * pij;
           s2 += pij * (log(pij) - 1.0);
           rs[t] += pij;
@@ -451,8 +473,8 @@ __device__ void final_pass(const Prob& p, int k, int buf, int c0, int c1, const 
           gl = gj[c];
           cl = cs[c];
         }
-      p.g[jb + lane] = gl;
-      const double d = cl - p.b[jb + lane];
+      gg[jb + lane] = gl;
+      const double d = cl - bb[jb + lane];
       l1c += fabs(d);
       l2c += d * d;
     }
@@ -523,7 +545,7 @@ __device__ __forceinline__ double row_update(double ai, double ucur, double tot,
 
 // Sums of the team's partials part[gp][4] (all four columns) in a fixed
 // order, computed by warp 0 and returned to every thread.
-__device__ __forceinline__ void team_sum4(const double* part, int gp, const Shared& sh, double (&t)[4]) {
+__device__ __forceinline__ void team_sum4(const double* part, int gp, const Shared sh, double (&t)[4]) {
   if ((threadIdx.x >> 5) == 0) {
     const int lane = threadIdx.x & 31;
     double x[4] = {0.0, 0.0, 0.0, 0.0};
@@ -544,7 +566,7 @@ __device__ __forceinline__ void team_sum4(const double* part, int gp, const Shar
 
 // Sums of the team's partials part[gp][4] (columns j0, j1) in a fixed order,
 // computed by warp 0 and returned to every thread.
-__device__ __forceinline__ void team_sum2(const double* part, int gp, int j0, int j1, const Shared& sh, double& t0,
+__device__ __forceinline__ void team_sum2(const double* part, int gp, int j0, int j1, const Shared sh, double& t0,
                                           double& t1) {
   if ((threadIdx.x >> 5) == 0) {
     const int lane = threadIdx.x & 31;
@@ -574,12 +596,14 @@ __device__ __forceinline__ void team_sum2(const double* part, int gp, int j0, in
 // parity selects the partial buffers, so a member may run one round ahead of
 // another that is still reading.  Returns false after a failed wait.
 template <int RPT, int CW, bool WARP, bool RES, bool REREAD>
-__device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& sh, unsigned& q, unsigned* dctl,
+__device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh, unsigned& q, unsigned* dctl,
                       volatile unsigned* done, double* pw) {
   const int tid = threadIdx.x;
   const int m = p.m, gp = p.gp;
   const int c0 = strip_begin(p.n, gp, k), c1 = strip_begin(p.n, gp, k + 1);
   const bool redundant = RPT <= 8 && (p.mode & MODE_REDUNDANT) != 0;  // the host sets it for m <= 4096 only
+  const double* const pa = p.a;
+  double* const su = sh.su;
   const unsigned long long t_start = globaltimer_ns();
   int par = 0;
   unsigned nb = 0;
@@ -647,6 +671,16 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
   int rd = 0, iter = 0;
   double err = 1000.0;
   bool unsafe = false;
+  const bool timing = k == 0 && tid == 0;
+  double ph[3] = {0.0, 0.0, 0.0};  // column passes, merges + decisions, team barriers (member 0)
+  unsigned long long tl = timing ? globaltimer_ns() : 0ull;
+  auto lap = [&](int i) {
+    if (timing) {
+      const unsigned long long t = globaltimer_ns();
+      ph[i] += (double)(t - tl);
+      tl = t;
+    }
+  };
   while (true) {
     const int buf = rd & 1;
     const double* rp = p.rowp + (size_t)buf * gp * m;
@@ -664,13 +698,13 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       const double cb = tid < gp ? __ldcg(cp + (size_t)tid * 4 + 1) : 0.0;
       double e = 0.0, bd = 0.0;
       if (WARP) {
-        if (tid < m) un[0] = row_update(p.a[tid], sh.su[tid], row_total(rp, gp, m, tid), init, e, bd);
+        if (tid < m) un[0] = row_update(pa[tid], su[tid], row_total(rp, gp, m, tid), init, e, bd);
       } else {
 #pragma unroll
         for (int t = 0; t < RPT; ++t)
           if (valid[t]) {
             const int i = tid + t * NTT;
-            un[t] = row_update(p.a[i], u[t], row_total(rp, gp, m, i), init, e, bd);
+            un[t] = row_update(pa[i], u[t], row_total(rp, gp, m, i), init, e, bd);
           }
       }
       double tt[4] = {e, bd, ce, cb};
@@ -686,7 +720,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       for (int un_ = k; un_ < p.nunits; un_ += gp) {
         const double tot = merge_unit(rp, gp, m, un_);
         const int i = un_ * kUnit + 4 * (tid >> 5) + (tid & 31);
-        if ((tid & 31) < 4 && i < m) unext[i] = row_update(p.a[i], init ? 1.0 : __ldcg(ucur + i), tot, init, e, bd);
+        if ((tid & 31) < 4 && i < m) unext[i] = row_update(pa[i], init ? 1.0 : __ldcg(ucur + i), tot, init, e, bd);
       }
       double tt[2] = {e, bd};
       block_sum_cols<2, NW>(tt, sh.red, par);
@@ -697,10 +731,12 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
         mp[2] = p.colp[((size_t)buf * gp + k) * 4 + 0];
         mp[3] = p.colp[((size_t)buf * gp + k) * 4 + 1];
       }
+      lap(1);
       if (!team_sync(p, nb, false, dctl, sh, pw)) {
         drain();
         return false;
       }
+      lap(2);
       double t4[4];
       team_sum4(p.mrgp + (size_t)buf * gp * 4, gp, sh, t4);
       er = t4[0];
@@ -710,6 +746,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
     }
     // ---- decision of round rd (the same inputs and order in every member)
     if (k == 0 && tid == 0) atomicAdd(dctl + DC_PROGRESS, 1u);
+    lap(1);
     if (rbad != 0.0 || cbad != 0.0) {
       unsafe = true;
       break;
@@ -724,7 +761,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
     const int nbuf = rd & 1;
     if (redundant) {
       if (WARP) {
-        if (tid < m) sh.su[tid] = un[0];
+        if (tid < m) su[tid] = un[0];
         __syncthreads();
       } else {
 #pragma unroll
@@ -733,7 +770,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
     } else {
       const double* ucur = p.ug + (size_t)nbuf * m;
       if (WARP) {
-        for (int i = tid; i < m; i += NTT) sh.su[i] = __ldcg(ucur + i);
+        for (int i = tid; i < m; i += NTT) su[i] = __ldcg(ucur + i);
         __syncthreads();
       } else {
 #pragma unroll
@@ -786,10 +823,12 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       p.colp[((size_t)nbuf * gp + k) * 4 + 0] = ecol;
       p.colp[((size_t)nbuf * gp + k) * 4 + 1] = bcol;
     }
+    lap(0);
     if (!team_sync(p, nb, false, dctl, sh, pw)) {
       drain();
       return false;
     }
+    lap(2);
   }
   drain();
 
@@ -810,7 +849,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
     for (int i = tid; i < m; i += NTT) us[i] = 0.0;
   } else if (redundant || !WARP) {
     if (WARP) {
-      for (int i = tid; i < m; i += NTT) us[i] = sh.su[i];
+      for (int i = tid; i < m; i += NTT) us[i] = su[i];
     } else if (redundant) {
 #pragma unroll
       for (int t = 0; t < RPT; ++t)
@@ -820,7 +859,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       for (int i = tid; i < m; i += NTT) us[i] = __ldcg(ucur + i);
     }
   } else {
-    for (int i = tid; i < m; i += NTT) us[i] = sh.su[i];
+    for (int i = tid; i < m; i += NTT) us[i] = su[i];
   }
   __syncthreads();
   const int fbuf = (rd + 1) & 1;
@@ -851,6 +890,9 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared& s
       p.res[7] = sqrt(lc2);
       p.res[8] = (double)(globaltimer_ns() - t_start);
       p.res[9] = (double)t_form;
+      p.res[10] = ph[0];
+      p.res[11] = ph[1];
+      p.res[12] = ph[2];
       __threadfence_system();
       done[pi] = 1u;
     }
@@ -1130,13 +1172,13 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   Prob* dprob = (Prob*)scratch(ctx, SBT_DESC, sizeof(Prob) * np);
   double* dK = (double*)scratch(ctx, SBT_K, sizeof(double) * std::max<long long>(kd, 32));
   double* dW = (double*)scratch(ctx, SBT_WORK, sizeof(double) * std::max<long long>(wd, 32));
-  double* dres = (double*)scratch(ctx, SBT_RES, sizeof(double) * 10 * np);
+  double* dres = (double*)scratch(ctx, SBT_RES, sizeof(double) * kResStride * np);
   unsigned* ctrl = (unsigned*)scratch(ctx, SBT_CTRL, sizeof(unsigned) * (8 + 2 + kMaxProbs));
   unsigned* pctl = (unsigned*)scratch(ctx, SBT_PCTL, sizeof(unsigned) * 4 * kMaxProbs);
   const bool profile = option("batch.profile", 0.0) != 0.0;
   double* dprof = profile ? (double*)scratch(ctx, SBT_PROF, sizeof(double) * 4 * G) : nullptr;
   if (!dprob || !dK || !dW || !dres || !ctrl || !pctl || (profile && !dprof)) return RWIG_E_NOMEM;
-  for (int s = 0; s < np; ++s) bind(hp[s], dK + koff[s], dW + woff[s], dres + 10 * (size_t)s, pctl + 4 * s);
+  for (int s = 0; s < np; ++s) bind(hp[s], dK + koff[s], dW + woff[s], dres + kResStride * (size_t)s, pctl + 4 * s);
   unsigned* pub = ctrl + 8;
   unsigned* done = ctrl + 10;
   const unsigned hpub[2] = {(unsigned)np, 1u};
@@ -1144,14 +1186,14 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   RWIG_CUDA_TRY(cudaMemcpyAsync(pub, hpub, sizeof(hpub), cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned) * kMaxProbs, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(pctl, 0, sizeof(unsigned) * 4 * np, st));
-  RWIG_CUDA_TRY(cudaMemsetAsync(dres, 0, sizeof(double) * 10 * np, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(dres, 0, sizeof(double) * kResStride * np, st));
   if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
   const int rc = launch_service(ctx, st, dprob, pub, done, ctrl, dprof, 0ull, (unsigned)np | kClosed);
   if (rc) return rc;
   if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   ++*launches;
-  std::vector<double> hres(10 * (size_t)np);
-  RWIG_CUDA_TRY(cudaMemcpyAsync(hres.data(), dres, sizeof(double) * 10 * np, cudaMemcpyDeviceToHost, st));
+  std::vector<double> hres(kResStride * (size_t)np);
+  RWIG_CUDA_TRY(cudaMemcpyAsync(hres.data(), dres, sizeof(double) * kResStride * np, cudaMemcpyDeviceToHost, st));
   unsigned hctl[4] = {0, 0, 0, 0};
   RWIG_CUDA_TRY(cudaMemcpyAsync(hctl, ctrl, sizeof(hctl), cudaMemcpyDeviceToHost, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1162,11 +1204,11 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
     const int rc2 = print_profile(ctx, dprof, np, kms);
     if (rc2) return rc2;
     // per placement class: problems, member-iterations, solve and formation time, K bytes per member-us
-    struct Agg { int n = 0; double mi = 0, dev = 0, form = 0, bytes = 0, mus = 0; };
+    struct Agg { int n = 0; double mi = 0, dev = 0, form = 0, bytes = 0, mus = 0, it = 0, ph[3] = {0, 0, 0}; };
     Agg agg[4];
     for (int s2 = 0; s2 < np; ++s2) {
       const Prob& d = hp[s2];
-      const double* r = hres.data() + 10 * (size_t)s2;
+      const double* r = hres.data() + kResStride * (size_t)s2;
       const int c = ((d.mode & MODE_RESIDENT) ? 0 : 2) + (d.m > kWarpRows ? 1 : 0);
       agg[c].n += 1;
       agg[c].mi += r[2] * d.gp;
@@ -1174,6 +1216,8 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
       agg[c].form += r[9] * 1e-6;
       agg[c].bytes += r[2] * (double)d.ldk * d.n * 8.0;
       agg[c].mus += (r[8] - r[9]) * 1e-3 * d.gp;
+      agg[c].it += r[2];
+      for (int j = 0; j < 3; ++j) agg[c].ph[j] += r[10 + j] * 1e-3;
     }
     const char* lab[4] = {"resident m<=512", "resident m>512", "streamed m<=512", "streamed m>512"};
     for (int c = 0; c < 4; ++c)
@@ -1183,11 +1227,15 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
                      "%8.2f | member-us per member-iteration %6.2f | GB/s per member %6.1f\n",
                      lab[c], agg[c].n, agg[c].mi, agg[c].dev, agg[c].form,
                      agg[c].mi > 0 ? agg[c].mus / agg[c].mi : 0.0, agg[c].mus > 0 ? agg[c].bytes / agg[c].mus * 1e-3 : 0.0);
+    for (int c = 0; c < 4; ++c)
+      if (agg[c].it > 0)
+        std::fprintf(stderr, "  %-16s per iteration (member 0, us): column pass %.2f | merge + decision %.2f | team barriers %.2f\n",
+                     lab[c], agg[c].ph[0] / agg[c].it, agg[c].ph[1] / agg[c].it, agg[c].ph[2] / agg[c].it);
   }
   for (int s = 0; s < np; ++s) {
     const int i = idx[ord[s]];
     rwig_result& o = out[i];
-    const double* r = hres.data() + 10 * (size_t)s;
+    const double* r = hres.data() + kResStride * (size_t)s;
     if (r[3] == kUnsafeStatus) {
       if (probs[i].C) percall.push_back(i);
       else o.status = RWIG_E_UNSUPPORTED;  // outside the scaling form; the per-call path takes C
@@ -1486,7 +1534,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
   if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
     return fail(e, "done");
-  if ((e = cudaHostAlloc(&s->hres, sizeof(double) * 10 * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
+  if ((e = cudaHostAlloc(&s->hres, sizeof(double) * batch::kResStride * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
     return fail(e, "results");
   if ((e = cudaHostGetDevicePointer(&s->dpub, s->hpub, 0)) != cudaSuccess) return fail(e, "pub map");
   if ((e = cudaHostGetDevicePointer(&s->ddone, s->hdone, 0)) != cudaSuccess) return fail(e, "done map");
@@ -1561,7 +1609,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   d.f = df;
   d.g = dg;
   d.P = dP;
-  bind(d, dk, dw, s->dres + 10 * (size_t)slot, s->dpctl + 4 * (size_t)slot);
+  bind(d, dk, dw, s->dres + batch::kResStride * (size_t)slot, s->dpctl + 4 * (size_t)slot);
   RWIG_CUDA_TRY(cudaMemsetAsync(s->dpctl + 4 * (size_t)slot, 0, sizeof(unsigned) * 4, s->cs));
   s->staged[slot] = d;  // the copy source must outlive the asynchronous copy
   RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &s->staged[slot], sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
@@ -1601,7 +1649,7 @@ extern "C" int rwig_server_poll(rwig_server* s, int ticket, rwig_result* out) {
   }
   std::atomic_thread_fence(std::memory_order_seq_cst);
   auto& sl = s->slots[slot];
-  const double* r = s->hres + 10 * (size_t)slot;
+  const double* r = s->hres + batch::kResStride * (size_t)slot;
   *out = rwig_result{};
   if (r[3] == batch::kUnsafeStatus) {
     out->status = RWIG_E_UNSUPPORTED;  // outside the scaling form: solve with rwig_sinkhorn_log
