@@ -78,7 +78,7 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "batch.max_team": largest team of CTAs per batched problem (default:
  *       half the SM count);
  *   "batch.resident_team": problems with M > 512 keep their K strips in
- *       shared memory when that takes at most this many CTAs (default 16),
+ *       shared memory when that takes at most this many CTAs (default 32),
  *       else stream strips of about "batch.stream_strip_kb" (default 1024)
  *       from memory every iteration;
  *   "batch.redundant_rows": teams with gp * M up to this (and M <= 4096)

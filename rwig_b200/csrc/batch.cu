@@ -108,13 +108,14 @@ struct Shared {
   double* su;        // kWarpRows doubles: u in warp mode
   double* red;       // 2 * NW * 16 doubles: block reductions
   double* dec;       // 8 doubles: values broadcast to the CTA
+  double* tim;       // 4 doubles: thread 0's phase timers
   int* flag;         // 4 ints
 };
 
 // dynamic shared memory of one CTA
 __host__ __device__ constexpr size_t smem_bytes() {
-  return (size_t)kArea * 8 + 64 + (size_t)kWarpRows * 8 + (size_t)2 * NW * 16 * 8 + 8 * 8 + 4 * 4 + sizeof(Prob) +
-         64;
+  return (size_t)kArea * 8 + 64 + (size_t)kWarpRows * 8 + (size_t)2 * NW * 16 * 8 + 8 * 8 + 4 * 8 + 4 * 4 +
+         sizeof(Prob) + 64;
 }
 
 __device__ __forceinline__ int strip_begin(int n, int gp, int k) { return (int)(((long long)k * n) / gp); }
@@ -671,14 +672,18 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
   int rd = 0, iter = 0;
   double err = 1000.0;
   bool unsafe = false;
+  // phase timers of member 0 (column passes, merges + decisions, team
+  // barriers), kept by thread 0 in shared memory: tim[3] holds the last stamp
   const bool timing = k == 0 && tid == 0;
-  double ph[3] = {0.0, 0.0, 0.0};  // column passes, merges + decisions, team barriers (member 0)
-  unsigned long long tl = timing ? globaltimer_ns() : 0ull;
+  if (timing) {
+    sh.tim[0] = sh.tim[1] = sh.tim[2] = 0.0;
+    sh.tim[3] = (double)globaltimer_ns();
+  }
   auto lap = [&](int i) {
     if (timing) {
-      const unsigned long long t = globaltimer_ns();
-      ph[i] += (double)(t - tl);
-      tl = t;
+      const double t = (double)globaltimer_ns();
+      sh.tim[i] += t - sh.tim[3];
+      sh.tim[3] = t;
     }
   };
   while (true) {
@@ -890,9 +895,9 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
       p.res[7] = sqrt(lc2);
       p.res[8] = (double)(globaltimer_ns() - t_start);
       p.res[9] = (double)t_form;
-      p.res[10] = ph[0];
-      p.res[11] = ph[1];
-      p.res[12] = ph[2];
+      p.res[10] = sh.tim[0];
+      p.res[11] = sh.tim[1];
+      p.res[12] = sh.tim[2];
       __threadfence_system();
       done[pi] = 1u;
     }
@@ -961,7 +966,8 @@ __global__ void __launch_bounds__(NTT, 1) service_kernel(const Prob* probs, cons
   sh.su = reinterpret_cast<double*>(smem + (size_t)kArea * 8 + 64);
   sh.red = sh.su + kWarpRows;
   sh.dec = sh.red + 2 * NW * 16;
-  sh.flag = reinterpret_cast<int*>(sh.dec + 8);
+  sh.tim = sh.dec + 8;
+  sh.flag = reinterpret_cast<int*>(sh.tim + 4);
   Prob* sp = reinterpret_cast<Prob*>(sh.flag + 4);
   const int tid = threadIdx.x, cta = blockIdx.x;
   if (tid == 0) {
@@ -1051,7 +1057,7 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
   const int gp_res = (int)((q.N + cols - 1) / cols);
   const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)(G / 2))));
-  const int res_team = std::min(maxteam, (int)option("batch.resident_team", 16.0));
+  const int res_team = std::min(maxteam, (int)option("batch.resident_team", 32.0));
   int mode = 0;
   if (gp_res <= res_team || (q.M <= kWarpRows && gp_res <= maxteam)) {
     mode |= MODE_RESIDENT;
