@@ -7,7 +7,8 @@ zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
 --workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)),
 --workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50),
 --workload wdl5000 (WDL training steps, V = 5000, K = 16, batch 64, L = 20, Adam),
---workload stream (200 mixed-size log-Sinkhorn requests, batched vs per call).
+--workload stream (200 mixed-size log-Sinkhorn requests, batched vs per call),
+--workload sinkgrad2048 (log-Sinkhorn 2048 x 2048 with its gradient w.r.t. a, L = 100).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
@@ -720,7 +721,7 @@ class StreamWorkload:
         achieved = alg / (batch_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "peak_source": src,
-                "kernel": "batch_kernel (one CTA per problem) + per-call path for the largest",
+                "kernel": "service_kernel (a team of CTAs per problem)",
                 "alg_bytes": alg, "note": "K read once per iteration plus the K build and final passes; "
                                            "small problems stay in L2, so frac may exceed 1"}
         in_kernel = sum(1 for r in bres if r["path"] == 0)
@@ -823,12 +824,146 @@ class StreamWorkload:
         raise NotImplementedError
 
 
+class GradWorkload:
+    """One log-Sinkhorn solve with a fixed unroll depth plus its gradient with
+    respect to a per step: the forward records every iteration's potentials,
+    one cooperative launch runs the L backward steps."""
+
+    higher_is_better = True
+
+    def __init__(self, m=2048, n=2048, reg=0.05, L=100):
+        self.m, self.n, self.reg, self.L = m, n, reg, L
+        self.unit = "solves/s"
+        self.metric = f"log-Sinkhorn solve + gradient w.r.t. a per second ({m}x{n}, L={L}, FP64)"
+        self.desc = (f"log-Sinkhorn {m}x{n} FP64 with grad_a, Dirichlet(0.5) marginals, uniform points in [0,1]^2, "
+                     f"squared-Euclidean cost / max, eps={reg:g}, L={L} unrolled iterations (tol 0), "
+                     f"outputs f, g, loss, grad_a")
+
+    def inputs(self):
+        from rwig_b200 import synth
+        return synth.sinkhorn_problem(self.m, self.n, 0.5, 2)
+
+    def cpu_seconds(self, threads):
+        """CPU port time of one step: runs with 2 and 4 unrolled iterations
+        (forward + backward), extrapolated to L."""
+        import oracle
+        a, b, C = self.inputs()
+        t = {}
+        for it in (2, 4):
+            t0 = time.perf_counter()
+            oracle.sinkhorn_log(a, b, C, self.reg, with_grad=True, max_iter=it, zero_tol=0.0, n_threads=threads)
+            t[it] = time.perf_counter() - t0
+        per_iter = max((t[4] - t[2]) / 2, 1e-9)
+        fixed = max(t[2] - 2 * per_iter, 0.0)
+        sample = (f"2- and 4-iteration runs with gradient of the same {self.m}x{self.n} problem ({threads} threads "
+                  f"forward, backward serial as in the reference), extrapolated to L={self.L}: "
+                  f"{per_iter * 1e3:.0f} ms per forward+backward iteration")
+        return fixed + self.L * per_iter, threads, sample
+
+    def run(self, args, dev, world, rank, clocks_cls):
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        m, n = self.m, self.n
+        a, b, C = self.inputs()
+        ta, tb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        tC = torch.from_numpy(C.T).to(dev)
+        f = torch.empty(m, dtype=torch.float64, device=dev)
+        g = torch.empty(n, dtype=torch.float64, device=dev)
+        ga = torch.empty(m, dtype=torch.float64, device=dev)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+        stream = torch.cuda.current_stream()
+
+        def step():
+            return rw.sinkhorn_log_device(ta, tb, tC, self.reg, self.L, 0.0, f=f, g=g, grad_a=ga, stream=stream)
+
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        torch.cuda.synchronize()
+        times, reps = [], []
+        with clocks_cls(dev.index) as clocks:
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                reps.append(rw.last_report())
+            torch.cuda.synchronize()
+        tot_ms = max_over_ranks(sum(times), world, dev)
+        # end to end through the host-pointer entry with pinned buffers
+        hC = torch.from_numpy(C.T.copy()).pin_memory()
+        ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+        hf, hg, hga = (torch.empty(k, dtype=torch.float64).pin_memory() for k in (m, n, m))
+        L = _lib.load()
+        dp = ctypes.POINTER(ctypes.c_double)
+
+        def cp(t):
+            return ctypes.cast(ctypes.c_void_p(t.data_ptr()), dp)
+
+        def host_step():
+            loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+            _lib.check(L.rwig_sinkhorn_log(None, cp(hga), cp(hf), cp(hg), ctypes.byref(loss), ctypes.byref(it),
+                                           ctypes.byref(err), cp(ha), cp(hb), cp(hC), m, n, self.reg, 1, self.L, 0.0))
+
+        host_step()
+        e2e_s = 0.0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            host_step()
+            e2e_s += time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, world, dev)
+        assert np.array_equal(hga.numpy(), ga.cpu().numpy()), "host and device gradients disagree"
+        if rank != 0:
+            return None
+        peak, peak_kind = measured_peaks()
+        gms = sum(r["grad_ms"] for r in reps) / len(reps)
+        # backward kernel: one read of the m x n cost per unrolled step
+        alg = self.L * m * n * 8.0
+        achieved = alg / (gms / 1e3) / 1e9 if gms > 0 else None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": None, "peak_source": peak_kind,
+                "kernel": "grad_kernel (unrolled backward, 2 exp per element per step)",
+                "kernel_ms_per_step": gms, "alg_bytes_per_step": alg,
+                "forward_ms_per_step": tot_ms / args.steps - gms}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1)
+            cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
+        return {"value": args.steps * world / (tot_ms / 1e3), "ms_per_step": tot_ms / args.steps,
+                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
+                           "l2": "flushed between steps (256 MB write)"},
+                "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
+                        "h2d_bytes_per_step": (m * n + m + n) * 8, "d2h_bytes_per_step": (2 * m + n) * 8},
+                "gpu_launches": sum(r["kernel_launches"] for r in reps), "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clocks.summary()}
+
+    def reference(self, args):
+        threads = os.cpu_count() or 1
+        for _ in range(args.warmup):
+            self.cpu_seconds(threads)
+        secs, cores, sample = [], 1, ""
+        for _ in range(args.steps):
+            s_, cores, sample = self.cpu_seconds(threads)
+            secs.append(s_)
+        return sum(secs), cores, sample
+
+
 WORKLOADS = {
     "log4096": SinkhornWorkload("log", 4096, 4096, 0.01, 0.5, 2000, 1e-9),
     "vanilla256": SinkhornWorkload("vanilla", 256, 256, 0.1, 1.0, 1000, 1e-9),
     "barycenter2048": BarycenterWorkload(),
     "wdl5000": WdlWorkload(),
     "stream": StreamWorkload(),
+    "sinkgrad2048": GradWorkload(),
 }
 
 

@@ -55,6 +55,7 @@ typedef struct rwig_report {
   int support_m;         /* rows kept after dropping zero-mass entries of a */
   int support_n;         /* columns kept after dropping zero-mass entries of b */
   double bary_norm;      /* barycenters: sum of the un-normalised barycenter b */
+  double grad_ms;        /* Sinkhorn with withgrad: device time of the backward launch */
 } rwig_report;
 
 /* ---- context ---------------------------------------------------------- */

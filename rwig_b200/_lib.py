@@ -54,6 +54,7 @@ class Report(ctypes.Structure):
         ("support_m", _i),
         ("support_n", _i),
         ("bary_norm", _d),
+        ("grad_ms", _d),
     ]
 
     def as_dict(self):

@@ -352,33 +352,36 @@ def _ptr(t):
 
 
 def sinkhorn_vanilla_device(a, b, C_cm, reg, max_iter=1000, zero_tol=1e-6, P=None, u=None, v=None,
-                            stream=None) -> dict:
-    """Vanilla Sinkhorn on device buffers (layout as sinkhorn_log_device)."""
+                            stream=None, grad_a=None) -> dict:
+    """Vanilla Sinkhorn on device buffers (layout as sinkhorn_log_device);
+    grad_a (M, device) receives the gradient w.r.t. a when given."""
     M, N = a.shape[0], b.shape[0]
     if C_cm.numel() != M * N:
         raise ValueError("C must hold M*N entries")
     loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
     st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
-    rc = _lib.load().rwig_sinkhorn_vanilla_dev(_ptr(P), None, _ptr(u), _ptr(v), ctypes.byref(loss),
+    rc = _lib.load().rwig_sinkhorn_vanilla_dev(_ptr(P), _ptr(grad_a), _ptr(u), _ptr(v), ctypes.byref(loss),
                                                ctypes.byref(it), ctypes.byref(err), _ptr(a), _ptr(b),
-                                               _ptr(C_cm), M, N, float(reg), 0, int(max_iter),
+                                               _ptr(C_cm), M, N, float(reg), int(grad_a is not None), int(max_iter),
                                                float(zero_tol), st)
     _lib.check(rc)
     return {"loss": loss.value, "iter": it.value, "err": err.value, "return_status": rc}
 
 
 def sinkhorn_log_device(a, b, C_cm, reg, max_iter=1000, zero_tol=1e-6, P=None, f=None, g=None,
-                        stream=None) -> dict:
+                        stream=None, grad_a=None) -> dict:
     """Log-Sinkhorn on device buffers.  C_cm is the M x N cost in column-major
-    order, i.e. a contiguous (N, M) tensor holding C^T row-major; P likewise."""
+    order, i.e. a contiguous (N, M) tensor holding C^T row-major; P likewise.
+    grad_a (M, device) receives the gradient w.r.t. a when given."""
     M, N = a.shape[0], b.shape[0]
     if C_cm.numel() != M * N:
         raise ValueError("C must hold M*N entries")
     loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
     st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
-    rc = _lib.load().rwig_sinkhorn_log_dev(_ptr(P), None, _ptr(f), _ptr(g), ctypes.byref(loss),
+    rc = _lib.load().rwig_sinkhorn_log_dev(_ptr(P), _ptr(grad_a), _ptr(f), _ptr(g), ctypes.byref(loss),
                                            ctypes.byref(it), ctypes.byref(err), _ptr(a), _ptr(b),
-                                           _ptr(C_cm), M, N, float(reg), 0, int(max_iter), float(zero_tol),
+                                           _ptr(C_cm), M, N, float(reg), int(grad_a is not None), int(max_iter),
+                                           float(zero_tol),
                                            st)
     _lib.check(rc)
     return {"loss": loss.value, "iter": it.value, "err": err.value, "return_status": rc}

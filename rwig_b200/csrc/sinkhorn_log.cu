@@ -726,6 +726,7 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   if (M < 1 || N < 1) return set_error(RWIG_E_INVALID, "M and N must be >= 1");
   if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
   const bool want_grad = withgrad && grad_a;
+  double grad_ms = 0.0;
   if (want_grad && max_iter < 0) return set_error(RWIG_E_INVALID, "max_iter must be >= 0");
   int launches = 0;
 
@@ -1081,9 +1082,15 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   if (want_grad) {
     // vanilla: K = exp(-C/eps) is the kernel the scalings were computed on
     const double* Kv = vanilla ? (const double*)scratch(ctx, SL_KT, sizeof(double) * ldc * n) : nullptr;
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->evs0, st));
     rc = sinkhorn_grad(ctx, st, vanilla, Cr, Kv, ldc, ar, br, loga, logb, fh, gh, m, n, (int)res[0], reg, d_ridx, M,
                        vanilla ? 1.0 : reg, grad_a, &launches);
     if (rc != 0) return rc;
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->evs1, st));
+    RWIG_CUDA_TRY(cudaEventSynchronize(ctx->evs1));
+    float gms = 0.f;
+    cudaEventElapsedTime(&gms, ctx->evs0, ctx->evs1);
+    grad_ms = gms;
   }
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   RWIG_CUDA_TRY(cudaEventSynchronize(ctx->ev1));
@@ -1112,6 +1119,7 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   R.kernel_launches = launches;
   R.support_m = m;
   R.support_n = n;
+  R.grad_ms = grad_ms;
   return status;
 }
 
