@@ -1035,6 +1035,43 @@ def run_single(args):
 
     import rwig_b200 as rw
     from rwig_b200 import synth
+    if args.workload.startswith("sinkgrad"):
+        # two log-Sinkhorn solves with gradient, --m x --n, --iters unrolled iterations
+        dev = torch.device("cuda", 0)
+        a, b, C = synth.sinkhorn_problem(args.m, args.n, 0.5, 2)
+        ta, tb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        tC = torch.from_numpy(C.T.copy()).to(dev)
+        ga = torch.empty(args.m, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            r = rw.sinkhorn_log_device(ta, tb, tC, 0.05, args.iters, 0.0, grad_a=ga)
+        torch.cuda.synchronize()
+        rep = rw.last_report()
+        print(json.dumps({"m": args.m, "n": args.n, "iter": r["iter"], "device_ms": rep["device_ms"],
+                          "grad_ms": rep["grad_ms"], "launches": rep["kernel_launches"]}))
+        return 0
+    if args.workload == "stream":
+        # two batched calls of --iters fixed iterations: one streamed 2048 x 2048
+        # problem, then 64 resident 300 x 1500 problems
+        from rwig_b200 import _lib
+        dev = torch.device("cuda", 0)
+        L = _lib.load()
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        for cases in ([(2048, 2048)], [(300, 1500)] * 64):
+            keep, arr = [], (_lib.Problem * len(cases))()
+            for k, (m, n) in enumerate(cases):
+                a, b, C = synth.sinkhorn_problem(m, n, 1.0, salt=k + 1)
+                t = [torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev),
+                     torch.from_numpy(np.ascontiguousarray(C.T)).to(dev),
+                     torch.empty(m, dtype=torch.float64, device=dev), torch.empty(n, dtype=torch.float64, device=dev)]
+                keep.append(t)
+                arr[k] = _lib.Problem(vp(t[0]), vp(t[1]), vp(t[2]), m, n, 0.05, args.iters, 0.0, None, vp(t[3]),
+                                      vp(t[4]))
+            res = (_lib.Result * len(cases))()
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(arr, len(cases), res, None))
+            rep = rw.last_report()
+            print(json.dumps({"problems": len(cases), "m": cases[0][0], "n": cases[0][1], "iter": res[0].iter,
+                              "device_ms": rep["device_ms"], "launches": rep["kernel_launches"]}))
+        return 0
     if args.workload.startswith("wdl"):
         # one batched WDL gradient step on device buffers: V = --n words,
         # --s topics, --m documents, --iters iterations

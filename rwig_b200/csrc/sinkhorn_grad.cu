@@ -31,6 +31,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "fastexp.cuh"
 #include "sk_common.cuh"
 #include "sk_host.h"
 
@@ -63,7 +64,11 @@ struct Params {
 
 template <int RPT, int CW, bool VAN>
 __global__ void __launch_bounds__(NTT, 1) grad_kernel(Params p) {
-  extern __shared__ __align__(16) double red[];  // [2][NW][CW]
+  extern __shared__ __align__(16) double red[];  // [2][NW][max(CW, 32)], then the 2^(j/64) table
+  double* tbl = red + 2 * NW * (CW > 32 ? CW : 32);
+  load_exp_table_spread(tbl);
+  __syncthreads();
+  const double* tbl_l = tbl + (threadIdx.x & (kExpTableSpread - 1));
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, cta = blockIdx.x, G = p.G;
   const int m = p.m, n = p.n;
   const double eps = p.eps, inv_eps = 1.0 / eps;
@@ -131,7 +136,9 @@ __global__ void __launch_bounds__(NTT, 1) grad_kernel(Params p) {
               s[t] += pb;
               term = pb;
             } else {
-              term = exp(((ra[t] + gl[c]) - cij[t][c]) * inv_eps) * rx[t];   // X_ij fbar_i
+              // X_ij fbar_i; the table exponential (within 2 ulp, arguments below
+              // -708 give 3e-308, negligible in this sum)
+              term = exp_tbl<kExpTableSpread>(((ra[t] + gl[c]) - cij[t][c]) * inv_eps, tbl_l) * rx[t];
             }
           } else {
             if (last) {
@@ -157,7 +164,7 @@ __global__ void __launch_bounds__(NTT, 1) grad_kernel(Params p) {
         for (int t = 0; t < RPT; ++t) {
           if (!valid[t]) continue;
           if (!VAN) {
-            const double W = exp(((rb[t] + gl[c]) - cij[t][c]) * inv_eps - p.logb[j]);
+            const double W = exp_tbl<kExpTableSpread>(((rb[t] + gl[c]) - cij[t][c]) * inv_eps - p.logb[j], tbl_l);
             r[t] += W * col;
           } else if (last) {
             const double P = (rb[t] * kij[VAN ? t : 0][VAN ? c : 0]) * gl[c];
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(NTT, 1) grad_kernel(Params p) {
 template <int RPT, int CW, bool VAN>
 int launch_t(Context* ctx, Params& p, cudaStream_t st) {
   auto kern = grad_kernel<RPT, CW, VAN>;
-  const size_t smem = sizeof(double) * std::max(2 * NW * CW, 2 * NW * 32);
+  const size_t smem = sizeof(double) * (2 * NW * std::max(CW, 32) + 64 * kExpTableSpread);
   int nblk = 0;
   RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, kern, NTT, smem));
   if (nblk < 1) return set_error(RWIG_E_UNSUPPORTED, "gradient kernel does not fit on an SM");
