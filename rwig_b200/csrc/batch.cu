@@ -77,7 +77,8 @@ constexpr int kResStride = 16;  // doubles of results per problem
 enum : int { MODE_RESIDENT = 1, MODE_WARP = 2, MODE_REDUNDANT = 4, MODE_KEEP_L2 = 8 };
 
 // Device control words of a launch.
-enum : int { DC_AVAIL = 0, DC_HEAD = 1, DC_ERR = 2, DC_PROGRESS = 3, DC_ACTIVE = 4 };
+enum : int { DC_AVAIL = 0, DC_HEAD = 1, DC_ERR = 2, DC_PROGRESS = 3, DC_ACTIVE = 4, DC_FREE = 5, DC_OLDEST = 6,
+             DC_OLDEST_T = 7 };
 
 struct Prob {
   const double* a;
@@ -95,7 +96,7 @@ struct Prob {
   double* colp;      // [2][gp][4] column-strip partials
   double* mrgp;      // [2][gp][4] merge partials (split merges)
   double* ug;        // [2][m] u (split merges)
-  unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals
+  unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals, [2] 0 unopened, 1 opened, 2 opening
   double* res;       // [16]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, formation
                      // ns, then member 0's ns in column passes, merges + decisions, team barriers
   int m, n, max_iter, gp, mode, nunits;
@@ -905,20 +906,41 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
   return true;
 }
 
-// Claim of the next member slot (thread 0): the oldest published problem
-// whose team is incomplete.  Returns the problem and member index, or pi = -1
-// when the launch is closing (or on an error).  The published count is taken
-// from pub[0] until the launch closes (stop flag, or idle_ns with nothing to
-// claim and no team running); after that it is frozen, so a member never
-// waits for CTAs that have left.
+// Claim of a member slot (thread 0).  Team formation with reservation:
+// F = (CTAs looking for work) - (unfilled slots of opened problems) never goes
+// below zero.  A CTA that starts looking adds one to F; it first takes an
+// unfilled slot of an opened problem; else it opens one -- the oldest
+// unopened problem, or (backfilling, while that one has waited less than
+// backfill_us) a later one in a window of kBackfillWindow -- by taking the
+// problem's gp from F with a compare-and-swap.  So every opened team has
+// enough free CTAs to fill it and no team waits on CTAs that are busy
+// elsewhere.  Returns the problem and member index, or pi = -1 when the launch
+// is closing (or on an error).  The published count is taken from pub[0]
+// until the launch closes (stop flag, or idle_ns with nothing to do and no
+// team running); after that it is frozen.
+constexpr int kBackfillWindow = 64;
+constexpr int kScanWindow = 256;  // problems from the scan start examined per pass
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned* problem_ctl(const Prob* probs, unsigned h) {
+  return reinterpret_cast<unsigned*>(__ldcg(reinterpret_cast<const unsigned long long*>(&probs[h].ctl)));
+}
+
 __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned* dctl, unsigned long long idle_ns,
-                      int& pi, int& k) {
+                      unsigned backfill_us, int& pi, int& k) {
   pi = -1;
   k = -1;
+  int* F = reinterpret_cast<int*>(dctl + DC_FREE);
+  atomicAdd(F, 1);
   const unsigned long long t_idle = globaltimer_ns();
   while (true) {
-    if (*(volatile unsigned*)(dctl + DC_ERR) != 0u) return;
-    const unsigned W = *(volatile unsigned*)(dctl + DC_AVAIL);
+    if (ld_relaxed(dctl + DC_ERR) != 0u) return;
+    const unsigned W = ld_relaxed(dctl + DC_AVAIL);
     const unsigned npx = W & ~kClosed;
     if (!(W & kClosed)) {
       const unsigned p0 = min(pub[0], (unsigned)kMaxProbs);
@@ -927,24 +949,86 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
         continue;
       }
     }
-    for (unsigned h = *(volatile unsigned*)(dctl + DC_HEAD); h < npx; ++h) {
-      const int gp = __ldcg(&probs[h].gp);
-      unsigned* ctl = reinterpret_cast<unsigned*>(__ldcg(reinterpret_cast<const unsigned long long*>(&probs[h].ctl)));
-      const unsigned c = atomicAdd(ctl, 1u);
-      if ((int)c < gp) {
-        if ((int)c == gp - 1) atomicMax(dctl + DC_HEAD, h + 1);
-        pi = (int)h;
-        k = (int)c;
-        return;
+    // 1. an unfilled slot of an opened problem; states and claim counts are
+    // read 8 problems at a time (the loads overlap)
+    const unsigned head = ld_relaxed(dctl + DC_HEAD);
+    const unsigned end = min(npx, head + kScanWindow);
+    unsigned oldest = npx;  // oldest problem not yet opened
+    bool open_slots = false, prefix_full = true;
+    for (unsigned h0 = head; h0 < end; h0 += 8) {
+      unsigned st[8], cl[8];
+      int gp[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const unsigned h = h0 + u;
+        unsigned* ctl = h < end ? problem_ctl(probs, h) : nullptr;
+        st[u] = ctl ? ld_relaxed(ctl + 2) : 1u;
+        cl[u] = ctl ? ld_relaxed(ctl) : 0u;
+        gp[u] = h < end ? __ldcg(&probs[h].gp) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const unsigned h = h0 + u;
+        if (h >= end) break;
+        if (st[u] == 1u) {
+          if ((int)cl[u] < gp[u]) {
+            open_slots = true;
+            const unsigned c = atomicAdd(problem_ctl(probs, h), 1u);
+            if ((int)c < gp[u]) {
+              pi = (int)h;
+              k = (int)c;
+              return;
+            }
+          } else if (prefix_full) {
+            atomicMax(dctl + DC_HEAD, h + 1);  // opened and full up to here: later scans start after it
+          }
+        } else {
+          prefix_full = false;
+          if (oldest == npx) oldest = h;
+        }
+        if (st[u] == 1u && (int)cl[u] < gp[u]) prefix_full = false;
       }
     }
-    if (W & kClosed) return;
-    const bool idle = globaltimer_ns() - t_idle > idle_ns && *(volatile unsigned*)(dctl + DC_ACTIVE) == 0u;
-    if (pub[1] != 0u || idle) {
-      atomicCAS(dctl + DC_AVAIL, W, W | kClosed);
-      continue;
+    // 2. open a problem
+    if (oldest < npx) {
+      const unsigned now_us = (unsigned)(globaltimer_ns() / 1000ull);
+      if (ld_relaxed(dctl + DC_OLDEST) != oldest + 1u) {
+        atomicExch(dctl + DC_OLDEST_T, now_us);
+        atomicExch(dctl + DC_OLDEST, oldest + 1u);
+      }
+      const bool backfill = now_us - ld_relaxed(dctl + DC_OLDEST_T) < backfill_us;
+      bool opened = false;
+      for (unsigned h = oldest; h < end && h < oldest + kBackfillWindow && !opened; ++h) {
+        if (h != oldest && !backfill) break;
+        unsigned* ctl = problem_ctl(probs, h);
+        if (ld_relaxed(ctl + 2) != 0u) continue;
+        const int gp = __ldcg(&probs[h].gp);
+        if (gp > (int)ld_relaxed(reinterpret_cast<unsigned*>(F))) continue;
+        if (atomicCAS(ctl + 2, 0u, 2u) != 0u) continue;  // another CTA is opening it
+        while (true) {
+          const int f = (int)ld_relaxed(reinterpret_cast<unsigned*>(F));
+          if (f < gp) break;
+          if (atomicCAS(F, f, f - gp) == f) {
+            opened = true;
+            break;
+          }
+        }
+        atomicExch(ctl + 2, opened ? 1u : 0u);
+      }
+      if (opened) continue;
     }
-    __nanosleep(1000);
+    // 3. nothing to take now
+    if (W & kClosed) {
+      if (oldest == npx && !open_slots && end == npx) return;  // everything published is opened and full
+    } else {
+      const bool idle = oldest == npx && !open_slots && globaltimer_ns() - t_idle > idle_ns &&
+                        ld_relaxed(dctl + DC_ACTIVE) == 0u;
+      if (pub[1] != 0u || idle) {
+        atomicCAS(dctl + DC_AVAIL, W, W | kClosed);
+        continue;
+      }
+    }
+    __nanosleep(500);
   }
 }
 
@@ -958,7 +1042,7 @@ int __host__ __device__ row_class(int m) { return m <= 512 ? 0 : m <= 1024 ? 1 :
 // [2] claim ns, [3] member slots solved.
 __global__ void __launch_bounds__(NTT, 1) service_kernel(const Prob* probs, const volatile unsigned* pub,
                                                           volatile unsigned* done, unsigned* dctl, double* prof,
-                                                          unsigned long long idle_ns) {
+                                                          unsigned long long idle_ns, unsigned backfill_us) {
   extern __shared__ __align__(128) unsigned char smem[];
   Shared sh;
   sh.area = reinterpret_cast<double*>(smem);
@@ -982,7 +1066,7 @@ __global__ void __launch_bounds__(NTT, 1) service_kernel(const Prob* probs, cons
     const unsigned long long t0 = globaltimer_ns();
     if (tid == 0) {
       int pi, k;
-      claim(probs, pub, dctl, idle_ns, pi, k);
+      claim(probs, pub, dctl, idle_ns, backfill_us, pi, k);
       sh.flag[1] = pi;
       sh.flag[2] = k;
       if (pi >= 0) {
@@ -1125,7 +1209,8 @@ int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, cons
   unsigned* ctl = dctl;
   double* pr = dprof;
   unsigned long long idle = idle_ns;
-  void* args[] = {(void*)&dp, (void*)&pb, (void*)&dn, (void*)&ctl, (void*)&pr, (void*)&idle};
+  unsigned bf = (unsigned)std::max(0.0, option("batch.backfill_us", 5000.0));
+  void* args[] = {(void*)&dp, (void*)&pb, (void*)&dn, (void*)&ctl, (void*)&pr, (void*)&idle, (void*)&bf};
   RWIG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)service_kernel, dim3(ctx->sm_count), dim3(NTT), args,
                                             smem_bytes(), st));
   return 0;
