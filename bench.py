@@ -770,7 +770,7 @@ class StreamWorkload:
             _, _, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
             pts.append((np.asfortranarray(x), np.asfortranarray(y)))
         lat = np.zeros(R)
-        with rw.Server(mem_budget_bytes=64e9, idle_ms=5.0) as srv:
+        with rw.Server(mem_budget_bytes=64e9, idle_ms=200.0) as srv:
             pending, idx, done = {}, 0, 0
             t0 = time.perf_counter()
             while done < R:

@@ -252,13 +252,16 @@ RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_
  * No counterpart in the reference.  A server keeps one service launch of the
  * batched kernel running while requests arrive: rwig_server_submit copies a
  * request (host pointers; M <= 8192) to the device and publishes it to the
- * running kernel, which admits it at its next iteration and iterates it
- * together with the others; rwig_server_poll returns 1 once the request is
+ * running kernel, where free CTAs form its team as soon as enough are free
+ * and solve it beside the others; rwig_server_poll returns 1 once the request is
  * finished (f, g and P copied to the pointers given at submit; out filled),
  * 0 while it runs.  submit returns the request's ticket (>= 0), or
  * RWIG_E_BUSY when admitting it would exceed the device-memory budget or the
  * slot table (512 requests) is full -- poll and retry.  The kernel ends after
- * idle_ms without work and is restarted by the next submit or poll.
+ * idle_ms without work and is restarted by the next submit or poll; while it
+ * runs it holds every SM, and a restart delays the requests that wait for it,
+ * so sparse arrivals want idle_ms well above the gap between requests (at
+ * 300 requests/s the p99 latency was 582 ms with 5 ms, 111 ms with 500 ms).
  * Results are bitwise those of rwig_batch_sinkhorn_log for the same problem.
  * One thread drives a server. */
 typedef struct rwig_server rwig_server;

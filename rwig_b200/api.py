@@ -288,7 +288,7 @@ class Server:
     admits a request into the running service kernel, poll() returns its
     result once finished.  One thread drives a server."""
 
-    def __init__(self, mem_budget_bytes=8e9, idle_ms=2.0):
+    def __init__(self, mem_budget_bytes=8e9, idle_ms=50.0):
         self._L = _lib.load()
         h = ctypes.c_void_p()
         _lib.check(self._L.rwig_server_create(ctypes.byref(h), float(mem_budget_bytes), float(idle_ms)))
