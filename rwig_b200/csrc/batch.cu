@@ -422,81 +422,6 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
   }
 }
 
-// Column pass of one round, thread per row (RPT rows per thread, groups of
-// CW columns): u from usrc (shared memory, or global memory written by other
-// members when u_global), v -> g, row partials -> rowp_out, the column error
-// and range flag -> ecol, bcol.  Streamed strips run the stage ring (q0: the
-// problem's first stage; q, issued: consumed and issued stages).  A function
-// of its own, so that its registers do not carry the solver's state.
-// Returns false after a failed copy wait (error word set).
-template <int RPT, int CW, bool REREAD, bool RES>
-__device__ __noinline__ bool block_pass(const Prob& p, const double* usrc, bool u_global, double* rowp_out, int c0,
-                                        int c1, const Shared sh, unsigned q0, unsigned* qp, unsigned* issuedp,
-                                        int* parp, double* ecol, double* bcol, unsigned* dctl) {
-  const int tid = threadIdx.x;
-  const int m = p.m;
-  const long long ldk = p.ldk;
-  bool valid[RPT];
-  double u[RPT], r[RPT];
-#pragma unroll
-  for (int t = 0; t < RPT; ++t) {
-    const int i = tid + t * NTT;
-    valid[t] = i < m;
-    u[t] = valid[t] ? (u_global ? __ldcg(usrc + i) : usrc[i]) : 0.0;
-    r[t] = 0.0;
-  }
-  int par = *parp;
-  double e = 0.0, bd = 0.0;
-  bool ok = true;
-  if (RES) {
-    for (int jb = c0; jb < c1; jb += CW)
-      block_group<RPT, CW, REREAD>(p, sh.area + (size_t)(jb - c0) * ldk + tid, jb, min(CW, c1 - jb), u, r, valid,
-                                   sh.red, par, e, bd, nullptr, 0u);
-  } else {
-    Ring ring{};
-    ring.buf = sh.area;
-    ring.bar = sh.bar;
-    ring.pol = (p.mode & MODE_KEEP_L2) ? l2_policy_evict_last() : l2_policy_evict_first();
-    ring.K = p.K;
-    ring.ldk = ldk;
-    ring.c0 = c0;
-    ring.c1 = c1;
-    ring.cw = CW;
-    ring.ngroups = (c1 - c0 + CW - 1) / CW;
-    ring.q0 = q0;
-    unsigned q = *qp, issued = *issuedp;
-    if (tid == 0)
-      for (unsigned s2 = issued; s2 < q + STAGES; ++s2) ring.issue(s2);
-    issued = max(issued, q + STAGES);
-    for (int gi = 0; gi < ring.ngroups; ++gi) {
-      const unsigned seq = q;
-      if (!ring.wait(seq)) {
-        atomicOr(dctl + DC_ERR, KERR_MBAR_TIMEOUT);
-        ok = false;
-        break;
-      }
-      const int jb = ring.group_begin(seq);
-      block_group<RPT, CW, REREAD>(p, ring.slot(seq) + tid, jb, min(CW, c1 - jb), u, r, valid, sh.red, par, e, bd,
-                                   &ring, seq);
-      q = seq + 1;
-      issued = seq + STAGES + 1;  // block_group issued stage seq + STAGES
-    }
-    *qp = q;
-    *issuedp = issued;
-  }
-  if (ok) {
-#pragma unroll
-    for (int t = 0; t < RPT; ++t)
-      if (valid[t]) rowp_out[tid + t * NTT] = r[t];
-    double tt[2] = {e, bd};
-    block_sum_cols<2, NW>(tt, sh.red, par);
-    *ecol = tt[0];
-    *bcol = tt[1];
-  }
-  *parp = par;
-  return ok;
-}
-
 // Final pass over the strip with u in shared memory (area): g = eps log v,
 // P, loss and column-marginal partials -> colp[buf][k], row sums -> rowp[buf][k].
 template <int RPT, int CW>
@@ -740,10 +665,11 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
     __syncthreads();
   };
 
-  // u of the current round: shared memory with redundant merges (su in warp
-  // mode, else the area's last 4096 doubles, free in thread-per-row mode with
-  // M <= 4096), else ug[round parity]; un: the merged u of the next round
-  double* const u_sm = WARP ? su : sh.area + kResident;
+  // u of the current round: registers (thread per row), su (warp mode) or
+  // ug[round parity] (split merges); un: the merged u of the next round
+  double u[RPT];
+#pragma unroll
+  for (int t = 0; t < RPT; ++t) u[t] = 0.0;
   int rd = 0, iter = 0;
   double err = 1000.0;
   bool unsafe = false;
@@ -784,7 +710,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
         for (int t = 0; t < RPT; ++t)
           if (valid[t]) {
             const int i = tid + t * NTT;
-            un[t] = row_update(pa[i], u_sm[i], row_total(rp, gp, m, i), init, e, bd);
+            un[t] = row_update(pa[i], u[t], row_total(rp, gp, m, i), init, e, bd);
           }
       }
       double tt[4] = {e, bd, ce, cb};
@@ -842,16 +768,20 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
     if (redundant) {
       if (WARP) {
         if (tid < m) su[tid] = un[0];
+        __syncthreads();
       } else {
 #pragma unroll
-        for (int t = 0; t < RPT; ++t)
-          if (valid[t]) u_sm[tid + t * NTT] = un[t];
+        for (int t = 0; t < RPT; ++t) u[t] = un[t];
       }
-      __syncthreads();
-    } else if (WARP) {
+    } else {
       const double* ucur = p.ug + (size_t)nbuf * m;
-      for (int i = tid; i < m; i += NTT) su[i] = __ldcg(ucur + i);
-      __syncthreads();
+      if (WARP) {
+        for (int i = tid; i < m; i += NTT) su[i] = __ldcg(ucur + i);
+        __syncthreads();
+      } else {
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) u[t] = valid[t] ? __ldcg(ucur + tid + t * NTT) : 0.0;
+      }
     }
     // ---- column pass of round rd: v = b / (K^T u), row partials of K v
     double ecol = 0.0, bcol = 0.0;
@@ -861,12 +791,39 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
       else if (m <= 256) warp_pass<8>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
       else warp_pass<16>(p, k, nbuf, c0, c1, sh.area, sh, par, ecol, bcol);
     } else {
-      const double* usrc = redundant ? u_sm : p.ug + (size_t)nbuf * m;
-      if (!block_pass<RPT, CW, REREAD, RES>(p, usrc, !redundant, p.rowp + ((size_t)nbuf * gp + k) * m, c0, c1, sh,
-                                            ring.q0, &q, &issued, &par, &ecol, &bcol, dctl)) {
-        drain();
-        return false;
+      double r[RPT];
+#pragma unroll
+      for (int t = 0; t < RPT; ++t) r[t] = 0.0;
+      double e = 0.0, bd = 0.0;
+      if constexpr (RES) {
+        for (int jb = c0; jb < c1; jb += CW)
+          block_group<RPT, CW, REREAD>(p, sh.area + (size_t)(jb - c0) * p.ldk + tid, jb, min(CW, c1 - jb), u, r,
+                                       valid, sh.red, par, e, bd, nullptr, 0u);
+      } else {
+        if (tid == 0)
+          for (unsigned s2 = issued; s2 < q + STAGES; ++s2) ring.issue(s2);
+        issued = max(issued, q + STAGES);
+        for (int gi = 0; gi < ring.ngroups; ++gi) {
+          const unsigned seq = q;
+          if (!ring.wait(seq)) {
+            atomicOr(dctl + DC_ERR, KERR_MBAR_TIMEOUT);
+            drain();
+            return false;
+          }
+          const int jb = ring.group_begin(seq);
+          block_group<RPT, CW, REREAD>(p, ring.slot(seq) + tid, jb, min(CW, c1 - jb), u, r, valid, sh.red, par, e,
+                                       bd, &ring, seq);
+          q = seq + 1;
+          issued = seq + STAGES + 1;  // block_group issued stage seq + STAGES
+        }
       }
+#pragma unroll
+      for (int t = 0; t < RPT; ++t)
+        if (valid[t]) p.rowp[((size_t)nbuf * gp + k) * m + tid + t * NTT] = r[t];
+      double tt[2] = {e, bd};
+      block_sum_cols<2, NW>(tt, sh.red, par);
+      ecol = tt[0];
+      bcol = tt[1];
     }
     if (tid == 0) {
       p.colp[((size_t)nbuf * gp + k) * 4 + 0] = ecol;
@@ -900,7 +857,9 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
     if (WARP) {
       for (int i = tid; i < m; i += NTT) us[i] = su[i];
     } else if (redundant) {
-      for (int i = tid; i < m; i += NTT) us[i] = u_sm[i];
+#pragma unroll
+      for (int t = 0; t < RPT; ++t)
+        if (valid[t]) us[tid + t * NTT] = u[t];
     } else {
       const double* ucur = p.ug + (size_t)(rd & 1) * m;
       for (int i = tid; i < m; i += NTT) us[i] = __ldcg(ucur + i);
@@ -1196,8 +1155,7 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
     if (kbytes <= option("batch.l2_keep_mb", 48.0) * 1048576.0) mode |= MODE_KEEP_L2;
   }
   const long long red_rows = (long long)option("batch.redundant_rows", 16384.0);
-  if ((mode & MODE_RESIDENT) && q.M <= 4096 && (d.gp == 1 || (long long)d.gp * q.M <= red_rows))
-    mode |= MODE_REDUNDANT;
+  if (q.M <= 4096 && (d.gp == 1 || (long long)d.gp * q.M <= red_rows)) mode |= MODE_REDUNDANT;
   d.mode = mode;
   d.nunits = (q.M + kUnit - 1) / kUnit;
   d.max_iter = q.max_iter;
