@@ -366,6 +366,48 @@ __device__ __noinline__ void warp_pass(const Prob& p, int k, int buf, int c0, in
   bad = tt[1];
 }
 
+// Column sums of a group of CW (a power of two, <= 16) columns over the
+// block, returned to lane c < CW of every warp as the total of column c.
+// Inside a warp a transposed reduction: at each of log2 CW levels a lane
+// trades half of the columns it holds with its partner (lane ^ o) and keeps
+// the sum of the other half, then a butterfly over the remaining lane bits --
+// CW - 1 + 5 - log2 CW shuffles instead of 5 CW.  One partial per warp and
+// column goes to shared memory; the owning lanes add the NW partials in warp
+// order.  A fixed pattern: the same bits on every run.
+template <int CW>
+__device__ __forceinline__ double block_col_sums(const double (&v)[CW], double* red, int& par) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int LG = CW >= 16 ? 4 : CW >= 8 ? 3 : CW >= 4 ? 2 : CW >= 2 ? 1 : 0;
+  double x[CW];
+#pragma unroll
+  for (int c = 0; c < CW; ++c) x[c] = v[c];
+  int col = 0;
+#pragma unroll
+  for (int st = 0; st < LG; ++st) {
+    const int o = 16 >> st;
+    const int half = CW >> (st + 1);
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const double send = upper ? x[j] : x[j + half];
+      const double recv = __shfl_xor_sync(0xffffffffu, send, o);
+      x[j] = (upper ? x[j + half] : x[j]) + recv;
+    }
+    if (upper) col += half;
+  }
+  double sum = x[0];
+#pragma unroll
+  for (int o = 16 >> LG; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((lane & ((32 >> LG) - 1)) == 0) red[(par * NW + w) * CW + col] = sum;
+  __syncthreads();
+  double tot = 0.0;
+  if (lane < CW)
+#pragma unroll
+    for (int q = 0; q < NW; ++q) tot += red[(par * NW + q) * CW + lane];
+  par ^= 1;
+  return tot;
+}
+
 // One group of CW columns, thread per row (RPT rows per thread): column sums
 // with u, v = b / s (warp 0, lane c owns column jb + c), r += K v.  `buf`
 // points at column jb's row 0 (+ tid), leading dimension ldk.
@@ -388,11 +430,8 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
       sum[c] = fma(x, u[t], sum[c]);
     }
   }
-  block_sum_cols<CW, NW>(sum, red, par);
-  double s_l = 1.0;
-#pragma unroll
-  for (int c = 0; c < CW; ++c)
-    if (c == lane) s_l = sum[c];
+  double s_l = block_col_sums<CW>(sum, red, par);  // (its barrier: every thread has read the stage)
+  if (lane >= CW) s_l = 1.0;
   const bool owner = lane < nc;
   const double v_l = owner ? bl / s_l : 0.0;
   if (w == 0 && owner) {
@@ -404,7 +443,7 @@ __device__ __forceinline__ void block_group(const Prob& p, const double* buf, in
   double v[CW];
 #pragma unroll
   for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);
-  // streamed, registers hold the stage: every thread has read it (block_sum_cols)
+  // streamed, registers hold the stage: every thread has read it (block_col_sums)
   if (!REREAD && ring && tid == 0) ring->issue(seq + STAGES);
 #pragma unroll
   for (int t = 0; t < RPT; ++t) {
