@@ -77,7 +77,7 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "batch.strip_kb": target K strip per team member of a batched problem,
  *       at most 184 (default); strips up to that stay in shared memory;
  *   "batch.max_team": largest team of CTAs per batched problem (default:
- *       half the SM count);
+ *       0.4 x the SM count);
  *   "batch.resident_team": problems with M > 512 keep their K strips in
  *       shared memory when that takes at most this many CTAs (default 32),
  *       else stream strips of about "batch.stream_strip_kb" (default 1024)

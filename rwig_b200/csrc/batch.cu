@@ -1179,7 +1179,7 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   const long long strip_target = (long long)(option("batch.strip_kb", 184.0) * 1024.0 / 8.0);
   const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
   const int gp_res = (int)((q.N + cols - 1) / cols);
-  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", (double)(G / 2))));
+  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", std::floor(0.4 * G))));
   const int res_team = std::min(maxteam, (int)option("batch.resident_team", 32.0));
   int mode = 0;
   if (gp_res <= res_team || (q.M <= kWarpRows && gp_res <= maxteam)) {
