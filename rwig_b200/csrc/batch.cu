@@ -78,7 +78,7 @@ enum : int { MODE_RESIDENT = 1, MODE_WARP = 2, MODE_REDUNDANT = 4, MODE_KEEP_L2 
 
 // Device control words of a launch.
 enum : int { DC_AVAIL = 0, DC_HEAD = 1, DC_ERR = 2, DC_PROGRESS = 3, DC_ACTIVE = 4, DC_FREE = 5, DC_OLDEST = 6,
-             DC_OLDEST_T = 7 };
+             DC_OLDEST_T = 7, DC_PUB_T = 8, kCtlWords = 16 };
 
 struct Prob {
   const double* a;
@@ -977,15 +977,22 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
   int* F = reinterpret_cast<int*>(dctl + DC_FREE);
   atomicAdd(F, 1);
   const unsigned long long t_idle = globaltimer_ns();
+  unsigned nap = 256;  // sleep between empty passes, doubled up to 8 us
   while (true) {
     if (ld_relaxed(dctl + DC_ERR) != 0u) return;
     const unsigned W = ld_relaxed(dctl + DC_AVAIL);
     const unsigned npx = W & ~kClosed;
     if (!(W & kClosed)) {
-      const unsigned p0 = min(pub[0], (unsigned)kMaxProbs);
-      if (p0 > npx) {
-        atomicCAS(dctl + DC_AVAIL, W, p0);
-        continue;
+      // the published count lives in host memory for a server: one CTA of
+      // the grid reads it at most every 20 us, the others see DC_AVAIL
+      const unsigned now_us = (unsigned)(globaltimer_ns() / 1000ull);
+      const unsigned last = ld_relaxed(dctl + DC_PUB_T);
+      if (now_us - last >= 20u && atomicCAS(dctl + DC_PUB_T, last, now_us) == last) {
+        const unsigned p0 = min(pub[0], (unsigned)kMaxProbs);
+        if (p0 > npx) {
+          atomicCAS(dctl + DC_AVAIL, W, p0);
+          continue;
+        }
       }
     }
     // 1. an unfilled slot of an opened problem; states and claim counts are
@@ -1067,7 +1074,8 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
         continue;
       }
     }
-    __nanosleep(500);
+    __nanosleep(nap);
+    nap = min(nap * 2, 8192u);
   }
 }
 
@@ -1240,7 +1248,8 @@ int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, cons
   int nblk = 0;
   RWIG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, service_kernel, NTT, smem_bytes()));
   if (nblk < 1) return set_error(RWIG_E_UNSUPPORTED, "batched Sinkhorn kernel does not fit on an SM");
-  const unsigned h0[8] = {avail0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned h0[kCtlWords] = {};
+  h0[DC_AVAIL] = avail0;
   RWIG_CUDA_TRY(cudaMemcpyAsync(dctl, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
   const Prob* dp = dprob;
   const volatile unsigned* pb = pub;
@@ -1303,14 +1312,14 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   double* dK = (double*)scratch(ctx, SBT_K, sizeof(double) * std::max<long long>(kd, 32));
   double* dW = (double*)scratch(ctx, SBT_WORK, sizeof(double) * std::max<long long>(wd, 32));
   double* dres = (double*)scratch(ctx, SBT_RES, sizeof(double) * kResStride * np);
-  unsigned* ctrl = (unsigned*)scratch(ctx, SBT_CTRL, sizeof(unsigned) * (8 + 2 + kMaxProbs));
+  unsigned* ctrl = (unsigned*)scratch(ctx, SBT_CTRL, sizeof(unsigned) * (kCtlWords + 2 + kMaxProbs));
   unsigned* pctl = (unsigned*)scratch(ctx, SBT_PCTL, sizeof(unsigned) * 4 * kMaxProbs);
   const bool profile = option("batch.profile", 0.0) != 0.0;
   double* dprof = profile ? (double*)scratch(ctx, SBT_PROF, sizeof(double) * 4 * G) : nullptr;
   if (!dprob || !dK || !dW || !dres || !ctrl || !pctl || (profile && !dprof)) return RWIG_E_NOMEM;
   for (int s = 0; s < np; ++s) bind(hp[s], dK + koff[s], dW + woff[s], dres + kResStride * (size_t)s, pctl + 4 * s);
-  unsigned* pub = ctrl + 8;
-  unsigned* done = ctrl + 10;
+  unsigned* pub = ctrl + kCtlWords;
+  unsigned* done = ctrl + kCtlWords + 2;
   const unsigned hpub[2] = {(unsigned)np, 1u};
   RWIG_CUDA_TRY(cudaMemcpyAsync(dprob, hp.data(), sizeof(Prob) * np, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(pub, hpub, sizeof(hpub), cudaMemcpyHostToDevice, st));
@@ -1659,7 +1668,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaStreamCreateWithFlags(&s->ks, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
   if ((e = cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
   if ((e = cudaMalloc(&s->dprob, sizeof(batch::Prob) * batch::kMaxProbs)) != cudaSuccess) return fail(e, "descriptors");
-  if ((e = cudaMalloc(&s->dctl, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  if ((e = cudaMalloc(&s->dctl, sizeof(unsigned) * batch::kCtlWords)) != cudaSuccess) return fail(e, "control");
   if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * 4 * batch::kMaxProbs)) != cudaSuccess) return fail(e, "slot control");
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
   if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
@@ -1669,7 +1678,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaHostGetDevicePointer(&s->dpub, s->hpub, 0)) != cudaSuccess) return fail(e, "pub map");
   if ((e = cudaHostGetDevicePointer(&s->ddone, s->hdone, 0)) != cudaSuccess) return fail(e, "done map");
   if ((e = cudaHostGetDevicePointer(&s->dres, s->hres, 0)) != cudaSuccess) return fail(e, "results map");
-  if ((e = cudaMemset(s->dctl, 0, sizeof(unsigned) * 8)) != cudaSuccess) return fail(e, "control");
+  if ((e = cudaMemset(s->dctl, 0, sizeof(unsigned) * batch::kCtlWords)) != cudaSuccess) return fail(e, "control");
   for (auto& sl : s->slots)
     if ((e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "events");
   s->hpub[0] = 0;
