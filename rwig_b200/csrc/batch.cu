@@ -1580,6 +1580,10 @@ struct rwig_server {
   double* dres = nullptr;
   unsigned* dctl = nullptr;                 // device control words
   unsigned* dpctl = nullptr;                // device, 4 control words per slot
+  // the requests' memory: a pool of the server's own that keeps what it has
+  // mapped (release threshold: unlimited), so freeing a collected request
+  // never unmaps device memory -- which would wait for the running launch
+  cudaMemPool_t pool = nullptr;
   unsigned hctl_err = 0;
   int nslots = 0, npub = 0, next_ticket = 0;
   bool launched = false;
@@ -1669,6 +1673,16 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   if ((e = cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
   if ((e = cudaMalloc(&s->dprob, sizeof(batch::Prob) * batch::kMaxProbs)) != cudaSuccess) return fail(e, "descriptors");
   if ((e = cudaMalloc(&s->dctl, sizeof(unsigned) * batch::kCtlWords)) != cudaSuccess) return fail(e, "control");
+  {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    if ((e = cudaMemPoolCreate(&s->pool, &props)) != cudaSuccess) return fail(e, "memory pool");
+    unsigned long long keep = ~0ull;
+    if ((e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+      return fail(e, "memory pool");
+  }
   if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * 4 * batch::kMaxProbs)) != cudaSuccess) return fail(e, "slot control");
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
   if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
@@ -1719,7 +1733,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   const double bytes = 8.0 * (double)(io + kd + wd);
   if (s->inflight + bytes > s->budget) return RWIG_E_BUSY;
   void* mem = nullptr;
-  RWIG_CUDA_TRY(cudaMallocAsync(&mem, (size_t)bytes, s->cs));
+  RWIG_CUDA_TRY(cudaMallocFromPoolAsync(&mem, (size_t)bytes, s->pool, s->cs));
   double* base = (double*)mem;
   double* da = base;
   double* db = da + al(M);
@@ -1826,6 +1840,7 @@ extern "C" int rwig_server_destroy(rwig_server* s) {
     for (auto& sl : s->slots)
       if (sl.mem) cudaFreeAsync(sl.mem, s->cs);
     if (s->cs) cudaStreamSynchronize(s->cs);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->dprob) cudaFree(s->dprob);
     if (s->dctl) cudaFree(s->dctl);
     if (s->dpctl) cudaFree(s->dpctl);
