@@ -262,6 +262,9 @@ RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_
  * runs it holds every SM, and a restart delays the requests that wait for it,
  * so sparse arrivals want idle_ms well above the gap between requests (at
  * 300 requests/s the p99 latency was 582 ms with 5 ms, 111 ms with 500 ms).
+ * Requests are allocated from a memory pool of the server's own, which keeps
+ * what it maps until rwig_server_destroy; create maps min(budget, 4 GB) of it
+ * up front, and the pool grows on demand up to the budget.
  * Results are bitwise those of rwig_batch_sinkhorn_log for the same problem.
  * One thread drives a server. */
 typedef struct rwig_server rwig_server;

@@ -1682,6 +1682,13 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
     unsigned long long keep = ~0ull;
     if ((e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
       return fail(e, "memory pool");
+    // map up to 4 GB of the budget now, while no launch runs (growing the
+    // pool later waits for the running launch)
+    void* prime = nullptr;
+    const size_t pb = (size_t)std::min(mem_budget_bytes, 4.0 * (1ull << 30));
+    if ((e = cudaMallocFromPoolAsync(&prime, pb, s->pool, s->cs)) != cudaSuccess) return fail(e, "memory pool");
+    if ((e = cudaFreeAsync(prime, s->cs)) != cudaSuccess) return fail(e, "memory pool");
+    if ((e = cudaStreamSynchronize(s->cs)) != cudaSuccess) return fail(e, "memory pool");
   }
   if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * 4 * batch::kMaxProbs)) != cudaSuccess) return fail(e, "slot control");
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
