@@ -259,9 +259,8 @@ RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_
  * RWIG_E_BUSY when admitting it would exceed the device-memory budget or the
  * slot table (512 requests) is full -- poll and retry.  The kernel ends after
  * idle_ms without work and is restarted by the next submit or poll; while it
- * runs it holds every SM, and a restart delays the requests that wait for it,
- * so sparse arrivals want idle_ms well above the gap between requests (at
- * 300 requests/s the p99 latency was 582 ms with 5 ms, 111 ms with 500 ms).
+ * runs it holds every SM (other work on the GPU waits), so idle_ms trades the
+ * restart of the launch (tens of microseconds) against that.
  * Requests are allocated from a memory pool of the server's own, which keeps
  * what it maps until rwig_server_destroy; create maps min(budget, 4 GB) of it
  * up front, and the pool grows on demand up to the budget.
