@@ -299,7 +299,16 @@ class SinkhornWorkload:
         if world == 1 and not args.no_cpu_baseline:
             secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1, int(round(it_mean)))
             cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
-        return {"value": value, "ms_per_step": tot_ms / args.steps,
+        ref_gpu = None
+        if self.method == "vanilla" and world == 1:
+            import oracle
+            ref_gpu = reference_gpu_timing(
+                lambda: oracle.ref_gpu_sinkhorn_vanilla(a, b, C, self.reg, self.max_iter, self.tol),
+                lambda: rw.sinkhorn(a, b, C, {"reg": self.reg, "method": "vanilla", "max_iter": self.max_iter,
+                                              "zero_tol": self.tol}),
+                args.steps, "cuda_sinkhorn_vanilla (src/cuda_sinkhorn.cu:181) vs rw.sinkhorn(method='vanilla'), "
+                            "host arrays in and out")
+        return {"value": value, "ms_per_step": tot_ms / args.steps, "reference_gpu": ref_gpu,
                 "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
                            "iterations_per_solve": it_mean, "l2": "flushed between steps (256 MB write)"},
                 "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
@@ -470,7 +479,19 @@ class BarycenterWorkload:
             secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1)
             cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
         MS, NN = n * S * 8, n * n * 8
+        ref_gpu = None
+        if world == 1:
+            import oracle
+            ref_gpu = reference_gpu_timing(
+                lambda: oracle.ref_gpu_barycenter_parallel(A, C, w, be, reg=self.reg, with_grad=True,
+                                                          max_iter=self.L, zero_tol=0.0),
+                lambda: rw.barycenter(A, C, w, be, {"reg": self.reg, "method": "parallel", "with_grad": True,
+                                                    "max_iter": self.L, "zero_tol": 0.0}),
+                args.steps, "parallel barycenter + gradient on this workload's inputs (the reference has no GPU log "
+                            "barycenter): cuda_barycenter_parallel (src/cuda_barycenter.cu:268) vs "
+                            "rw.barycenter(method='parallel'), host arrays")
         return {"value": args.steps * world / (tot_ms / 1e3), "ms_per_step": tot_ms / args.steps,
+                "reference_gpu": ref_gpu,
                 "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (256 MB write)"},
                 "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
@@ -985,6 +1006,26 @@ WORKLOADS = {
     "stream": StreamWorkload(),
     "sinkgrad2048": GradWorkload(),
 }
+
+
+def reference_gpu_timing(ref_call, engine_call, steps, what):
+    """rwig's own GPU code (oracle/_ref, compiled from the reference's sources:
+    cuBLAS products, per-call device allocation) against the engine's
+    host-pointer entry on the same problem: wall-clock calls per second of
+    each, two untimed calls first.  None when oracle/_ref was not built."""
+    import oracle
+    if not oracle.ref_gpu_available():
+        return None
+    out = {}
+    for name, fn in (("value", ref_call), ("engine_same_call", engine_call)):
+        fn()
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        out[name] = steps / (time.perf_counter() - t0)
+    out.update(unit="solves/s", call=what, speedup_engine_over_reference=out["engine_same_call"] / out["value"])
+    return out
 
 
 def max_over_ranks(x, world, dev):

@@ -34,6 +34,75 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+_REF_GPU_PATH = os.path.join(_HERE, "_ref", "librwig_ref_gpu.so")
+_REF_SOURCES = os.environ.get("RWIG_REFERENCE_DIR", "/root/reference")
+_ref_gpu = None
+
+
+def build_ref_gpu() -> str | None:
+    """Compile rwig's own GPU vanilla Sinkhorn and parallel barycenter from the
+    reference's sources (``make -C oracle ref``) when those sources are present;
+    elsewhere the prebuilt library is used as is."""
+    if os.path.isdir(os.path.join(_REF_SOURCES, "src")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={_REF_SOURCES}"], check=True)
+    return _REF_GPU_PATH if os.path.exists(_REF_GPU_PATH) else None
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(_REF_GPU_PATH)
+
+
+def ref_gpu():
+    """The reference's GPU path (oracle/_ref), loaded on first use."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(_REF_GPU_PATH):
+            raise RuntimeError(f"reference GPU library not built: {_REF_GPU_PATH} (make -C oracle ref)")
+        L = ctypes.CDLL(_REF_GPU_PATH)
+        i, d = ctypes.c_int, ctypes.c_double
+        L.ref_gpu_sinkhorn_vanilla.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, i, i, d, i, i, d]
+        L.ref_gpu_sinkhorn_vanilla.restype = None
+        L.ref_gpu_barycenter_parallel.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp,
+                                                  i, i, i, d, i, i, d]
+        L.ref_gpu_barycenter_parallel.restype = None
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def ref_gpu_sinkhorn_vanilla(a, b, C, reg, max_iter=1000, zero_tol=1e-6):
+    """rwig's own GPU vanilla Sinkhorn (src/cuda_sinkhorn.cu:181), host buffers."""
+    a, b = _f64(a).ravel(), _f64(b).ravel()
+    C = _f64(C)
+    M, N = C.shape
+    P, u, v = np.zeros((M, N), order="F"), np.zeros(M), np.zeros(N)
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    ref_gpu().ref_gpu_sinkhorn_vanilla(_ptr(P), None, _ptr(u), _ptr(v), ctypes.byref(loss), ctypes.byref(it),
+                                       ctypes.byref(err), _ptr(a), _ptr(b), _ptr(C), M, N, float(reg), 0,
+                                       int(max_iter), float(zero_tol))
+    return {"P": P, "u": u, "v": v, "loss": loss.value, "iter": it.value, "err": err.value}
+
+
+def ref_gpu_barycenter_parallel(A, C, w, b_ext=None, reg=0.1, with_grad=False, max_iter=1000, zero_tol=1e-6):
+    """rwig's own GPU parallel barycenter (src/cuda_barycenter.cu:268), host buffers."""
+    A, C = _f64(A), _f64(C)
+    w = _f64(w).ravel()
+    M, S = A.shape
+    N = C.shape[1]
+    U, V = np.zeros((M, S), order="F"), np.zeros((N, S), order="F")
+    b = np.zeros(N)
+    gA = np.zeros((M, S), order="F") if with_grad else None
+    gw = np.zeros(S) if with_grad else None
+    be = _f64(b_ext).ravel() if b_ext is not None else np.zeros(N)
+    loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    ref_gpu().ref_gpu_barycenter_parallel(_ptr(U), _ptr(V), _ptr(b), _ptr(gA), _ptr(gw), ctypes.byref(loss),
+                                          ctypes.byref(it), ctypes.byref(err), _ptr(A), _ptr(w), _ptr(C), _ptr(be),
+                                          M, N, S, float(reg), int(bool(with_grad)), int(max_iter), float(zero_tol))
+    out = {"b": b, "U": U, "V": V, "iter": it.value, "err": err.value}
+    if with_grad:
+        out.update(grad_A=gA, grad_w=gw, loss=loss.value)
+    return out
+
+
 def lib():
     global _lib
     if _lib is None:
