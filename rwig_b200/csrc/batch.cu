@@ -408,80 +408,6 @@ __device__ __forceinline__ double block_col_sums(const double (&v)[CW], double* 
   return tot;
 }
 
-// Pipelined streamed column pass, part A of a stage: the sums of this
-// thread's rows of the stage's CW columns with u and the warp's transposed
-// reduction (as in block_col_sums) into red_half[w * CW + column].
-template <int RPT, int CW>
-__device__ __forceinline__ void stage_a(const double* buf, int nc, long long ldk, const double (&u)[RPT],
-                                        const bool (&valid)[RPT], double* red_half) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double x[CW];
-#pragma unroll
-  for (int c = 0; c < CW; ++c) {
-    x[c] = 0.0;
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-      const double k = (c < nc && valid[t]) ? buf[(size_t)c * ldk + t * NTT] : 0.0;
-      x[c] = fma(k, u[t], x[c]);
-    }
-  }
-  constexpr int LG = CW >= 16 ? 4 : CW >= 8 ? 3 : CW >= 4 ? 2 : CW >= 2 ? 1 : 0;
-  int col = 0;
-#pragma unroll
-  for (int st = 0; st < LG; ++st) {
-    const int o = 16 >> st;
-    const int half = CW >> (st + 1);
-    const bool upper = (lane & o) != 0;
-#pragma unroll
-    for (int j = 0; j < half; ++j) {
-      const double send = upper ? x[j] : x[j + half];
-      const double recv = __shfl_xor_sync(0xffffffffu, send, o);
-      x[j] = (upper ? x[j + half] : x[j]) + recv;
-    }
-    if (upper) col += half;
-  }
-  double sum = x[0];
-#pragma unroll
-  for (int o = 16 >> LG; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-  if ((lane & ((32 >> LG) - 1)) == 0) red_half[w * CW + col] = sum;
-}
-
-// Part B of a stage, after the block barrier that follows its part A: lane
-// c < CW adds the warps' partials of column c in warp order (as
-// block_col_sums), v = b / s, warp 0 records g and the column error, r += K v
-// with K read from the stage again.
-template <int RPT, int CW>
-__device__ __forceinline__ void stage_b(double* gg, int jb, int nc, double bl, const double* buf, long long ldk,
-                                        const bool (&valid)[RPT], const double* red_half, double (&r)[RPT],
-                                        double& e, double& bd) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double s_l = 1.0;
-  if (lane < CW) {
-    double tot = 0.0;
-#pragma unroll
-    for (int q = 0; q < NW; ++q) tot += red_half[q * CW + lane];
-    s_l = tot;
-  }
-  const bool owner = lane < nc;
-  const double v_l = owner ? bl / s_l : 0.0;
-  if (w == 0 && owner) {
-    gg[jb + lane] = v_l;
-    const double d = (v_l * s_l) / bl - 1.0;  // first-order form of log(v s) - log b
-    e += d * d;
-    if (!(v_l >= kScaleMin && v_l <= kScaleMax) || !(s_l >= 1e-300 && s_l <= 1e300)) bd = 1.0;
-  }
-  double v[CW];
-#pragma unroll
-  for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);
-#pragma unroll
-  for (int t = 0; t < RPT; ++t) {
-    double acc = r[t];
-#pragma unroll
-    for (int c = 0; c < CW; ++c) acc = fma((c < nc && valid[t]) ? buf[(size_t)c * ldk + t * NTT] : 0.0, v[c], acc);
-    r[t] = acc;
-  }
-}
-
 // One group of CW columns, thread per row (RPT rows per thread): column sums
 // with u, v = b / s (warp 0, lane c owns column jb + c), r += K v.  `buf`
 // points at column jb's row 0 (+ tid), leading dimension ldk.
@@ -912,7 +838,7 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
         for (int jb = c0; jb < c1; jb += CW)
           block_group<RPT, CW, REREAD>(p, sh.area + (size_t)(jb - c0) * p.ldk + tid, jb, min(CW, c1 - jb), u, r,
                                        valid, sh.red, par, e, bd, nullptr, 0u);
-      } else if constexpr (REREAD) {
+      } else {
         if (tid == 0)
           for (unsigned s2 = issued; s2 < q + STAGES; ++s2) ring.issue(s2);
         issued = max(issued, q + STAGES);
@@ -929,51 +855,6 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
           q = seq + 1;
           issued = seq + STAGES + 1;  // block_group issued stage seq + STAGES
         }
-      } else {
-        // pipelined: part A of stage g+1 (loads, sums, warp reduction) runs
-        // beside part B of stage g (cross-warp sums, v, row update re-reading
-        // the stage); one block barrier per stage, the reduction buffer
-        // alternates halves, and a slot is refilled after its part B
-        if (tid == 0)
-          for (unsigned s2 = issued; s2 < q + STAGES; ++s2) ring.issue(s2);
-        const int ng = ring.ngroups;
-        const long long ldk = p.ldk;
-        double* const gg = p.g;
-        double* const redh[2] = {sh.red, sh.red + NW * CW};
-        if (!ring.wait(q)) {
-          atomicOr(dctl + DC_ERR, KERR_MBAR_TIMEOUT);
-          issued = max(issued, q + STAGES);
-          drain();
-          return false;
-        }
-        int jbA = ring.group_begin(q), ncA = min(CW, c1 - jbA);
-        double blA = (tid & 31) < ncA ? p.b[jbA + (tid & 31)] : 1.0;
-        stage_a<RPT, CW>(ring.slot(q) + tid, ncA, ldk, u, valid, redh[0]);
-        for (int gi = 0; gi < ng; ++gi) {
-          __syncthreads();  // stage gi's partials are in shared memory; stage gi-1 is done with
-          if (gi > 0 && tid == 0) ring.issue(q + gi - 1 + STAGES);
-          const int jbB = jbA, ncB = ncA;
-          const double blB = blA;
-          if (gi + 1 < ng) {
-            const unsigned sq = q + gi + 1;
-            if (!ring.wait(sq)) {
-              atomicOr(dctl + DC_ERR, KERR_MBAR_TIMEOUT);
-              issued = max(q + gi + STAGES, q + STAGES);  // stages issued so far
-              q += gi + 1;  // stages q .. q + gi were consumed; drain the rest
-              drain();
-              return false;
-            }
-            jbA = ring.group_begin(sq);
-            ncA = min(CW, c1 - jbA);
-            blA = (tid & 31) < ncA ? p.b[jbA + (tid & 31)] : 1.0;
-            stage_a<RPT, CW>(ring.slot(sq) + tid, ncA, ldk, u, valid, redh[(gi + 1) & 1]);
-          }
-          stage_b<RPT, CW>(gg, jbB, ncB, blB, ring.slot(q + gi) + tid, ldk, valid, redh[gi & 1], r, e, bd);
-        }
-        __syncthreads();  // the last stage is done with
-        if (tid == 0) ring.issue(q + ng - 1 + STAGES);
-        q += ng;
-        issued = q + STAGES;
       }
 #pragma unroll
       for (int t = 0; t < RPT; ++t)
