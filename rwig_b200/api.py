@@ -232,6 +232,42 @@ def wdl_batch_grad(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0):
     return gA, gl
 
 
+def wdl_batch_grad_dp(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0, group=None, grad_fn=None):
+    """Data-parallel batched WDL gradient over the ranks of a torch.distributed
+    group (one process per GPU).  Every rank passes the whole batch; its D
+    documents are split into contiguous shards, rank r taking documents
+    [r D / R, (r + 1) D / R), and each rank computes its shard's mean gradient
+    with `grad_fn` (default: this engine's wdl_batch_grad on the rank's
+    current GPU).  One all-reduce of the shard sums (g_Alpha, N x S, and
+    g_lambda, S) then gives every rank the whole batch's mean gradient, as
+    WassersteinDictionaryLearning::_train_batch_batched averages it
+    (src/wdl_impl.cpp:236-243), so every rank can take the same optimizer step.
+    The all-reduce runs on the group's backend: a CUDA buffer for NCCL, a host
+    buffer otherwise.  Returns (g_Alpha, g_lambda) as numpy arrays."""
+    import torch
+    import torch.distributed as dist
+    A = _mat(A, "A")
+    W_B = _mat(W_B, "W_B")
+    Y_B = _mat(Y_B, "Y_B")
+    N, S = A.shape
+    D = W_B.shape[1]
+    if W_B.shape[0] != S or Y_B.shape != (N, D):
+        raise ValueError("A (N x S), W_B (S x D) and Y_B (N x D) do not match")
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    lo, hi = rank * D // world, (rank + 1) * D // world
+    fn = grad_fn if grad_fn is not None else wdl_batch_grad
+    buf = np.zeros(N * S + S)
+    if hi > lo:
+        gA, gl = fn(A, np.asfortranarray(W_B[:, lo:hi]), np.asfortranarray(Y_B[:, lo:hi]), K_or_C, reg, L, mode)
+        buf[:N * S] = np.asarray(gA).ravel(order="F") * (hi - lo)
+        buf[N * S:] = np.asarray(gl) * (hi - lo)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    t = torch.from_numpy(buf).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    out = t.cpu().numpy() / D
+    return np.asfortranarray(out[:N * S].reshape((N, S), order="F")), out[N * S:].copy()
+
+
 def _cost_or_points(q):
     """(C, None, None) from q["C"], or (None, X, Y) from point clouds q["x"]
     (M x d), q["y"] (N x d), column-major; sizes checked against a, b."""
