@@ -862,7 +862,40 @@ class StreamWorkload:
                 "sample": f"3 smallest requests solved by the oracle ({t:.2f} s), scaled by element-iterations"}
 
     def reference(self, args):
-        raise NotImplementedError
+        """The oracle (all host threads) on the three smallest requests, timed in
+        full, scaled to the whole stream by element-iterations; the stream's
+        per-request iteration counts come from tests/golden/stream_iters.json
+        (tests/golden/make_stream_iters.py).  Returns the time of `steps`
+        requests at the stream's mean cost per request."""
+        import oracle
+        from rwig_b200 import synth
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "stream_iters.json")
+        with open(path) as fh:
+            iters = json.load(fh)["iters"]
+        reqs = synth.stream_requests(self.R)
+        if len(iters) != len(reqs):
+            raise RuntimeError("stream_iters.json does not match the stream")
+        elems = [q["m"] * q["n"] for q in reqs]
+        order = sorted(range(len(reqs)), key=lambda i: elems[i])[:3]
+        threads = os.cpu_count() or 1
+        secs = []
+        for _ in range(max(1, args.warmup) + args.steps):
+            t, work = 0.0, 0.0
+            for i in order:
+                q = reqs[i]
+                a, b, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
+                C = synth.sq_euclid_cost(x, y)
+                t0 = time.perf_counter()
+                r = oracle.sinkhorn_log(a, b, C, q["eps"], max_iter=self.max_iter, zero_tol=self.tol,
+                                        n_threads=threads, want_P=False)
+                t += time.perf_counter() - t0
+                work += (r["iter"] + 2) * elems[i]
+            total = sum((iters[i] + 2) * elems[i] for i in range(len(reqs)))
+            secs.append(t * total / work / len(reqs))  # mean seconds per request
+        per = secs[max(1, args.warmup):]
+        sample = (f"the 3 smallest requests solved by the oracle ({threads} threads), scaled to the 200-request "
+                  f"stream by element-iterations")
+        return sum(per), threads, sample
 
 
 class GradWorkload:
