@@ -54,7 +54,8 @@ std::map<std::string, double> g_opts;
 const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "log_sinkhorn.l2_hot", "batch.profile",
                                    "batch.strip_kb", "batch.max_team", "batch.redundant_rows",
                                    "batch.l2_keep_mb", "batch.max_elems", "batch.resident_team",
-                                   "batch.stream_strip_kb", "batch.backfill_us"};
+                                   "batch.stream_strip_kb", "batch.backfill_us",
+                                   "wdl.infer_docs"};
 }  // namespace
 
 double option(const char* name, double dflt) {

@@ -342,11 +342,205 @@ __global__ void opt_step(double* th, double* m, double* v, const double* g, int 
 enum {
   SW_UH = 120, SW_VH, SW_KVH, SW_KTH, SW_BH, SW_T, SW_T2, SW_AB, SW_GWP, SW_DOT, SW_WBAR, SW_K,
   SW_Y, SW_C, SW_ALPHA, SW_LAMBDA, SW_A, SW_W, SW_MA, SW_VA, SW_ML, SW_VL, SW_GA, SW_GL, SW_YHAT,
-  SW_HA, SW_HW, SW_HY, SW_HK, SW_HOUT
+  SW_HA, SW_HW, SW_HY, SW_HK, SW_HOUT, SW_IU, SW_IV, SW_IKV, SW_IKT, SW_IB, SW_IERR, SW_IST
 };
 
 // Columns per GEMM tile: whole documents, at most 64.
 int tile_cols(int S, int SD) { return std::min((64 / S) * S, SD); }
+
+// ---------------------------------------------------------------------------
+// Inference (wdl_impl.cpp:349-377; cuda_wdl.cu:754-776): the parallel
+// barycenter of every document, each with its own stopping test
+// (Barycenter::compute_parallel: `iter < max_iter && err >= tol`, err the
+// Frobenius norm of U o KV - A).  The reference solves the documents one by
+// one; here a chunk of documents is one set of stacked columns, as in the
+// training step, and a document whose test stops it is frozen: the
+// epilogues skip its columns, so its state -- and its barycenter -- stays
+// that of its own last iteration.
+// ---------------------------------------------------------------------------
+// After KVB = K VB: store KVB and UB = A / KVB for the running documents;
+// unless `first`, the squared residual (U_l o KVB - A, with U_l the UB this
+// overwrites) summed over each row's S columns -> errp[document * N + row]
+// (one entry per row whatever rows the GEMM hands this call: with split-K a
+// tile's rows are divided among the cluster's CTAs).
+struct EpiYInf {
+  const double* A;
+  const int* active;
+  int N, S, W, D, first;
+  double* KVB;
+  double* UB;
+  double* errp;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double* ws) const {
+    if (nr <= 0) return;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      double sq = 0.0;
+      if (gc < W && active[gc / S]) {
+        const int i = r0 + r;
+        const size_t k = (size_t)i + (size_t)gc * N;
+        const double y = t[c * ldt + r];
+        const double a = A[i + (size_t)(gc % S) * N];
+        if (!first) {
+          const double res = UB[k] * y - a;
+          sq = res * res;
+        }
+        KVB[k] = y;
+        UB[k] = a / y;
+      }
+      ws[c * ldt + r] = sq;
+    }
+    if (first) return;
+    __syncthreads();
+    const int ng = nc / S;
+    for (int p = threadIdx.x; p < nr * ng; p += blockDim.x) {
+      const int r = p % nr, q = p / nr, g0 = c0 + q * S;
+      if (g0 >= W) continue;
+      double acc = 0.0;
+      for (int s = 0; s < S; ++s) acc += ws[(q * S + s) * ldt + r];
+      errp[(size_t)(g0 / S) * N + r0 + r] = acc;
+    }
+  }
+};
+
+// After KTUB = K^T UB: for the running documents KTUB, their barycenters bB
+// and VB = bB / KTUB (EpiZ's arithmetic).
+struct EpiZInf {
+  const double* Wb;
+  const int* active;
+  int N, S, W;
+  double* KTUB;
+  double* VB;
+  double* bB;
+  __device__ void operator()(int r0, int nr, int c0, int nc, double* t, int ldt, double* ws) const {
+    if (nr <= 0) return;
+    double* wb = ws + nc * ldt;
+    const int ng = nc / S;
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      ws[c * ldt + r] = gc < W ? pow(t[c * ldt + r], Wb[gc]) : 1.0;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < nr * ng; p += blockDim.x) {
+      const int r = p % nr, q = p / nr, g0 = c0 + q * S;
+      if (g0 >= W || !active[g0 / S]) continue;
+      double acc = 1.0;  // barycenter_impl_parallel.cpp:120 order
+      for (int s = 0; s < S; ++s) acc *= ws[(q * S + s) * ldt + r];
+      bB[(size_t)(r0 + r) + (size_t)(g0 / S) * N] = acc;
+      wb[q * ldt + r] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+      const int r = e % nr, c = e / nr, gc = c0 + c;
+      if (gc >= W || !active[gc / S]) continue;
+      const size_t k = (size_t)(r0 + r) + (size_t)gc * N;
+      const double z = t[c * ldt + r];
+      KTUB[k] = z;
+      VB[k] = wb[(c / S) * ldt + r] / z;
+    }
+  }
+};
+
+// One iteration's bookkeeping, one block per document: err = sqrt of the
+// document's per-row residual sums (256 strided partial sums, then a tree:
+// a fixed order), then the stopping test.  state[d] = iterations run,
+// state[D + d] = running flag, state[2 D] counts the documents still running.
+__global__ void infer_update(const double* errp, int N, int D, int L, double tol, int* state) {
+  __shared__ double sh[256];
+  const int d = blockIdx.x;
+  if (!state[D + d]) return;  // the same for every thread of the block
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < N; j += blockDim.x) acc += errp[(size_t)d * N + j];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double err = sqrt(sh[0]);
+    const int it = ++state[d];
+    if (!(it < L && err >= tol)) {
+      state[D + d] = 0;
+      atomicSub(state + 2 * D, 1);
+    }
+  }
+}
+
+__global__ void infer_init(int D, int* state) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < D; d += gridDim.x * blockDim.x) {
+    state[d] = 0;
+    state[D + d] = 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) state[2 * D] = D;
+}
+
+// Yhat[:, d] = bB[:, d] / sum(bB[:, d]) (normalise_b's order: 1024 strided
+// partial sums, then a tree).
+__global__ void infer_output(const double* bB, int N, double* Yhat) {
+  __shared__ double sh[1024];
+  const double* b = bB + (size_t)blockIdx.x * N;
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < N; j += blockDim.x) acc += b[j];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double tot = sh[0];
+  for (int j = threadIdx.x; j < N; j += blockDim.x) Yhat[(size_t)blockIdx.x * N + j] = b[j] / tot;
+}
+
+// Inference of documents [0, M): A (N x S), W (S x M), K padded (ldk); Yhat
+// (N x M).  Chunks of at most wdl.infer_docs documents (default 1024).
+int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const double* K, long long ldk, int N,
+          int S, int M, int L, double tol, double* Yhat, int* launches) {
+  const int chunk = std::max(1, std::min(M, (int)option("wdl.infer_docs", 1024.0)));
+  const size_t NWc = (size_t)N * S * chunk;
+  double* UB = (double*)scratch(ctx, SW_IU, sizeof(double) * NWc);
+  double* VB = (double*)scratch(ctx, SW_IV, sizeof(double) * NWc);
+  double* KV = (double*)scratch(ctx, SW_IKV, sizeof(double) * NWc);
+  double* KT = (double*)scratch(ctx, SW_IKT, sizeof(double) * NWc);
+  double* bB = (double*)scratch(ctx, SW_IB, sizeof(double) * (size_t)N * chunk);
+  double* errp = (double*)scratch(ctx, SW_IERR, sizeof(double) * (size_t)N * chunk);
+  int* state = (int*)scratch(ctx, SW_IST, sizeof(int) * (2 * (size_t)chunk + 1));
+  if (!UB || !VB || !KV || !KT || !bB || !errp || !state) return RWIG_E_NOMEM;
+  for (int m0 = 0; m0 < M; m0 += chunk) {
+    const int D = std::min(chunk, M - m0);
+    const int SD = S * D;
+    const size_t NW = (size_t)N * SD;
+    const double* Wb = W + (size_t)m0 * S;
+    const int tc = tile_cols(S, SD);
+    auto gemm = [&](int trans, const double* X, auto epi) -> int {
+      ++*launches;
+      const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
+      return trans ? dg::gemm<1>(ctx, g, epi, st) : dg::gemm<0>(ctx, g, epi, st);
+    };
+    fill<<<grid_for(ctx, NW), TPB, 0, st>>>(VB, NW, 1.0);
+    infer_init<<<std::max(1, (D + 255) / 256), 256, 0, st>>>(D, state);
+    *launches += 2;
+    int rc = gemm(0, VB, EpiYInf{A, state + D, N, S, SD, D, 1, KV, UB, errp});  // U_1 = A / K 1
+    if (rc) return rc;
+    for (int l = 0; l < L; ++l) {
+      rc = gemm(1, UB, EpiZInf{Wb, state + D, N, S, SD, KT, VB, bB});
+      if (rc) return rc;
+      rc = gemm(0, VB, EpiYInf{A, state + D, N, S, SD, D, 0, KV, UB, errp});
+      if (rc) return rc;
+      infer_update<<<D, 256, 0, st>>>(errp, N, D, L, tol, state);
+      ++*launches;
+      if (tol > 0.0 && l + 1 < L) {  // stop early once every document has stopped
+        int running = 0;
+        RWIG_CUDA_TRY(cudaMemcpyAsync(&running, state + 2 * D, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+        if (running == 0) break;
+      }
+    }
+    infer_output<<<D, 1024, 0, st>>>(bB, N, Yhat + (size_t)m0 * N);
+    ++*launches;
+    RWIG_CUDA_TRY(cudaGetLastError());
+  }
+  return 0;
+}
 
 // Batched gradient on device buffers: K padded (ldk), A (N x S), Wb (S x D),
 // Yb (N x D); outputs gA (N x S) and gl (S).
@@ -609,13 +803,19 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   if (W) RWIG_CUDA_TRY(cudaMemcpyAsync(W, dW, sizeof(double) * SM, cudaMemcpyDeviceToHost, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   if (Yhat) {
-    // inference: the parallel barycenter of every document (wdl_impl.cpp:349-377)
+    // inference: the parallel barycenter of every document (wdl_impl.cpp:349-377),
+    // all documents at once; without iterations the reference's b is 0 / 0
     double* dYh = (double*)scratch(ctx, SW_YHAT, sizeof(double) * NM);
     if (!dYh) return RWIG_E_NOMEM;
-    for (int m = 0; m < M; ++m) {
-      rc = bary::run(ctx, st, false, nullptr, nullptr, dYh + (size_t)m * N, nullptr, nullptr, nullptr, nullptr,
-                     nullptr, dA, dW + (size_t)m * S, dC, nullptr, N, N, S, reg, 0, max_iter, zero_tol);
+    if (max_iter >= 1) {
+      rc = infer(ctx, st, dA, dW, K, ldk, N, S, M, max_iter, zero_tol, dYh, &launches);
       if (rc < 0) return rc;
+    } else {
+      for (int m = 0; m < M; ++m) {
+        rc = bary::run(ctx, st, false, nullptr, nullptr, dYh + (size_t)m * N, nullptr, nullptr, nullptr, nullptr,
+                       nullptr, dA, dW + (size_t)m * S, dC, nullptr, N, N, S, reg, 0, max_iter, zero_tol);
+        if (rc < 0) return rc;
+      }
     }
     RWIG_CUDA_TRY(cudaMemcpyAsync(Yhat, dYh, sizeof(double) * NM, cudaMemcpyDeviceToHost, st));
     RWIG_CUDA_TRY(cudaStreamSynchronize(st));

@@ -101,3 +101,29 @@ def test_invalid_arguments():
         rw.wdl_batch_grad(Abig, np.full((65, 2), 1 / 65), Y, K, 0.1, 3)
     with pytest.raises(ValueError):
         rw.wdl_cpp(Y, C[:, :-1], 0.1, 3, 2, 1)
+
+
+def test_batched_inference_chunks_and_per_document_stops():
+    """Inference solves every document's barycenter in stacked columns and
+    freezes each document at its own stop (iter < max_iter && err >= tol);
+    chunks of 1024, 4 or 1 documents give the oracle's per-document results."""
+    N, M, S, B, L, reg, tol = 80, 9, 3, 3, 25, 0.1, 1e-4
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=13)
+    lib = rw.load()
+    outs = []
+    try:
+        for docs in (1024, 4, 1):
+            lib.rwig_set_option(b"wdl.infer_docs", float(docs))
+            outs.append(rw.wdl_cpp(Y, C, reg, S, B, 1, max_iter=L, zero_tol=tol, optimizer=1, eta=1e-3,
+                                   Alpha0=A0, Lambda0=L0, max_steps=2))
+    finally:
+        lib.rwig_set_option(b"wdl.infer_docs", 1024.0)
+    ref = oracle.wdl_train(Y, C, S, reg, L, B, 1, A0, L0, opt=1, eta=1e-3, max_steps=2)
+    iters = set()
+    for m in range(M):
+        r = oracle.barycenter_parallel(ref["A"], C, ref["W"][:, m], None, reg, with_grad=False, max_iter=L,
+                                       zero_tol=tol)
+        iters.add(r["iter"])
+        for o in outs:
+            assert rel_err(o["Yhat"][:, m], r["b"]) <= 1e-9, (m, rel_err(o["Yhat"][:, m], r["b"]))
+    assert len(iters) > 1, iters  # the documents stopped at different iterations
