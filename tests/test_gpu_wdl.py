@@ -107,7 +107,7 @@ def test_batched_inference_chunks_and_per_document_stops():
     """Inference solves every document's barycenter in stacked columns and
     freezes each document at its own stop (iter < max_iter && err >= tol);
     chunks of 1024, 4 or 1 documents give the oracle's per-document results."""
-    N, M, S, B, L, reg, tol = 80, 9, 3, 3, 25, 0.1, 1e-4
+    N, M, S, B, L, reg, tol = 80, 9, 3, 3, 25, 0.1, 1e-6
     Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=13)
     lib = rw.load()
     outs = []
