@@ -583,6 +583,16 @@ class WdlWorkload:
             torch.cuda.synchronize()
         dev_ms = max_over_ranks(rep["device_ms"], world, dev)
         wall = max_over_ranks(wall, world, dev)
+        # inference: every document's parallel barycenter (max_iter = L,
+        # zero_tol 1e-6, per-document stop) under the initial topics, one
+        # rwig_wdl call with no training epoch (host buffers, copies and K included)
+        Yh = np.zeros((N, M), order="F")
+        t0 = time.perf_counter()
+        _lib.check(L.rwig_wdl(dp(A), dp(W), dp(Yh), dp(Y), dp(C), N, M, S, self.reg, self.L, 1e-6, self.B, 0, 1,
+                              self.lr, 0.01, 0.9, 0.999, 1e-8, 42, 0, dp(A0), dp(L0), 0))
+        inf_s = time.perf_counter() - t0
+        infer = {"docs": M, "seconds": inf_s, "docs_per_s": M / inf_s, "max_iter": self.L, "zero_tol": 1e-6,
+                 "call": "rwig_wdl with no training epoch: all documents in stacked columns, per-document stop"}
         if rank != 0:
             return None
         tf_peak = measured_dgemm_tflops(dev)
@@ -605,7 +615,7 @@ class WdlWorkload:
                         "d2h_bytes_per_step": (N * S + S * M) * 8 / args.steps,
                         "note": "one rwig_wdl call with host buffers (copies, K, training) over all steps"},
                 "gpu_launches": rep["kernel_launches"], "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clocks.summary()}
+                "inference": infer, "clocks": clocks.summary()}
 
     def reference(self, args):
         secs, sample, cores = [], "", 1
