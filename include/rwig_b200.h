@@ -102,7 +102,7 @@ RWIG_API int rwig_set_option(const char* name, double value);
  * continues, u, v zero off the support.  a: M, b: N, C: M x N.  Outputs (any
  * may be NULL): P (M x N), grad_a (M, needs withgrad), u (M), v (N), loss.
  * grad_a is the unrolled backward Sinkhorn::_bwd_vanilla (:169-213), zero off
- * the support; it needs at most 4096 non-zero entries of a and keeps every
+ * the support; it needs at most 8192 non-zero entries of a and keeps every
  * iteration's scalings on the device (8 (max_iter + 2)(M + N) bytes, at most
  * 32 GiB), else RWIG_E_UNSUPPORTED.
  */

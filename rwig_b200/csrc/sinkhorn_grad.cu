@@ -250,7 +250,7 @@ int sinkhorn_grad(Context* ctx, cudaStream_t st, bool vanilla, const double* C, 
                   const double* gh, int m, int n, int L, double eps, const int* ridx, int M, double out_scale,
                   double* grad_a, int* launches) {
   using namespace skgrad;
-  if (m > 4096) return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient supports up to 4096 rows of support");
+  if (m > 8192) return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient supports up to 8192 rows of support");
   double* ga = (double*)scratch(ctx, 232, sizeof(double) * m);
   double* xbar = (double*)scratch(ctx, 233, sizeof(double) * m);
   unsigned* ctrl = (unsigned*)scratch(ctx, 234, sizeof(unsigned) * 4);
@@ -265,12 +265,14 @@ int sinkhorn_grad(Context* ctx, cudaStream_t st, bool vanilla, const double* C, 
       if (m <= 512) rc = launch_t<1, 16, true>(ctx, p, st);
       else if (m <= 1024) rc = launch_t<2, 8, true>(ctx, p, st);
       else if (m <= 2048) rc = launch_t<4, 4, true>(ctx, p, st);
-      else rc = launch_t<8, 2, true>(ctx, p, st);
+      else if (m <= 4096) rc = launch_t<8, 2, true>(ctx, p, st);
+      else rc = launch_t<16, 1, true>(ctx, p, st);
     } else {
       if (m <= 512) rc = launch_t<1, 16, false>(ctx, p, st);
       else if (m <= 1024) rc = launch_t<2, 8, false>(ctx, p, st);
       else if (m <= 2048) rc = launch_t<4, 4, false>(ctx, p, st);
-      else rc = launch_t<8, 2, false>(ctx, p, st);
+      else if (m <= 4096) rc = launch_t<8, 2, false>(ctx, p, st);
+      else rc = launch_t<16, 1, false>(ctx, p, st);
     }
     if (rc) return rc;
     ++*launches;

@@ -823,7 +823,7 @@ int sinkhorn_device(Context* ctx, cudaStream_t st, bool vanilla, double* P, doub
   double* fh = nullptr;
   double* gh = nullptr;
   if (want_grad) {
-    if (m > 4096) return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient supports up to 4096 rows of support");
+    if (m > 8192) return set_error(RWIG_E_UNSUPPORTED, "the Sinkhorn gradient supports up to 8192 rows of support");
     const size_t hb_f = sizeof(double) * ((size_t)max_iter + 2) * m, hb_g = sizeof(double) * ((size_t)max_iter + 1) * n;
     if (hb_f + hb_g > kMaxHistoryBytes)
       return set_error(RWIG_E_UNSUPPORTED, "the gradient's iteration history (max_iter x (M + N)) exceeds 32 GiB");

@@ -46,7 +46,7 @@ def test_golden_vectors(golden, method):
 @pytest.mark.parametrize("method", ["vanilla", "log"])
 @pytest.mark.parametrize("m,n,reg", [
     (64, 64, 0.1), (100, 37, 0.2), (37, 100, 0.2), (513, 300, 0.1), (1500, 700, 0.05),
-    (2048, 900, 0.1), (4096, 256, 0.1), (1, 5, 0.1), (5, 1, 0.1), (2, 2, 0.5),
+    (2048, 900, 0.1), (4096, 256, 0.1), (6000, 300, 0.1), (1, 5, 0.1), (5, 1, 0.1), (2, 2, 0.5),
 ])
 def test_parity_shapes(method, m, n, reg):
     a, b, C = synth.sinkhorn_problem(m, n, 1.0, salt=m * 17 + n)
@@ -92,6 +92,6 @@ def test_grad_is_deterministic():
 
 
 def test_rows_beyond_limit_rejected():
-    a, b, C = synth.sinkhorn_problem(4097, 8, 1.0, salt=23)
+    a, b, C = synth.sinkhorn_problem(8193, 8, 1.0, salt=23)
     with pytest.raises(rw.RwigError):
         rw.sinkhorn(a, b, C, {"reg": 0.1, "method": "log", "with_grad": True, "max_iter": 5})
