@@ -435,12 +435,10 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
     launches += 3;
     // Y = K X (rows M, contraction N) and Z = K^T X (rows N, contraction M)
     auto gemm_y = [&](const double* X, auto epi) -> int {
-      ++launches;
-      return dg::gemm<0>(ctx, dg::GemmArgs{K, ldk, M, N, S, X, N, 0}, epi, q);
+      return dg::gemm<0>(ctx, dg::GemmArgs{K, ldk, M, N, S, X, N, 0}, epi, q, 0, &launches);
     };
     auto gemm_z = [&](const double* X, auto epi) -> int {
-      ++launches;
-      return dg::gemm<1>(ctx, dg::GemmArgs{K, ldk, N, M, S, X, M, 0}, epi, q);
+      return dg::gemm<1>(ctx, dg::GemmArgs{K, ldk, N, M, S, X, M, 0}, epi, q, 0, &launches);
     };
     // Y_0 = K V_0, U_1 = A / Y_0
     int rc = gemm_y(slot(Vh, NS, 0), EpiY{A, logA, nullptr, slot(Yh, MS, 0), slot(Uh, MS, 1), nullptr, M, S,
@@ -459,8 +457,7 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
                                         need_err ? D : nullptr, M, S, (int)ldd, logdomain ? 1 : 0});
       if (rc) return rc;
       if (need_err) {
-        ++launches;
-        rc = dg::gemm<1>(ctx, dg::GemmArgs{D, ldd, S, M, S, D, ldd, 0}, dg::EpiStore{gram, S, S}, q);
+        rc = dg::gemm<1>(ctx, dg::GemmArgs{D, ldd, S, M, S, D, ldd, 0}, dg::EpiStore{gram, S, S}, q, 0, &launches);
         if (rc) return rc;
         if (!fixed) {  // the stopping test needs err now
           std::vector<double> G((size_t)S * S);

@@ -33,6 +33,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "engine.h"
@@ -43,6 +44,7 @@ namespace dg {
 constexpr int BM = 64, BK = 32, NTH = 256, STAGES = 4;
 constexpr int PAD = 4;  // doubles of padding per shared row
 constexpr int kMaxSplits = 8;
+constexpr int kDmmaK = 4;  // DMMA shape of the product paths (m16n8k4)
 
 struct GemmArgs {
   const double* K;
@@ -53,6 +55,7 @@ struct GemmArgs {
   int splits;        // cluster size along z: 1, 2, 4 or 8
   int tcols;         // output columns per tile (<= BN; 0: BN).  A multiple of an
                      // epilogue's column group keeps every group inside one tile.
+  int tile0;         // first tile of the launch (wide-tile kernel; 0 otherwise)
 };
 
 template <int TRANS>
@@ -93,6 +96,23 @@ __device__ __forceinline__ void mma_16x8x4(double (&d)[4], double a0, double a1,
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// m16n8k8 and m16n8k16 (PTX ISA 7.8, sm_90 and later): thread (gid, tig)
+// holds A(gid + 8 (i % 2), tig + 4 (i / 2)) in a_i and B(tig + 4 i, gid) in b_i.
+__device__ __forceinline__ void mma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+__device__ __forceinline__ void mma_16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 __device__ __forceinline__ unsigned cluster_nctarank() {
   unsigned r;
   asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
@@ -115,16 +135,16 @@ __device__ __forceinline__ double ld_cluster(const double* p, unsigned rank) {
 // Issues the copies of contraction step [k0, k0 + BK) into one ring stage.
 // XV = 2: X columns copied as 16-byte pairs (ldx even, X 16-byte aligned);
 // XV = 1: 8-byte copies.  Out-of-range elements are zero-filled.
-template <int TRANS, int NT, int XV>
+template <int TRANS, int NT, int XV, int BMT = BM>
 __device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double* Bs, int m0, int n0, int tc,
                                            int k0, int kend) {
   const int tid = threadIdx.x;
   if (!TRANS) {
-    // A[k][m] = K[m + k*ldk]: 32 k x 32 m-pairs
+    // A[k][m] = K[m + k*ldk]: 32 k x BMT/2 m-pairs
 #pragma unroll
-    for (int c = 0; c < (BK * BM / 2) / NTH; ++c) {
+    for (int c = 0; c < (BK * BMT / 2) / NTH; ++c) {
       const int idx = tid + c * NTH;
-      const int kk = idx >> 5, mp = (idx & 31) * 2;
+      const int kk = idx / (BMT / 2), mp = (idx % (BMT / 2)) * 2;
       const int gk = k0 + kk, gm = m0 + mp;
       int bytes = 0;
       const double* src = g.K;
@@ -132,12 +152,12 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double
         bytes = (gm + 1 < g.Mo) ? 16 : 8;
         src = g.K + gm + (long long)gk * g.ldk;
       }
-      cp_async16(As + kk * (BM + PAD) + mp, src, bytes);
+      cp_async16(As + kk * (BMT + PAD) + mp, src, bytes);
     }
   } else {
-    // A[m][k] = K[k + m*ldk]: 64 m x 16 k-pairs
+    // A[m][k] = K[k + m*ldk]: BMT m x 16 k-pairs
 #pragma unroll
-    for (int c = 0; c < (BM * BK / 2) / NTH; ++c) {
+    for (int c = 0; c < (BMT * BK / 2) / NTH; ++c) {
       const int idx = tid + c * NTH;
       const int mm = idx >> 4, kp = (idx & 15) * 2;
       const int gk = k0 + kp, gm = m0 + mm;
@@ -182,7 +202,8 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, double* As, double
   }
 }
 
-template <int TRANS, int NT, int XV, class Epi>
+// KM: k extent of one DMMA instruction (4, 8 or 16).
+template <int TRANS, int NT, int XV, class Epi, int KM>
 __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
   extern __shared__ __align__(16) double smem[];
   constexpr int BN = NT * 8;
@@ -228,18 +249,28 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
     const double* A = As + (s % STAGES) * ASZ;
     const double* B = Bs + (s % STAGES) * BSZ;
 #pragma unroll
-    for (int k4 = 0; k4 < BK / 2; k4 += 4) {
-      const int kk = kh + k4;
-      double a0, a1;
-      if (!TRANS) {
-        a0 = A[(kk + tig) * (BM + PAD) + wm + gid];
-        a1 = A[(kk + tig) * (BM + PAD) + wm + gid + 8];
-      } else {
-        a0 = A[(wm + gid) * (BK + PAD) + kk + tig];
-        a1 = A[(wm + gid + 8) * (BK + PAD) + kk + tig];
+    for (int k0 = 0; k0 < BK / 2; k0 += KM) {
+      const int kk = kh + k0;
+      // A(wm + gid + 8 (i % 2), kk + tig + 4 (i / 2)), i < KM / 2
+      double a[KM / 2];
+#pragma unroll
+      for (int i = 0; i < KM / 2; ++i) {
+        const int r = wm + gid + 8 * (i & 1), k = kk + tig + 4 * (i >> 1);
+        a[i] = !TRANS ? A[k * (BM + PAD) + r] : A[r * (BK + PAD) + k];
       }
 #pragma unroll
-      for (int t = 0; t < NT; ++t) mma_16x8x4(acc[t], a0, a1, B[(t * 8 + gid) * (BK + PAD) + kk + tig]);
+      for (int t = 0; t < NT; ++t) {
+        const double* bp = B + (t * 8 + gid) * (BK + PAD) + kk + tig;
+        if constexpr (KM == 4) {
+          mma_16x8x4(acc[t], a[0], a[1], bp[0]);
+        } else if constexpr (KM == 8) {
+          const double b[2] = {bp[0], bp[4]};
+          mma_16x8x8(acc[t], *reinterpret_cast<const double(*)[4]>(a), b);
+        } else {
+          const double b[4] = {bp[0], bp[4], bp[8], bp[12]};
+          mma_16x8x16(acc[t], *reinterpret_cast<const double(*)[8]>(a), b);
+        }
+      }
     }
   }
   cp_async_wait<0>();
@@ -290,6 +321,143 @@ __global__ void __launch_bounds__(NTH) dgemm_kernel(GemmArgs g, Epi epi) {
   if (splits > 1) cluster_wait();  // peers are done reading this CTA
 }
 
+// ---------------------------------------------------------------------------
+// Wide-tile variant for long products with 64-column tiles: a BM2 x 64 tile
+// per CTA (one CTA per SM), the 8 warps in a 4 x 2 grid of 32 x 32 blocks,
+// each over the whole BK step (two m16 x four n8 DMMA tiles per k chunk, so a
+// warp issues BK / KM * 8 DMMAs between barriers and reads 8 fragments per 8
+// DMMAs).  Same operand ring, split-K cluster and epilogue interface as
+// dgemm_kernel; without split-K the partial tile itself (row stride BM2 + 1)
+// goes to the epilogue.
+constexpr int BM2 = 128, STAGES2 = 4;
+template <int TRANS>
+__host__ __device__ constexpr int a2_stage_doubles() {
+  return TRANS ? BM2 * (BK + PAD) : BK * (BM2 + PAD);
+}
+template <int TRANS>
+__host__ __device__ constexpr int smem2_doubles() {
+  // ring, or partial tile + epilogue scratch (no split), or partial tile +
+  // summed rows + scratch (split-K, at most BM2 / 2 rows per CTA)
+  constexpr int ring = STAGES2 * (a2_stage_doubles<TRANS>() + b_stage_doubles<8>());
+  constexpr int e1 = 64 * (BM2 + 1) + 2 * 65 * (BM2 + 1);
+  constexpr int e2 = 64 * (BM2 + 1) + 64 * (BM2 / 2) + 2 * 65 * (BM2 / 2);
+  return ring > e1 ? (ring > e2 ? ring : e2) : (e1 > e2 ? e1 : e2);
+}
+
+template <int TRANS, int XV, class Epi, int KM>
+__global__ void __launch_bounds__(NTH, 1) dgemm2_kernel(GemmArgs g, Epi epi) {
+  extern __shared__ __align__(16) double smem[];
+  constexpr int NT = 8, BN = 64;
+  constexpr int ASZ = a2_stage_doubles<TRANS>(), BSZ = b_stage_doubles<NT>();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int tc = g.tcols > 0 ? g.tcols : BN;
+  const int ntiles = (g.W + tc - 1) / tc;
+  const int tile = (int)blockIdx.x + g.tile0;
+  const int m0 = (tile / ntiles) * BM2, n0 = (tile % ntiles) * tc;
+  const int splits = g.splits;
+  if (splits > 1 && (int)cluster_nctarank() != splits) return;
+  const int z = blockIdx.z;
+  int slice = (g.Kd + splits - 1) / splits;
+  slice = ((slice + BK - 1) / BK) * BK;
+  const int kbeg = z * slice;
+  const int kend = min(g.Kd, kbeg + slice);
+  const int nsteps = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][t][e] = 0.0;
+
+  double* As = smem;
+  double* Bs = smem + STAGES2 * ASZ;
+#pragma unroll
+  for (int s = 0; s < STAGES2 - 1; ++s) {
+    if (s < nsteps)
+      load_stage<TRANS, NT, XV, BM2>(g, As + s * ASZ, Bs + s * BSZ, m0, n0, tc, kbeg + s * BK, kend);
+    cp_async_commit();
+  }
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  for (int s = 0; s < nsteps; ++s) {
+    cp_async_wait<STAGES2 - 2>();
+    __syncthreads();  // stage s visible; stage s-1 no longer read
+    const int nx = s + STAGES2 - 1;
+    if (nx < nsteps) {
+      const int q = nx % STAGES2;
+      load_stage<TRANS, NT, XV, BM2>(g, As + q * ASZ, Bs + q * BSZ, m0, n0, tc, kbeg + nx * BK, kend);
+    }
+    cp_async_commit();
+    const double* A = As + (s % STAGES2) * ASZ;
+    const double* B = Bs + (s % STAGES2) * BSZ;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += KM) {
+      double a[2][KM / 2], b[4][KM / 4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int i = 0; i < KM / 2; ++i) {
+          const int r = wm + 16 * mi + gid + 8 * (i & 1), k = kk + tig + 4 * (i >> 1);
+          a[mi][i] = !TRANS ? A[k * (BM2 + PAD) + r] : A[r * (BK + PAD) + k];
+        }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int i = 0; i < KM / 4; ++i) b[t][i] = B[(wn + 8 * t + gid) * (BK + PAD) + kk + tig + 4 * i];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          if constexpr (KM == 4) mma_16x8x4(acc[mi][t], a[mi][0], a[mi][1], b[t][0]);
+          else if constexpr (KM == 8) mma_16x8x8(acc[mi][t], a[mi], b[t]);
+          else mma_16x8x16(acc[mi][t], a[mi], b[t]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // partial tile -> shared memory, [c][r] with row stride BM2 + 1
+  double* red = smem;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = wm + 16 * mi + gid + ((e >> 1) << 3);
+        const int c = wn + 8 * t + tig * 2 + (e & 1);
+        red[c * (BM2 + 1) + r] = acc[mi][t][e];
+      }
+  if (splits == 1) {
+    __syncthreads();
+    epi(m0, min(BM2, g.Mo - m0), n0, tc, red, BM2 + 1, red + BN * (BM2 + 1));
+    return;
+  }
+  cluster_arrive();
+  cluster_wait();
+  // CTA z sums rows [z * rows, z * rows + nrl) of the tile; rows is a multiple
+  // of 8 (at most BM2 / 2), so every CTA's first row is too
+  const int rows = ((BM2 + splits - 1) / splits + 7) / 8 * 8;
+  const int rl0 = z * rows;
+  const int nrl = min(rows, BM2 - rl0);
+  double* fin = red + BN * (BM2 + 1);
+  double* ws = fin + BN * rows;
+  for (int e = threadIdx.x; e < nrl * BN; e += NTH) {
+    const int r = e % nrl, c = e / nrl;
+    const double* p = red + c * (BM2 + 1) + rl0 + r;
+    double v = 0.0;
+    for (int q = 0; q < splits; ++q) v += ld_cluster(p, (unsigned)q);
+    fin[c * rows + r] = v;
+  }
+  cluster_arrive();  // this CTA is done reading its peers
+  __syncthreads();
+  epi(m0 + rl0, min(nrl, g.Mo - (m0 + rl0)), n0, tc, fin, rows, ws);
+  cluster_wait();  // peers are done reading this CTA
+}
+
 // Epilogue that stores the tile: Y[r + c*ldy] for columns < W.
 struct EpiStore {
   double* Y;
@@ -321,10 +489,10 @@ inline int pick_splits(const Context* ctx, int Mo, int Kd, int W, int NT, int tc
 
 inline int clamp_splits(int s) { return s >= 8 ? 8 : s >= 4 ? 4 : s >= 2 ? 2 : 1; }
 
-template <int TRANS, int NT, int XV, class Epi>
+template <int TRANS, int NT, int XV, class Epi, int KM>
 int launch_kernel(const GemmArgs& g, const Epi& epi, cudaStream_t st) {
   constexpr size_t bytes = sizeof(double) * smem_doubles<TRANS, NT>();
-  auto kern = dgemm_kernel<TRANS, NT, XV, Epi>;
+  auto kern = dgemm_kernel<TRANS, NT, XV, Epi, KM>;
   static bool attr_set = false;  // once per instantiation (callers hold the context lock)
   if (!attr_set) {
     RWIG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -347,12 +515,132 @@ int launch_kernel(const GemmArgs& g, const Epi& epi, cudaStream_t st) {
   return 0;
 }
 
+template <int TRANS, int XV, class Epi, int KM>
+int prepare_kernel2() {
+  constexpr size_t bytes = sizeof(double) * smem2_doubles<TRANS>();
+  static_assert(bytes <= 227 * 1024, "wide-tile GEMM exceeds the shared memory of a CTA");
+  static bool attr_set = false;  // once per instantiation (callers hold the context lock)
+  if (!attr_set) {
+    RWIG_CUDA_TRY(cudaFuncSetAttribute(dgemm2_kernel<TRANS, XV, Epi, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes));
+    attr_set = true;
+  }
+  return 0;
+}
+
+// Clusters of `s` wide-tile CTAs that can be resident at once (cached per
+// instantiation; 0 if the query fails).
+template <int TRANS, int XV, class Epi, int KM>
+int max_clusters2(int s) {
+  static int cache[kMaxSplits + 1] = {};
+  if (cache[s] == 0) {
+    if (prepare_kernel2<TRANS, XV, Epi, KM>() != 0) return 0;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1, 1, (unsigned)s);
+    cfg.blockDim = dim3(NTH);
+    cfg.dynamicSmemBytes = sizeof(double) * smem2_doubles<TRANS>();
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = (unsigned)s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, dgemm2_kernel<TRANS, XV, Epi, KM>, &cfg) != cudaSuccess || n < 1) {
+      (void)cudaGetLastError();
+      n = -1;
+    }
+    cache[s] = n;
+  }
+  return cache[s] > 0 ? cache[s] : 0;
+}
+
+template <int TRANS, int XV, class Epi, int KM>
+int launch_kernel2(const GemmArgs& g, const Epi& epi, cudaStream_t st, int ntile) {
+  constexpr size_t bytes = sizeof(double) * smem2_doubles<TRANS>();
+  auto kern = dgemm2_kernel<TRANS, XV, Epi, KM>;
+  if (int rc = prepare_kernel2<TRANS, XV, Epi, KM>()) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ntile, 1, g.splits);
+  cfg.blockDim = dim3(NTH);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 1;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = (unsigned)g.splits;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  RWIG_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, g, epi));
+  return 0;
+}
+
 // Y = op(K) X with epilogue `epi`.  g.splits <= 0 picks the split count,
 // otherwise it is rounded down to 1, 2, 4 or 8.  Tiles of at most 32 columns
 // run on 32-column CTAs, wider ones on 64-column CTAs; g.tcols (<= 64) fixes
 // the columns per tile.  Returns 0 or an engine error code.
-template <int TRANS, class Epi>
-int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st) {
+// Split count of the wide-tile kernel (one CTA per SM) for `tiles` tiles:
+// the largest count up to 8 that keeps the CTAs within one wave and every
+// slice at least four BK steps.
+inline int pick_splits2(const Context* ctx, long long tiles, int Kd) {
+  int s = 1;
+  while (s < kMaxSplits && tiles * (s + 1) <= ctx->sm_count && Kd >= (s + 1) * 4 * BK) ++s;
+  return s;
+}
+inline long long wide_tiles(int Mo, int W, int tc) {
+  if (tc <= 0) tc = 64;
+  return (long long)((Mo + BM2 - 1) / BM2) * ((W + tc - 1) / tc);
+}
+
+// Wide-tile product: whole waves of unsplit tiles, then the tiles of a last
+// partial wave (when they fill at most half the SMs) as a second launch with
+// split-K, so the tail takes a fraction of a wave.
+template <int TRANS, int XV, class Epi, int KM>
+int gemm_wide(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st, int* launches) {
+  const long long tiles = wide_tiles(g.Mo, g.W, g.tcols);
+  const int sm = ctx->sm_count;
+  if (g.splits > 0 || tiles < sm) {
+    g.splits = g.splits > 0 ? std::min(g.splits, kMaxSplits) : pick_splits2(ctx, tiles, g.Kd);
+    g.tile0 = 0;
+    if (launches) ++*launches;
+    return launch_kernel2<TRANS, XV, Epi, KM>(g, epi, st, (int)tiles);
+  }
+  const long long tail = tiles % sm;
+  const long long full = (tail > 0 && 2 * tail <= sm) ? tiles - tail : tiles;
+  g.splits = 1;
+  g.tile0 = 0;
+  if (launches) ++*launches;
+  int rc = launch_kernel2<TRANS, XV, Epi, KM>(g, epi, st, (int)full);
+  if (rc != 0 || full == tiles) return rc;
+  // split count of the tail: the least waves of resident clusters per slice,
+  // ceil(tail / clusters(s)) / s (clusters wider than a TPC pair may leave SMs
+  // idle, so the count of resident clusters is asked of the runtime)
+  int best = 1;
+  double best_t = 1.0;
+  for (int s = 2; s <= kMaxSplits && g.Kd >= s * 4 * BK; ++s) {
+    const int nc = max_clusters2<TRANS, XV, Epi, KM>(s);
+    if (nc < 1) continue;
+    const double t = (double)((tail + nc - 1) / nc) / s;
+    if (t < best_t - 1e-9) {
+      best_t = t;
+      best = s;
+    }
+  }
+  g.splits = best;
+  g.tile0 = (int)full;
+  if (launches) ++*launches;
+  return launch_kernel2<TRANS, XV, Epi, KM>(g, epi, st, (int)(tiles - full));
+}
+
+// tile: 0 picks the tile height (128 rows for tiles of more than 32 columns
+// when the unsplit 128-row tiles fill every SM, else 64), 64 or 128 forces it
+// (128 only for tiles of more than 32 columns).  launches (optional) is
+// incremented by the number of kernel launches made (1, or 2 with a split
+// tail wave).
+template <int TRANS, class Epi, int KM = kDmmaK>
+int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st, int tile = 0, int* launches = nullptr) {
   if (!g.K || !g.X || g.Mo < 1 || g.Kd < 1 || g.W < 1)
     return set_error(RWIG_E_INVALID, "GEMM: null operand or empty shape");
   if ((g.ldk % 2) != 0 || (reinterpret_cast<uintptr_t>(g.K) % 16) != 0)
@@ -364,10 +652,16 @@ int gemm(const Context* ctx, GemmArgs g, const Epi& epi, cudaStream_t st) {
   if ((long long)((g.Mo + BM - 1) / BM) * ((g.W + (g.tcols > 0 ? g.tcols : NT * 8) - 1) /
                                           (g.tcols > 0 ? g.tcols : NT * 8)) > 0x7fffffffLL)
     return set_error(RWIG_E_INVALID, "GEMM: too many tiles");
-  g.splits = g.splits <= 0 ? pick_splits(ctx, g.Mo, g.Kd, g.W, NT, g.tcols) : clamp_splits(g.splits);
   const bool xv2 = (g.ldx % 2) == 0 && (reinterpret_cast<uintptr_t>(g.X) % 16) == 0;
-  if (NT == 4) return xv2 ? launch_kernel<TRANS, 4, 2>(g, epi, st) : launch_kernel<TRANS, 4, 1>(g, epi, st);
-  return xv2 ? launch_kernel<TRANS, 8, 2>(g, epi, st) : launch_kernel<TRANS, 8, 1>(g, epi, st);
+  if (tile == 0) tile = (NT == 8 && wide_tiles(g.Mo, g.W, g.tcols) >= ctx->sm_count) ? 128 : 64;
+  if (NT == 8 && tile == 128)
+    return xv2 ? gemm_wide<TRANS, 2, Epi, KM>(ctx, g, epi, st, launches)
+               : gemm_wide<TRANS, 1, Epi, KM>(ctx, g, epi, st, launches);
+  g.splits = g.splits <= 0 ? pick_splits(ctx, g.Mo, g.Kd, g.W, NT, g.tcols) : clamp_splits(g.splits);
+  if (launches) ++*launches;
+  if (NT == 4)
+    return xv2 ? launch_kernel<TRANS, 4, 2, Epi, KM>(g, epi, st) : launch_kernel<TRANS, 4, 1, Epi, KM>(g, epi, st);
+  return xv2 ? launch_kernel<TRANS, 8, 2, Epi, KM>(g, epi, st) : launch_kernel<TRANS, 8, 1, Epi, KM>(g, epi, st);
 }
 
 }  // namespace dg

@@ -512,9 +512,8 @@ int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const
     const double* Wb = W + (size_t)m0 * S;
     const int tc = tile_cols(S, SD);
     auto gemm = [&](int trans, const double* X, auto epi) -> int {
-      ++*launches;
       const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
-      return trans ? dg::gemm<1>(ctx, g, epi, st) : dg::gemm<0>(ctx, g, epi, st);
+      return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
     };
     fill<<<grid_for(ctx, NW), TPB, 0, st>>>(VB, NW, 1.0);
     infer_init<<<std::max(1, (D + 255) / 256), 256, 0, st>>>(D, state);
@@ -573,9 +572,8 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   auto Bb = [&](int l) { return Bh + ND * l; };
   const int tc = tile_cols(S, SD);
   auto gemm = [&](int trans, const double* X, auto epi) -> int {
-    ++*launches;
     const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
-    return trans ? dg::gemm<1>(ctx, g, epi, st) : dg::gemm<0>(ctx, g, epi, st);
+    return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
   };
   fill<<<grid_for(ctx, NW), TPB, 0, st>>>(V(0), NW, 1.0);
   ++*launches;

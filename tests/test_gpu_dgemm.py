@@ -75,3 +75,70 @@ def test_wide_outputs(W):
     ref = K @ X
     got = _run(K, X, 0)
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max() * 16
+
+
+class _Tile:
+    """Forces the GEMM's tile height (option dgemm.tile) and DMMA shape
+    (dgemm.kshape) for the duration of a block."""
+
+    def __init__(self, tile, kshape=None):
+        self.tile, self.kshape = tile, kshape
+
+    def __enter__(self):
+        lib = _lib.load()
+        assert lib.rwig_set_option(b"dgemm.tile", float(self.tile)) == 0
+        if self.kshape:
+            assert lib.rwig_set_option(b"dgemm.kshape", float(self.kshape)) == 0
+
+    def __exit__(self, *exc):
+        lib = _lib.load()
+        lib.rwig_set_option(b"dgemm.tile", 0.0)
+        lib.rwig_set_option(b"dgemm.kshape", 4.0)
+
+
+@pytest.mark.parametrize("trans", [0, 1])
+@pytest.mark.parametrize("kshape", [4, 8, 16])
+@pytest.mark.parametrize("Mk,Nk,S", [(333, 517, 47), (130, 70, 64), (1000, 129, 200), (127, 1, 33)])
+def test_wide_tiles(trans, kshape, Mk, Nk, S):
+    """128-row tiles (32 x 32 warp blocks) and every DMMA shape
+    (m16n8k4 / k8 / k16) on ragged shapes."""
+    g = np.random.default_rng(Mk + Nk * 3 + S)
+    K = g.standard_normal((Mk, Nk))
+    X = g.standard_normal((Mk if trans else Nk, S))
+    ref = (K.T if trans else K) @ X
+    with _Tile(128, kshape):
+        got = _run(K, X, trans)
+    assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * np.sqrt(X.shape[0])
+
+
+@pytest.mark.parametrize("splits", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_wide_tile_split_counts(splits):
+    """Wide tiles under every split count: CTA z of the cluster owns rows
+    [z r, z r + r) of the tile with r = 8 ceil(128 / (8 splits)), so counts
+    that do not divide 128 leave the last CTAs fewer (or no) rows."""
+    g = np.random.default_rng(splits)
+    K = g.random((300, 1100))
+    X = g.random((1100, 64))
+    ref = K @ X
+    with _Tile(128):
+        got = _run(K, X, 0, splits=splits)
+        assert _run.splits == splits
+        again = _run(K, X, 0, splits=splits)
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert np.array_equal(got, again)
+
+
+@pytest.mark.parametrize("Kd", [300, 1000])
+def test_wide_tile_tail_wave(Kd):
+    """Automatic tiles at the WDL product's width (1024 columns, 5000 rows):
+    whole waves of unsplit 128-row tiles, then the last partial wave's tiles
+    as a split-K launch (2 or 3 slices here)."""
+    g = np.random.default_rng(Kd)
+    K = g.standard_normal((5000, Kd))
+    X = g.standard_normal((Kd, 1024))
+    ref = K @ X
+    got = _run(K, X, 0)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max() * np.sqrt(Kd)
+    with _Tile(64):
+        narrow = _run(K, X, 0)
+    assert np.abs(narrow - ref).max() <= 1e-12 * np.abs(ref).max() * np.sqrt(Kd)
