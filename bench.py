@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling entry point: one warm-up and one measured solve of a chosen size
     ap.add_argument("--single", action="store_true")
+    ap.add_argument("--gemm", action="store_true",
+                    help="with --single: time the engine's FP64 product K X (--n x --n, --m columns) against "
+                         "cuBLAS (torch.matmul) on the same operands")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--iters", type=int, default=20)
@@ -1122,6 +1125,49 @@ def run_engine(args):
     return 0
 
 
+def run_gemm(args):
+    """Y = K X and Y = K^T X for an --n x --n K and --m columns through the
+    engine's GEMM self-check entry (the product kernels of the barycenter and
+    WDL paths, EpiStore epilogue) and through torch.matmul (cuBLAS), each the
+    median of 9 launches timed with CUDA events; relative max error vs
+    cuBLAS."""
+    import torch
+
+    from rwig_b200 import _lib
+    L = _lib.load()
+    dev = torch.device("cuda", 0)
+    n, w = args.n, args.m
+    g = torch.Generator(device="cpu").manual_seed(1)
+    K = torch.rand(n, n, dtype=torch.float64, generator=g).to(dev)  # column-major n x n (row-major K^T)
+    X = torch.rand(w, n, dtype=torch.float64, generator=g).to(dev)  # column-major n x w
+    Y = torch.empty(w, n, dtype=torch.float64, device=dev)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def timed(fn):
+        ts = []
+        for _ in range(9):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        return sorted(ts)[len(ts) // 2]
+
+    flops = 2.0 * n * n * w
+    for trans in (0, 1):
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the events' stream
+        ms = timed(lambda: _lib.check(L.rwig_selftest_dgemm(vp(K), n, trans, n, n, w, vp(X), n, vp(Y), n, 0, st)))
+        Kop = K.t() if trans == 0 else K
+        ref = Kop @ X.t()
+        cub = timed(lambda: torch.matmul(Kop, X.t()))
+        err = ((Y.t() - ref).abs().max() / ref.abs().max()).item()
+        print(json.dumps({"n": n, "columns": w, "trans": trans, "engine_ms": ms, "engine_tflops": flops / ms / 1e9,
+                          "cublas_ms": cub, "cublas_tflops": flops / cub / 1e9, "rel_err": err}))
+    return 0
+
+
 def run_single(args):
     """One warm-up plus one solve of an m x n log problem with a fixed iteration
     count (tol 0): the small case the kernel profiles are captured on.  With
@@ -1132,6 +1178,8 @@ def run_single(args):
 
     import rwig_b200 as rw
     from rwig_b200 import synth
+    if args.gemm:
+        return run_gemm(args)
     if args.workload.startswith("sinkgrad"):
         # two log-Sinkhorn solves with gradient, --m x --n, --iters unrolled iterations
         dev = torch.device("cuda", 0)
