@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="stream workload: skip tuning the batch.* options on the stream")
     # profiling entry point: one warm-up and one measured solve of a chosen size
     ap.add_argument("--single", action="store_true")
     ap.add_argument("--gemm", action="store_true",
@@ -754,6 +756,7 @@ class StreamWorkload:
         _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
         e2e_s = time.perf_counter() - t0
         serving = self.serve(data, hC, R / (batch_ms / 1e3))
+        tuned = None if args.no_autotune else self.autotuned(data, hC, probs, res, sp, stream)
         if rank != 0:
             return None
         hbm, src = measured_peaks()
@@ -781,8 +784,42 @@ class StreamWorkload:
                 "e2e": {"value": R / e2e_s, "unit": self.unit,
                         "h2d_bytes_per_step": sum((e + d["q"]["m"] + d["q"]["n"]) * 8 for e, d in zip(elems, data)) / R,
                         "d2h_bytes_per_step": sum((d["q"]["m"] + d["q"]["n"]) * 8 for d in data) / R},
-                "serving": serving,
+                "serving": serving, "autotuned": tuned,
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
+
+    def autotuned(self, data, hC, probs, res, sp, stream):
+        """The batch.* options tuned on this stream by rwig_b200.autotune
+        (coordinate search, every trial checked against the starting
+        setting's iteration counts and losses), then the whole batched call
+        timed again under them; the options are cleared afterwards."""
+        import torch
+
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        from rwig_b200.autotune import OPTIONS
+        L = _lib.load()
+        R = len(data)
+        qs = [{"a": d["ha"], "b": d["hb"], "C": hC[i].T, "reg": d["q"]["eps"], "max_iter": self.max_iter,
+               "zero_tol": self.tol} for i, d in enumerate(data)]
+        t0 = time.perf_counter()
+        r = rw.autotune_batch(qs, reps=2)
+        tune_s = time.perf_counter() - t0
+        del qs
+        try:
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+        finally:
+            for n in OPTIONS:
+                L.rwig_set_option(n.encode(), float("nan"))
+        return {"value": R / (ms / 1e3), "unit": self.unit, "options": r["options"],
+                "search_speedup": r["speedup"], "trials": len(r["trials"]), "rejected": len(r["rejected"]),
+                "tuning_seconds": tune_s}
 
     def serve(self, data, hC, capacity):
         """The continuous-batching server (rwig_server_*, point-cloud requests,

@@ -91,8 +91,12 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       path (default 2^26).
  * The batch.* options change team shapes and therefore the summation order
  * of a batched result (within rounding); a result is the same alone and in
- * any mix under the same options. */
+ * any mix under the same options.  A NaN value clears the option (its
+ * built-in default applies again). */
 RWIG_API int rwig_set_option(const char* name, double value);
+/* The value set for option `name`: 0 and *value, or 1 when the option is not
+ * set (its built-in default applies); RWIG_E_INVALID for an unknown name. */
+RWIG_API int rwig_get_option(const char* name, double* value);
 
 /* ---- vanilla Sinkhorn --------------------------------------------------
  * Replaces cuda_sinkhorn_vanilla (inst/include/cuda_interface.cuh:13-18,

@@ -84,6 +84,7 @@ SIGNATURES = {
     "rwig_version": (_i, []),
     "rwig_last_report": (_i, [ctypes.POINTER(Report)]),
     "rwig_set_option": (_i, [ctypes.c_char_p, _d]),
+    "rwig_get_option": (_i, [ctypes.c_char_p, ctypes.POINTER(_d)]),
     "rwig_sinkhorn_vanilla": (_i, [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _i, _i, _d, _i, _i, _d]),
     "rwig_sinkhorn_vanilla_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _i,
                                        _d, _vp]),

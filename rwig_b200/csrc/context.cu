@@ -1,6 +1,7 @@
 // context.cu -- per-device context, scratch arena and the error / report
 // entry points of the C ABI.
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -160,7 +161,21 @@ extern "C" int rwig_set_option(const char* name, double value) {
   for (const char* known : kOptionNames)
     if (std::strcmp(known, name) == 0) {
       std::lock_guard<std::mutex> lk(g_opt_mu);
-      g_opts[name] = value;
+      if (std::isnan(value)) g_opts.erase(name);  // back to the built-in default
+      else g_opts[name] = value;
+      return 0;
+    }
+  return set_error(RWIG_E_INVALID, std::string("unknown option: ") + name);
+}
+
+extern "C" int rwig_get_option(const char* name, double* value) {
+  if (!name || !value) return set_error(RWIG_E_INVALID, "option name or value pointer is null");
+  for (const char* known : kOptionNames)
+    if (std::strcmp(known, name) == 0) {
+      std::lock_guard<std::mutex> lk(g_opt_mu);
+      auto it = g_opts.find(name);
+      if (it == g_opts.end()) return 1;
+      *value = it->second;
       return 0;
     }
   return set_error(RWIG_E_INVALID, std::string("unknown option: ") + name);
