@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=20000,
+                    help="stream workload: requests per arrival rate of the serving run")
     ap.add_argument("--no-autotune", action="store_true",
                     help="stream workload: skip tuning the batch.* options on the stream")
     # profiling entry point: one warm-up and one measured solve of a chosen size
@@ -755,7 +757,7 @@ class StreamWorkload:
         t0 = time.perf_counter()
         _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
         e2e_s = time.perf_counter() - t0
-        serving = self.serve(data, hC, R / (batch_ms / 1e3))
+        serving = self.serve(data, hC, R / (batch_ms / 1e3), args.serve_requests)
         tuned = None if args.no_autotune else self.autotuned(data, hC, probs, res, sp, stream)
         if rank != 0:
             return None
@@ -821,13 +823,15 @@ class StreamWorkload:
                 "search_speedup": r["speedup"], "trials": len(r["trials"]), "rejected": len(r["rejected"]),
                 "tuning_seconds": tune_s}
 
-    def serve(self, data, hC, capacity):
+    def serve(self, data, hC, capacity, n_req=20000):
         """The continuous-batching server (rwig_server_*, point-cloud requests,
-        cost built on the device) in real time: first its capacity (every
-        request submitted at once, in the stream's order), then Poisson
-        arrivals at 50 % and 80 % of that capacity; beside it the per-call
-        path (rwig_sinkhorn_log, host buffers) as a FIFO queue of its measured
-        service times under the same arrivals.  Latency = completion - arrival."""
+        cost built on the device) in real time on n_req requests that cycle
+        through the stream's distinct requests: first its capacity (2000 of
+        them submitted at once), then Poisson arrivals (seeded unit-rate
+        exponential gaps) at 50 %, 80 % and 100 % of that capacity; beside it
+        the per-call path (rwig_sinkhorn_log, host buffers) as a FIFO queue of
+        its measured service times under the same arrivals.  Latency =
+        completion - arrival."""
         import rwig_b200 as rw
         from rwig_b200 import synth
         R = len(data)
@@ -837,18 +841,21 @@ class StreamWorkload:
             q = d["q"]
             _, _, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
             pts.append((np.asfortranarray(x), np.asfortranarray(y)))
-        gaps = np.array([d["q"]["gap"] for d in data])
+        n_req = max(R, int(n_req))
+        gaps = np.random.default_rng(2024).exponential(1.0, n_req)
 
         def run_server(arrivals):
-            lat = np.zeros(R)
+            n = len(arrivals)
+            lat = np.zeros(n)
             with rw.Server(mem_budget_bytes=64e9, idle_ms=200.0) as srv:
                 pending, idx, done = {}, 0, 0
                 t0 = time.perf_counter()
-                while done < R:
+                while done < n:
                     now = time.perf_counter() - t0
-                    while idx < R and arrivals[idx] <= now:
-                        a, b, _, eps = reqs[idx]
-                        t = srv.submit(a, b, None, eps, self.max_iter, self.tol, x=pts[idx][0], y=pts[idx][1])
+                    while idx < n and arrivals[idx] <= now:
+                        a, b, _, eps = reqs[idx % R]
+                        t = srv.submit(a, b, None, eps, self.max_iter, self.tol, x=pts[idx % R][0],
+                                       y=pts[idx % R][1])
                         if t is None:
                             break
                         pending[t] = idx
@@ -862,32 +869,34 @@ class StreamWorkload:
             return lat, span
 
         run_server(np.zeros(R))  # warm-up
-        _, span_all = run_server(np.zeros(R))
-        cap = R / span_all
+        n_cap = min(n_req, 2000)
+        _, span_all = run_server(np.zeros(n_cap))
+        cap = n_cap / span_all
         svc = np.zeros(R)
         for i, (a, b, C, eps) in enumerate(reqs):
             t1 = time.perf_counter()
             rw.sinkhorn(a, b, C, {"reg": eps, "method": "log", "max_iter": self.max_iter, "zero_tol": self.tol})
             svc[i] = time.perf_counter() - t1
         ms = lambda x, q: float(np.percentile(x, q) * 1e3)  # noqa: E731
-        out = {"server_capacity_per_s": cap,
-               "capacity": "all requests submitted at once in the stream's order",
-               "arrivals": "Poisson (unit-rate exponential gaps of the stream / rate)",
+        out = {"server_capacity_per_s": cap, "requests_per_rate": n_req, "distinct_requests": R,
+               "capacity": f"{n_cap} requests submitted at once in the stream's order",
+               "arrivals": "Poisson (seeded unit-rate exponential gaps / rate)",
                "requests": "server: histograms + point clouds (cost built on the device); per call: histograms + "
                            "host cost matrix",
                "per_call_mean_service_ms": float(svc.mean() * 1e3)}
-        for frac in (0.5, 0.8):
+        for frac in (0.5, 0.8, 1.0):
             rate = frac * cap
             arrivals = np.cumsum(gaps) / rate
+            arrivals -= arrivals[0]
             lat, span = run_server(arrivals)
-            fin, plat = 0.0, np.zeros(R)
-            for i in range(R):
-                fin = max(fin, arrivals[i]) + svc[i]
+            fin, plat = 0.0, np.zeros(n_req)
+            for i in range(n_req):
+                fin = max(fin, arrivals[i]) + svc[i % R]
                 plat[i] = fin - arrivals[i]
             out[f"at_{int(frac * 100)}pct"] = {
                 "arrival_rate_per_s": rate,
-                "server": {"solves_per_s": R / span, "p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99)},
-                "per_call_fifo": {"solves_per_s": R / (fin - arrivals[0]), "p50_ms": ms(plat, 50),
+                "server": {"solves_per_s": n_req / span, "p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99)},
+                "per_call_fifo": {"solves_per_s": n_req / (fin - arrivals[0]), "p50_ms": ms(plat, 50),
                                   "p99_ms": ms(plat, 99)}}
         return out
 

@@ -259,9 +259,12 @@ RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_
  * running kernel, where free CTAs form its team as soon as enough are free
  * and solve it beside the others; rwig_server_poll returns 1 once the request is
  * finished (f, g and P copied to the pointers given at submit; out filled),
- * 0 while it runs.  submit returns the request's ticket (>= 0), or
- * RWIG_E_BUSY when admitting it would exceed the device-memory budget or the
- * slot table (512 requests) is full -- poll and retry.  The kernel ends after
+ * 0 while it runs.  submit returns the request's ticket (>= 0; tickets
+ * number the requests in submission order), or RWIG_E_BUSY when admitting it
+ * would exceed the device-memory budget or the request submitted 512 tickets
+ * earlier has not been collected yet (at most 512 requests are out at once;
+ * their descriptor slots are reused while the launch runs) -- poll and
+ * retry.  The kernel ends after
  * idle_ms without work and is restarted by the next submit or poll; while it
  * runs it holds every SM (other work on the GPU waits), so idle_ms trades the
  * restart of the launch (tens of microseconds) against that.

@@ -67,7 +67,8 @@ constexpr int kResident = kArea - kTree;   // largest resident strip (184 KB)
 constexpr int kWarpRows = 512;             // m <= this: warp-per-column passes
 constexpr int kMaxRows = 8192;
 constexpr int kUnit = 64;                  // rows per merge unit (4 per warp)
-constexpr int kMaxProbs = 512;
+constexpr int kMaxProbs = 512;             // descriptor slots; problem number h lives in slot h % kMaxProbs
+constexpr int kCtlPerSlot = 8;             // control words per slot (Prob::ctl)
 constexpr int kMaxTeam = 160;              // CTAs of a team (the grid is one CTA per SM)
 constexpr double kScaleMin = 5.1e-283, kScaleMax = 1.95e282;  // e^-650, e^650
 constexpr double kUnsafeStatus = -100.0;
@@ -96,7 +97,9 @@ struct Prob {
   double* colp;      // [2][gp][4] column-strip partials
   double* mrgp;      // [2][gp][4] merge partials (split merges)
   double* ug;        // [2][m] u (split merges)
-  unsigned* ctl;     // [0] claimed member slots, [1] team barrier arrivals, [2] 0 unopened, 1 opened, 2 opening
+  unsigned* ctl;     // kCtlPerSlot words: 64-bit claim word at [0] (problem number << 32 | gp << 16 |
+                     // claimed member slots), 64-bit state word at [2] (problem number << 32 | 0 unopened,
+                     // 1 opened, 2 opening), [4] team barrier arrivals
   double* res;       // [16]: loss, err, iter, status, l1 row, l1 col, l2 row, l2 col, device ns, formation
                      // ns, then member 0's ns in column passes, merges + decisions, team barriers
   int m, n, max_iter, gp, mode, nunits;
@@ -160,7 +163,7 @@ __device__ __forceinline__ bool team_sync(const Prob& p, unsigned& nb, bool form
   ++nb;
   if (threadIdx.x == 0) {
     const unsigned long long t = prof_wait ? globaltimer_ns() : 0ull;
-    sh.flag[0] = team_wait(p.ctl + 1, nb * (unsigned)p.gp, dctl, forming) ? 1 : 0;
+    sh.flag[0] = team_wait(p.ctl + 4, nb * (unsigned)p.gp, dctl, forming) ? 1 : 0;
     if (prof_wait) *prof_wait += (double)(globaltimer_ns() - t);
   }
   __syncthreads();
@@ -945,18 +948,6 @@ __device__ __noinline__ bool solve(const Prob& p, int pi, int k, const Shared sh
   return true;
 }
 
-// Claim of a member slot (thread 0).  Team formation with reservation:
-// F = (CTAs looking for work) - (unfilled slots of opened problems) never goes
-// below zero.  A CTA that starts looking adds one to F; it first takes an
-// unfilled slot of an opened problem; else it opens one -- the oldest
-// unopened problem, or (backfilling, while that one has waited less than
-// backfill_us) a later one in a window of kBackfillWindow -- by taking the
-// problem's gp from F with a compare-and-swap.  So every opened team has
-// enough free CTAs to fill it and no team waits on CTAs that are busy
-// elsewhere.  Returns the problem and member index, or pi = -1 when the launch
-// is closing (or on an error).  The published count is taken from pub[0]
-// until the launch closes (stop flag, or idle_ns with nothing to do and no
-// team running); after that it is frozen.
 constexpr int kBackfillWindow = 64;
 constexpr int kScanWindow = 256;  // problems from the scan start examined per pass
 
@@ -965,11 +956,43 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-
-__device__ __forceinline__ unsigned* problem_ctl(const Prob* probs, unsigned h) {
-  return reinterpret_cast<unsigned*>(__ldcg(reinterpret_cast<const unsigned long long*>(&probs[h].ctl)));
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
 
+__host__ __device__ __forceinline__ unsigned slot_of(unsigned h) { return h & (unsigned)(kMaxProbs - 1); }
+
+// Control words of problem number h: [0] the claim word, [1] the state word.
+__device__ __forceinline__ unsigned long long* problem_ctl(const Prob* probs, unsigned h) {
+  return reinterpret_cast<unsigned long long*>(
+      __ldcg(reinterpret_cast<const unsigned long long*>(&probs[slot_of(h)].ctl)));
+}
+__host__ __device__ __forceinline__ unsigned long long claim_word(unsigned h, int gp, int claimed) {
+  return ((unsigned long long)h << 32) | ((unsigned long long)(unsigned)gp << 16) | (unsigned)claimed;
+}
+__host__ __device__ __forceinline__ unsigned long long state_word(unsigned h, unsigned st) {
+  return ((unsigned long long)h << 32) | st;
+}
+
+// Claim of a member slot (thread 0).  Team formation with reservation:
+// F = (CTAs looking for work) - (unfilled slots of opened problems) never goes
+// below zero.  A CTA that starts looking adds one to F; it first takes an
+// unfilled slot of an opened problem; else it opens one -- the oldest
+// unopened problem, or (backfilling, while that one has waited less than
+// backfill_us) a later one in a window of kBackfillWindow -- by taking the
+// problem's gp from F with a compare-and-swap.  So every opened team has
+// enough free CTAs to fill it and no team waits on CTAs that are busy
+// elsewhere.  Problems are numbered in publication order and problem h lives
+// in descriptor slot h % kMaxProbs, which a server reuses once h has been
+// collected: the claim and state words carry the problem number and change
+// only by compare-and-swap, so a scan that meets a reused slot (its number is
+// no longer h) counts h as finished and never touches the new problem.
+// Returns the slot and member index, or pi = -1 when the launch is closing
+// (or on an error).  The published count is taken from pub[0] until the
+// launch closes (stop flag, or idle_ns with nothing to do and no work in
+// flight).
 __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned* dctl, unsigned long long idle_ns,
                       unsigned backfill_us, int& pi, int& k) {
   pi = -1;
@@ -988,42 +1011,50 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
       const unsigned now_us = (unsigned)(globaltimer_ns() / 1000ull);
       const unsigned last = ld_relaxed(dctl + DC_PUB_T);
       if (now_us - last >= 20u && atomicCAS(dctl + DC_PUB_T, last, now_us) == last) {
-        const unsigned p0 = min(pub[0], (unsigned)kMaxProbs);
+        const unsigned p0 = pub[0] & ~kClosed;
         if (p0 > npx) {
           atomicCAS(dctl + DC_AVAIL, W, p0);
           continue;
         }
       }
     }
-    // 1. an unfilled slot of an opened problem; states and claim counts are
+    // 1. an unfilled slot of an opened problem; the state and claim words are
     // read 8 problems at a time (the loads overlap)
     const unsigned head = ld_relaxed(dctl + DC_HEAD);
     const unsigned end = min(npx, head + kScanWindow);
     unsigned oldest = npx;  // oldest problem not yet opened
     bool open_slots = false, prefix_full = true;
     for (unsigned h0 = head; h0 < end; h0 += 8) {
-      unsigned st[8], cl[8];
-      int gp[8];
+      unsigned long long sw[8], cw[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const unsigned h = h0 + u;
-        unsigned* ctl = h < end ? problem_ctl(probs, h) : nullptr;
-        st[u] = ctl ? ld_relaxed(ctl + 2) : 1u;
-        cl[u] = ctl ? ld_relaxed(ctl) : 0u;
-        gp[u] = h < end ? __ldcg(&probs[h].gp) : 0;
+        unsigned long long* ctl = h < end ? problem_ctl(probs, h) : nullptr;
+        sw[u] = ctl ? ld_relaxed64(ctl + 1) : 0ull;
+        cw[u] = ctl ? ld_relaxed64(ctl) : 0ull;
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const unsigned h = h0 + u;
         if (h >= end) break;
-        if (st[u] == 1u) {
-          if ((int)cl[u] < gp[u]) {
+        // a slot that no longer carries h was reused: h is finished
+        const bool mine = (unsigned)(sw[u] >> 32) == h && (unsigned)(cw[u] >> 32) == h;
+        const unsigned st = mine ? (unsigned)sw[u] : 1u;
+        const int gp = (int)((cw[u] >> 16) & 0xffffu), cl = (int)(cw[u] & 0xffffu);
+        const bool unfilled = mine && st == 1u && cl < gp;
+        if (st == 1u) {
+          if (unfilled) {
             open_slots = true;
-            const unsigned c = atomicAdd(problem_ctl(probs, h), 1u);
-            if ((int)c < gp[u]) {
-              pi = (int)h;
-              k = (int)c;
-              return;
+            unsigned long long* ctl = problem_ctl(probs, h);
+            unsigned long long w = cw[u];
+            while ((unsigned)(w >> 32) == h && (int)(w & 0xffffu) < (int)((w >> 16) & 0xffffu)) {
+              const unsigned long long prev = atomicCAS(ctl, w, w + 1ull);
+              if (prev == w) {
+                pi = (int)slot_of(h);
+                k = (int)(w & 0xffffu);
+                return;
+              }
+              w = prev;
             }
           } else if (prefix_full) {
             atomicMax(dctl + DC_HEAD, h + 1);  // opened and full up to here: later scans start after it
@@ -1032,7 +1063,7 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
           prefix_full = false;
           if (oldest == npx) oldest = h;
         }
-        if (st[u] == 1u && (int)cl[u] < gp[u]) prefix_full = false;
+        if (unfilled) prefix_full = false;
       }
     }
     // 2. open a problem
@@ -1046,11 +1077,13 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
       bool opened = false;
       for (unsigned h = oldest; h < end && h < oldest + kBackfillWindow && !opened; ++h) {
         if (h != oldest && !backfill) break;
-        unsigned* ctl = problem_ctl(probs, h);
-        if (ld_relaxed(ctl + 2) != 0u) continue;
-        const int gp = __ldcg(&probs[h].gp);
+        unsigned long long* ctl = problem_ctl(probs, h);
+        if (ld_relaxed64(ctl + 1) != state_word(h, 0u)) continue;
+        const unsigned long long cw = ld_relaxed64(ctl);
+        if ((unsigned)(cw >> 32) != h) continue;
+        const int gp = (int)((cw >> 16) & 0xffffu);
         if (gp > (int)ld_relaxed(reinterpret_cast<unsigned*>(F))) continue;
-        if (atomicCAS(ctl + 2, 0u, 2u) != 0u) continue;  // another CTA is opening it
+        if (atomicCAS(ctl + 1, state_word(h, 0u), state_word(h, 2u)) != state_word(h, 0u)) continue;  // another CTA is opening it
         while (true) {
           const int f = (int)ld_relaxed(reinterpret_cast<unsigned*>(F));
           if (f < gp) break;
@@ -1059,7 +1092,7 @@ __device__ void claim(const Prob* probs, const volatile unsigned* pub, unsigned*
             break;
           }
         }
-        atomicExch(ctl + 2, opened ? 1u : 0u);
+        atomicExch(ctl + 1, state_word(h, opened ? 1u : 0u));
       }
       if (opened) continue;
     }
@@ -1237,7 +1270,7 @@ void bind(batch::Prob& d, double* k, double* w, double* res, unsigned* ctl) {
 }
 
 int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, const unsigned* pub, unsigned* done,
-                   unsigned* dctl, double* dprof, unsigned long long idle_ns, unsigned avail0) {
+                   unsigned* dctl, double* dprof, unsigned long long idle_ns, unsigned avail0, unsigned head0) {
   using namespace batch;
   static bool attr = false;
   if (!attr) {
@@ -1250,6 +1283,7 @@ int launch_service(Context* ctx, cudaStream_t st, const batch::Prob* dprob, cons
   if (nblk < 1) return set_error(RWIG_E_UNSUPPORTED, "batched Sinkhorn kernel does not fit on an SM");
   unsigned h0[kCtlWords] = {};
   h0[DC_AVAIL] = avail0;
+  h0[DC_HEAD] = head0;
   RWIG_CUDA_TRY(cudaMemcpyAsync(dctl, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
   const Prob* dp = dprob;
   const volatile unsigned* pb = pub;
@@ -1313,21 +1347,28 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   double* dW = (double*)scratch(ctx, SBT_WORK, sizeof(double) * std::max<long long>(wd, 32));
   double* dres = (double*)scratch(ctx, SBT_RES, sizeof(double) * kResStride * np);
   unsigned* ctrl = (unsigned*)scratch(ctx, SBT_CTRL, sizeof(unsigned) * (kCtlWords + 2 + kMaxProbs));
-  unsigned* pctl = (unsigned*)scratch(ctx, SBT_PCTL, sizeof(unsigned) * 4 * kMaxProbs);
+  unsigned* pctl = (unsigned*)scratch(ctx, SBT_PCTL, sizeof(unsigned) * kCtlPerSlot * kMaxProbs);
   const bool profile = option("batch.profile", 0.0) != 0.0;
   double* dprof = profile ? (double*)scratch(ctx, SBT_PROF, sizeof(double) * 4 * G) : nullptr;
   if (!dprob || !dK || !dW || !dres || !ctrl || !pctl || (profile && !dprof)) return RWIG_E_NOMEM;
-  for (int s = 0; s < np; ++s) bind(hp[s], dK + koff[s], dW + woff[s], dres + kResStride * (size_t)s, pctl + 4 * s);
+  // problem s in slot s: claim word (s, gp, 0), state word (s, unopened), team barrier 0
+  std::vector<unsigned long long> hwords((size_t)np * kCtlPerSlot / 2, 0ull);
+  for (int s = 0; s < np; ++s) {
+    bind(hp[s], dK + koff[s], dW + woff[s], dres + kResStride * (size_t)s, pctl + kCtlPerSlot * s);
+    hwords[(size_t)s * kCtlPerSlot / 2 + 0] = claim_word((unsigned)s, hp[s].gp, 0);
+    hwords[(size_t)s * kCtlPerSlot / 2 + 1] = state_word((unsigned)s, 0u);
+  }
   unsigned* pub = ctrl + kCtlWords;
   unsigned* done = ctrl + kCtlWords + 2;
   const unsigned hpub[2] = {(unsigned)np, 1u};
   RWIG_CUDA_TRY(cudaMemcpyAsync(dprob, hp.data(), sizeof(Prob) * np, cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpyAsync(pub, hpub, sizeof(hpub), cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned) * kMaxProbs, st));
-  RWIG_CUDA_TRY(cudaMemsetAsync(pctl, 0, sizeof(unsigned) * 4 * np, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(pctl, hwords.data(), sizeof(unsigned long long) * hwords.size(),
+                                cudaMemcpyHostToDevice, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(dres, 0, sizeof(double) * kResStride * np, st));
   if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));
-  const int rc = launch_service(ctx, st, dprob, pub, done, ctrl, dprof, 0ull, (unsigned)np | kClosed);
+  const int rc = launch_service(ctx, st, dprob, pub, done, ctrl, dprof, 0ull, (unsigned)np | kClosed, 0u);
   if (rc) return rc;
   if (profile) RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   ++*launches;
@@ -1564,9 +1605,12 @@ extern "C" int rwig_batch_sinkhorn_log_dev(const rwig_problem* probs, int count,
 // Serving: requests are admitted into the running service kernel as they
 // arrive (continuous batching).  The caller drives the server from one
 // thread: submit() copies a request in and publishes it, poll() collects
-// finished ones.  Admission is bounded by a device-memory budget and by the
-// slot table of one launch (kMaxProbs); a full table is reused once every
-// slot of it has been collected and the kernel has gone idle.
+// finished ones.  Requests are numbered in submission order (the ticket) and
+// request h lives in descriptor slot h % kMaxProbs, reused as soon as its
+// previous occupant has been collected (the kernel's claim and state words
+// carry the request number, so a reused slot is never mistaken for the old
+// request).  Admission is bounded by a device-memory budget and by the
+// kMaxProbs requests that may be out at once.
 // ---------------------------------------------------------------------------
 struct rwig_server {
   rwig::Context* ctx = nullptr;
@@ -1579,13 +1623,13 @@ struct rwig_server {
   double* hres = nullptr;                   // mapped: 10 results per slot
   double* dres = nullptr;
   unsigned* dctl = nullptr;                 // device control words
-  unsigned* dpctl = nullptr;                // device, 4 control words per slot
+  unsigned* dpctl = nullptr;                // device, kCtlPerSlot control words per slot
   // the requests' memory: a pool of the server's own that keeps what it has
   // mapped (release threshold: unlimited), so freeing a collected request
   // never unmaps device memory -- which would wait for the running launch
   cudaMemPool_t pool = nullptr;
   unsigned hctl_err = 0;
-  int nslots = 0, npub = 0, next_ticket = 0;
+  int nsub = 0, npub = 0;  // requests submitted (the next ticket) and published
   bool launched = false;
   double budget = 0.0, inflight = 0.0;
   unsigned long long idle_ns = 0;
@@ -1601,6 +1645,7 @@ struct rwig_server {
   };
   std::vector<Slot> slots;
   std::vector<rwig::batch::Prob> staged;  // host copies of the descriptors (asynchronous copy sources)
+  std::vector<unsigned long long> staged_ctl;  // and of the control words, kCtlPerSlot / 2 per slot
 };
 
 namespace rwig {
@@ -1620,11 +1665,20 @@ int ensure_running(rwig_server* s) {
   unsigned err = 0;
   RWIG_CUDA_TRY(cudaMemcpy(&err, s->dctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (err) return set_error(RWIG_E_TIMEOUT, "a bounded wait in the serving kernel expired");
+  // only the last kMaxProbs published requests can be unfinished; the new
+  // launch's scan starts at the first of them
   bool pending = false;
-  for (int i = 0; i < s->npub; ++i)
-    if (!s->hdone[i]) pending = true;
+  int head0 = s->npub;
+  for (int h = std::max(0, s->npub - batch::kMaxProbs); h < s->npub; ++h) {
+    const int slot = h % batch::kMaxProbs;
+    if (s->slots[slot].ticket == h && !s->hdone[slot]) {
+      pending = true;
+      head0 = std::min(head0, h);
+    }
+  }
   if (!pending) return 0;
-  const int rc = launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns, 0u);
+  const int rc =
+      launch_service(s->ctx, s->ks, s->dprob, s->dpub, s->ddone, s->dctl, nullptr, s->idle_ns, 0u, (unsigned)head0);
   if (rc) return rc;
   s->launched = true;
   return 0;
@@ -1633,8 +1687,8 @@ int ensure_running(rwig_server* s) {
 // Publishes, in slot order, the submitted requests whose copies have landed.
 int publish_ready(rwig_server* s) {
   const int before = s->npub;
-  while (s->npub < s->nslots) {
-    const cudaError_t e = cudaEventQuery(s->slots[s->npub].ev);
+  while (s->npub < s->nsub) {
+    const cudaError_t e = cudaEventQuery(s->slots[s->npub % batch::kMaxProbs].ev);
     if (e == cudaErrorNotReady) break;
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
     ++s->npub;
@@ -1664,6 +1718,7 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
   s->idle_ns = (unsigned long long)(std::max(0.0, idle_ms) * 1e6);
   s->slots.resize(batch::kMaxProbs);
   s->staged.resize(batch::kMaxProbs);
+  s->staged_ctl.assign((size_t)batch::kMaxProbs * batch::kCtlPerSlot / 2, 0ull);
   auto fail = [&](cudaError_t e, const char* what) {
     rwig_server_destroy(s);
     return cuda_fail(e, what);
@@ -1690,7 +1745,8 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
     if ((e = cudaFreeAsync(prime, s->cs)) != cudaSuccess) return fail(e, "memory pool");
     if ((e = cudaStreamSynchronize(s->cs)) != cudaSuccess) return fail(e, "memory pool");
   }
-  if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * 4 * batch::kMaxProbs)) != cudaSuccess) return fail(e, "slot control");
+  if ((e = cudaMalloc(&s->dpctl, sizeof(unsigned) * batch::kCtlPerSlot * batch::kMaxProbs)) != cudaSuccess)
+    return fail(e, "slot control");
   if ((e = cudaHostAlloc(&s->hpub, sizeof(unsigned) * 2, cudaHostAllocMapped)) != cudaSuccess) return fail(e, "pub");
   if ((e = cudaHostAlloc(&s->hdone, sizeof(unsigned) * batch::kMaxProbs, cudaHostAllocMapped)) != cudaSuccess)
     return fail(e, "done");
@@ -1719,17 +1775,20 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   if (q->M > batch::kMaxRows) return set_error(RWIG_E_UNSUPPORTED, "M above 8192");
   std::lock_guard<std::mutex> lk(s->ctx->mu);
   using namespace batch;
-  // a fresh slot table once every slot of the current one has been collected
-  if (s->nslots == kMaxProbs) {
+  // request numbers stay below the kernel's closed flag (bit 31): start again
+  // from 0 once everything is collected and no launch runs
+  if (s->nsub >= 0x7fff0000) {
     bool all = true;
-    for (int i = 0; i < s->nslots; ++i) all = all && s->slots[i].collected;
+    for (const auto& sl : s->slots) all = all && sl.collected;
     if (!all || kernel_running(s)) return RWIG_E_BUSY;
-    s->nslots = 0;
+    s->nsub = 0;
     s->npub = 0;
-    std::memset(s->hdone, 0, sizeof(unsigned) * kMaxProbs);
+    for (auto& sl : s->slots) sl.ticket = -1;
     std::atomic_thread_fence(std::memory_order_seq_cst);
     *(volatile unsigned*)s->hpub = 0u;
   }
+  const int slot = s->nsub % kMaxProbs;
+  if (!s->slots[slot].collected) return RWIG_E_BUSY;  // its previous request is still out
   Prob d{};
   long long kd = 0, wd = 0;
   place(*q, s->ctx->sm_count, d, kd, wd);
@@ -1752,7 +1811,6 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   double* dw = dk + kd;
   RWIG_CUDA_TRY(cudaMemcpyAsync(da, q->a, sizeof(double) * M, cudaMemcpyHostToDevice, s->cs));
   RWIG_CUDA_TRY(cudaMemcpyAsync(db, q->b, sizeof(double) * N, cudaMemcpyHostToDevice, s->cs));
-  const int slot = s->nslots;
   if (pts) {
     RWIG_CUDA_TRY(cudaMemcpyAsync(dC, q->X, sizeof(double) * M * q->d, cudaMemcpyHostToDevice, s->cs));
     RWIG_CUDA_TRY(
@@ -1769,13 +1827,19 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   d.f = df;
   d.g = dg;
   d.P = dP;
-  bind(d, dk, dw, s->dres + batch::kResStride * (size_t)slot, s->dpctl + 4 * (size_t)slot);
-  RWIG_CUDA_TRY(cudaMemsetAsync(s->dpctl + 4 * (size_t)slot, 0, sizeof(unsigned) * 4, s->cs));
+  bind(d, dk, dw, s->dres + batch::kResStride * (size_t)slot, s->dpctl + kCtlPerSlot * (size_t)slot);
+  // control words: claim (request, gp, 0), state (request, unopened), team barrier 0
+  unsigned long long* hc = s->staged_ctl.data() + (size_t)slot * kCtlPerSlot / 2;
+  for (int w = 0; w < kCtlPerSlot / 2; ++w) hc[w] = 0ull;
+  hc[0] = claim_word((unsigned)s->nsub, d.gp, 0);
+  hc[1] = state_word((unsigned)s->nsub, 0u);
+  RWIG_CUDA_TRY(cudaMemcpyAsync(s->dpctl + kCtlPerSlot * (size_t)slot, hc, sizeof(unsigned) * kCtlPerSlot,
+                                cudaMemcpyHostToDevice, s->cs));
   s->staged[slot] = d;  // the copy source must outlive the asynchronous copy
   RWIG_CUDA_TRY(cudaMemcpyAsync(s->dprob + slot, &s->staged[slot], sizeof(Prob), cudaMemcpyHostToDevice, s->cs));
   RWIG_CUDA_TRY(cudaEventRecord(s->slots[slot].ev, s->cs));
   auto& sl = s->slots[slot];
-  sl.ticket = s->next_ticket++;
+  sl.ticket = s->nsub;
   sl.mem = mem;
   sl.bytes = bytes;
   sl.df = df;
@@ -1789,7 +1853,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   sl.collected = false;
   s->inflight += bytes;
   s->hdone[slot] = 0u;
-  s->nslots = slot + 1;
+  ++s->nsub;
   const int rc = publish_ready(s);
   if (rc) return rc;
   return sl.ticket;
@@ -1799,11 +1863,10 @@ extern "C" int rwig_server_poll(rwig_server* s, int ticket, rwig_result* out) {
   reset_report();
   if (!s || !out) return set_error(RWIG_E_INVALID, "null server or result");
   std::lock_guard<std::mutex> lk(s->ctx->mu);
-  int slot = -1;
-  for (int i = 0; i < s->nslots; ++i)
-    if (s->slots[i].ticket == ticket && !s->slots[i].collected) slot = i;
-  if (slot < 0) return set_error(RWIG_E_INVALID, "unknown or already collected ticket");
-  if (slot >= s->npub || !*(volatile unsigned*)(s->hdone + slot)) {
+  const int slot = ticket >= 0 ? ticket % batch::kMaxProbs : -1;
+  if (slot < 0 || ticket >= s->nsub || s->slots[slot].ticket != ticket || s->slots[slot].collected)
+    return set_error(RWIG_E_INVALID, "unknown or already collected ticket");
+  if (ticket >= s->npub || !*(volatile unsigned*)(s->hdone + slot)) {
     const int rc = publish_ready(s);  // and restart a kernel that went idle before seeing it
     return rc ? rc : 0;
   }

@@ -110,3 +110,41 @@ def test_cost_from_points_matches_host_cost():
         got = _wait(srv, tickets)
     for u, v in zip(rc, got):
         assert np.array_equal(u["f"], v["f"]) and u["iter"] == v["iter"]
+
+
+def test_slot_reuse_over_many_requests():
+    """More requests than descriptor slots (512): request h lives in slot
+    h % 512, reused once its previous request has been collected, without the
+    launch draining.  1300 requests cycling over 8 problems, submitted as the
+    window of outstanding tickets allows, with a pause longer than idle_ms in
+    the middle (the launch ends and the next one starts its scan at the first
+    unfinished request); every result bitwise equals the batched call's."""
+    small = [(64, 64, 0.1, 2), (100, 37, 0.1, 3), (37, 100, 0.1, 64), (200, 150, 0.05, 2), (128, 300, 0.1, 3),
+             (90, 90, 0.05, 2), (300, 64, 0.1, 2), (150, 200, 0.1, 3)]
+    probs = [_prob(100 + i, *s) for i, s in enumerate(small)]
+    ref = rw.batch_sinkhorn_log(probs)
+    n_req, window = 1300, 700
+    got = {}
+    with rw.Server(idle_ms=2.0) as srv:
+        pending = {}
+        nxt, t0 = 0, time.time()
+        while len(got) < n_req:
+            while nxt < n_req and len(pending) < window:
+                q = probs[nxt % len(probs)]
+                t = srv.submit(q["a"], q["b"], q["C"], q["reg"], q["max_iter"], q["zero_tol"])
+                if t is None:
+                    break
+                assert t == nxt  # tickets are request numbers
+                pending[t] = nxt
+                nxt += 1
+                if nxt == 650:
+                    time.sleep(0.05)  # > idle_ms: the launch may end while requests are out
+            for t in list(pending):
+                r = srv.poll(t)
+                if r is not None:
+                    got[pending.pop(t)] = r
+            assert time.time() - t0 < 120.0, "server did not finish"
+    for h in range(n_req):
+        e = ref[h % len(probs)]
+        assert np.array_equal(got[h]["f"], e["f"]) and np.array_equal(got[h]["g"], e["g"]), h
+        assert got[h]["iter"] == e["iter"] and got[h]["loss"] == e["loss"], h
