@@ -77,7 +77,8 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "batch.strip_kb": target K strip per team member of a batched problem,
  *       at most 184 (default); strips up to that stay in shared memory;
  *   "batch.max_team": largest team of CTAs per batched problem (default:
- *       0.4 x the SM count);
+ *       0.25 x the SM count for rwig_batch_sinkhorn_log*, 0.4 x for a
+ *       server);
  *   "batch.resident_team": problems with M > 512 keep their K strips in
  *       shared memory when that takes at most this many CTAs (default 32),
  *       else stream strips of about "batch.stream_strip_kb" (default 1024)
@@ -269,9 +270,11 @@ RWIG_API int rwig_batch_sinkhorn_log(const rwig_problem* probs, int count, rwig_
  * runs it holds every SM (other work on the GPU waits), so idle_ms trades the
  * restart of the launch (tens of microseconds) against that.
  * Requests are allocated from a memory pool of the server's own, which keeps
- * what it maps until rwig_server_destroy; create maps min(budget, 4 GB) of it
- * up front, and the pool grows on demand up to the budget.
- * Results are bitwise those of rwig_batch_sinkhorn_log for the same problem.
+ * what it maps until rwig_server_destroy; create maps the whole budget up
+ * front (at most 80 % of the free device memory; beyond that the pool grows
+ * on demand, which waits for the running launch).
+ * Results are bitwise those of rwig_batch_sinkhorn_log for the same problem
+ * under the same "batch.max_team" (set explicitly: the two defaults differ).
  * One thread drives a server. */
 typedef struct rwig_server rwig_server;
 RWIG_API int rwig_server_create(rwig_server** out, double mem_budget_bytes, double idle_ms);

@@ -35,8 +35,9 @@ OPTIONS = ("batch.max_team", "batch.resident_team", "batch.stream_strip_kb", "ba
 
 
 def defaults(sm_count: int) -> dict:
-    """Built-in values of the tuned options (rwig_b200/csrc/batch.cu)."""
-    return {"batch.max_team": float(math.floor(0.4 * sm_count)), "batch.resident_team": 32.0,
+    """Built-in values of the tuned options for a batched call
+    (rwig_b200/csrc/batch.cu; a server's largest team is 0.4 x the SMs)."""
+    return {"batch.max_team": float(math.floor(0.25 * sm_count)), "batch.resident_team": 32.0,
             "batch.stream_strip_kb": 1024.0, "batch.strip_kb": 184.0, "batch.redundant_rows": 16384.0,
             "batch.backfill_us": 5000.0}
 
@@ -121,7 +122,7 @@ def _device_batch(problems, dev):
     return keep, arr
 
 
-def autotune_batch(problems, space=None, reps: int = 2, min_gain: float = 0.02, apply: bool = True,
+def autotune_batch(problems, space=None, reps: int = 3, min_gain: float = 0.03, apply: bool = True,
                    loss_rtol: float = 1e-9) -> dict:
     """Tune the batch.* options for `problems` (dicts as in
     batch_sinkhorn_log: a, b, C or point clouds x, y, reg, max_iter,

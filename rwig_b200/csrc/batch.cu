@@ -1210,7 +1210,7 @@ enum { SBT_DESC = 200, SBT_K, SBT_WORK, SBT_CTRL, SBT_PROF, SBT_RES, SBT_PCTL, S
 // problem, the SM count and the engine options batch.strip_kb,
 // batch.max_team, batch.redundant_rows and batch.l2_keep_mb) and the sizes of
 // its K and work arrays.
-void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, long long& wdoubles) {
+void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, long long& wdoubles, bool server) {
   using namespace batch;
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   d = Prob{};
@@ -1220,7 +1220,10 @@ void place(const rwig_problem& q, int G, batch::Prob& d, long long& kdoubles, lo
   const long long strip_target = (long long)(option("batch.strip_kb", 184.0) * 1024.0 / 8.0);
   const long long cols = std::max<long long>(1, std::min<long long>(kResident, strip_target) / d.ldk);
   const int gp_res = (int)((q.N + cols - 1) / cols);
-  const int maxteam = std::max(1, std::min(G, (int)option("batch.max_team", std::floor(0.4 * G))));
+  // largest team: a quarter of the SMs for a batched call (throughput: more
+  // problems side by side), 0.4 for a server (latency: each request done sooner)
+  const int maxteam =
+      std::max(1, std::min(G, (int)option("batch.max_team", std::floor((server ? 0.4 : 0.25) * G))));
   const int res_team = std::min(maxteam, (int)option("batch.resident_team", 32.0));
   int mode = 0;
   if (gp_res <= res_team || (q.M <= kWarpRows && gp_res <= maxteam)) {
@@ -1336,7 +1339,7 @@ static int launch_group(Context* ctx, cudaStream_t st, const rwig_problem* probs
   long long kd = 0, wd = 0;
   for (int s = 0; s < np; ++s) {
     long long k1, w1;
-    place(probs[idx[ord[s]]], G, hp[s], k1, w1);
+    place(probs[idx[ord[s]]], G, hp[s], k1, w1, false);
     koff[s] = kd;
     woff[s] = wd;
     kd += k1;
@@ -1737,10 +1740,13 @@ extern "C" int rwig_server_create(rwig_server** out, double mem_budget_bytes, do
     unsigned long long keep = ~0ull;
     if ((e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
       return fail(e, "memory pool");
-    // map up to 4 GB of the budget now, while no launch runs (growing the
-    // pool later waits for the running launch)
+    // map the whole budget now (at most 80 % of the free memory), while no
+    // launch runs: growing the pool later waits for the running launch, which
+    // stalled admission whenever the requests out at once outgrew the mapping
     void* prime = nullptr;
-    const size_t pb = (size_t)std::min(mem_budget_bytes, 4.0 * (1ull << 30));
+    size_t free_b = 0, total_b = 0;
+    if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) return fail(e, "memory info");
+    const size_t pb = (size_t)std::min(mem_budget_bytes, 0.8 * (double)free_b);
     if ((e = cudaMallocFromPoolAsync(&prime, pb, s->pool, s->cs)) != cudaSuccess) return fail(e, "memory pool");
     if ((e = cudaFreeAsync(prime, s->cs)) != cudaSuccess) return fail(e, "memory pool");
     if ((e = cudaStreamSynchronize(s->cs)) != cudaSuccess) return fail(e, "memory pool");
@@ -1791,7 +1797,7 @@ extern "C" int rwig_server_submit(rwig_server* s, const rwig_problem* q) {
   if (!s->slots[slot].collected) return RWIG_E_BUSY;  // its previous request is still out
   Prob d{};
   long long kd = 0, wd = 0;
-  place(*q, s->ctx->sm_count, d, kd, wd);
+  place(*q, s->ctx->sm_count, d, kd, wd, true);
   auto al = [](long long x) { return ((x + 31) / 32) * 32; };
   const long long M = q->M, N = q->N;
   const long long cd = pts ? al(M * q->d) + al(N * q->d) : al(M * N);  // C, or the points

@@ -35,6 +35,22 @@ def _wait(server, tickets, timeout=60.0):
     return [out[t] for t in tickets]
 
 
+class _SameTeams:
+    """Sets batch.max_team for the block: a server's and a batched call's
+    default team limits differ, and their results are bitwise equal under the
+    same limit."""
+
+    def __enter__(self):
+        import torch
+        from rwig_b200 import _lib
+        sm = torch.cuda.get_device_properties(0).multi_processor_count
+        assert _lib.load().rwig_set_option(b"batch.max_team", float(int(0.4 * sm))) == 0
+
+    def __exit__(self, *exc):
+        from rwig_b200 import _lib
+        _lib.load().rwig_set_option(b"batch.max_team", float("nan"))
+
+
 def _submit(server, q):
     while True:
         t = server.submit(q["a"], q["b"], q["C"], q["reg"], q["max_iter"], q["zero_tol"])
@@ -45,7 +61,7 @@ def _submit(server, q):
 
 def test_in_mix_equals_alone_and_oracle():
     probs = [_prob(i, *s) for i, s in enumerate(SIZES)]
-    with rw.Server(idle_ms=5.0) as srv:
+    with _SameTeams(), rw.Server(idle_ms=5.0) as srv:
         alone = []
         for q in probs:  # one at a time
             alone.append(_wait(srv, [_submit(srv, q)])[0])
@@ -59,7 +75,8 @@ def test_in_mix_equals_alone_and_oracle():
         for key in ("f", "g"):
             assert np.array_equal(mix[k][key], alone[i][key]), (i, key)
         assert mix[k]["loss"] == alone[i]["loss"] and mix[k]["iter"] == alone[i]["iter"]
-    batch = rw.batch_sinkhorn_log(probs)
+    with _SameTeams():
+        batch = rw.batch_sinkhorn_log(probs)
     for i, q in enumerate(probs):
         assert np.array_equal(batch[i]["f"], alone[i]["f"]) and batch[i]["iter"] == alone[i]["iter"]
     for i in (0, 2, 5):
@@ -99,13 +116,14 @@ def test_cost_from_points_matches_host_cost():
         with_c.append({"a": a, "b": b, "C": synth.sq_euclid_cost(x, y), "reg": reg, "max_iter": 2000,
                        "zero_tol": 1e-9})
         with_pts.append({"a": a, "b": b, "x": x, "y": y, "reg": reg, "max_iter": 2000, "zero_tol": 1e-9})
-    rc = rw.batch_sinkhorn_log(with_c, with_plan=True)
-    rp = rw.batch_sinkhorn_log(with_pts, with_plan=True)
+    with _SameTeams():
+        rc = rw.batch_sinkhorn_log(with_c, with_plan=True)
+        rp = rw.batch_sinkhorn_log(with_pts, with_plan=True)
     for u, v in zip(rc, rp):
         for k in ("f", "g", "P"):
             assert np.array_equal(u[k], v[k]), k
         assert u["loss"] == v["loss"] and u["iter"] == v["iter"]
-    with rw.Server(idle_ms=2.0) as srv:
+    with _SameTeams(), rw.Server(idle_ms=2.0) as srv:
         tickets = [srv.submit(q["a"], q["b"], None, q["reg"], 2000, 1e-9, x=q["x"], y=q["y"]) for q in with_pts]
         got = _wait(srv, tickets)
     for u, v in zip(rc, got):
@@ -122,10 +140,11 @@ def test_slot_reuse_over_many_requests():
     small = [(64, 64, 0.1, 2), (100, 37, 0.1, 3), (37, 100, 0.1, 64), (200, 150, 0.05, 2), (128, 300, 0.1, 3),
              (90, 90, 0.05, 2), (300, 64, 0.1, 2), (150, 200, 0.1, 3)]
     probs = [_prob(100 + i, *s) for i, s in enumerate(small)]
-    ref = rw.batch_sinkhorn_log(probs)
+    with _SameTeams():
+        ref = rw.batch_sinkhorn_log(probs)
     n_req, window = 1300, 700
     got = {}
-    with rw.Server(idle_ms=2.0) as srv:
+    with _SameTeams(), rw.Server(idle_ms=2.0) as srv:
         pending = {}
         nxt, t0 = 0, time.time()
         while len(got) < n_req:
