@@ -89,7 +89,13 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "batch.l2_keep_mb": streamed problems whose K is at most this many MB
  *       read it with an L2 evict_last hint (default 48);
  *   "batch.max_elems": problems with more elements go through the per-call
- *       path (default 2^26).
+ *       path (default 2^26);
+ *   "batch.backfill_us": how long the oldest waiting problem may be passed
+ *       over by later ones that fit the free CTAs (default 5000);
+ *   "wdl.infer_docs": documents per stacked-column chunk of WDL inference
+ *       (default 1024);
+ *   "dgemm.kshape", "dgemm.tile": DMMA instruction shape (k = 4, 8 or 16)
+ *       and tile height (0 automatic, 64, 128) of rwig_selftest_dgemm only.
  * The batch.* options change team shapes and therefore the summation order
  * of a batched result (within rounding); a result is the same alone and in
  * any mix under the same options.  A NaN value clears the option (its
