@@ -497,14 +497,75 @@ class BarycenterWorkload:
                 args.steps, "parallel barycenter + gradient on this workload's inputs (the reference has no GPU log "
                             "barycenter): cuda_barycenter_parallel (src/cuda_barycenter.cu:268) vs "
                             "rw.barycenter(method='parallel'), host arrays")
+        batch = self.batch_timing(dev)
         return {"value": args.steps * world / (tot_ms / 1e3), "ms_per_step": tot_ms / args.steps,
-                "reference_gpu": ref_gpu,
+                "reference_gpu": ref_gpu, "batch": batch,
                 "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (256 MB write)"},
                 "e2e": {"value": args.steps * world / e2e_s, "unit": self.unit,
                         "h2d_bytes_per_step": MS + NN + (S + n) * 8, "d2h_bytes_per_step": 3 * MS + (n + S) * 8},
                 "gpu_launches": sum(r["kernel_launches"] for r in reps), "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clocks.summary()}
+
+    def batch_timing(self, dev):
+        """16 log barycenters with gradient of uneven sizes (N in {256, 512,
+        1024, 2048} x S in {4, 8, 16, 32}, L = 50, fixed iteration count) on
+        device buffers: one rwig_batch_barycenter_dev call against 16
+        rwig_barycenter_log_dev calls on the same stream, each the median of
+        3 rounds timed with CUDA events; results compared bitwise."""
+        import torch
+
+        from rwig_b200 import _lib, synth
+        L = _lib.load()
+        stream = torch.cuda.current_stream()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        vp = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        shapes = [(nn, ss) for nn in (256, 512, 1024, 2048) for ss in (4, 8, 16, 32)]
+        keep = []
+        arr = (_lib.BaryProblem * len(shapes))()
+        res = (_lib.BaryResult * len(shapes))()
+        for i, (nn, ss) in enumerate(shapes):
+            A, C, w, be = synth.barycenter_config(n=nn, S=ss, dim=10, salt=50 + i)
+            t = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (A.T, C.T, w, be)]
+            outs = [torch.empty(ss * nn, dtype=torch.float64, device=dev) for _ in range(3)] + \
+                   [torch.empty(nn, dtype=torch.float64, device=dev), torch.empty(ss, dtype=torch.float64, device=dev)]
+            keep.append((t, outs, nn, ss))
+            arr[i] = _lib.BaryProblem(vp(t[0]), vp(t[2]), vp(t[1]), vp(t[3]), nn, nn, ss, self.reg, 1, 1, self.L, 0.0,
+                                      vp(outs[0]), vp(outs[1]), vp(outs[3]), vp(outs[2]), vp(outs[4]))
+
+        def batched():
+            _lib.check(L.rwig_batch_barycenter_dev(arr, len(shapes), res, sp))
+
+        loss, err, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+
+        def one_by_one():
+            for (t, outs, nn, ss) in keep:
+                _lib.check(L.rwig_barycenter_log_dev(vp(outs[0]), vp(outs[1]), vp(outs[3]), vp(outs[2]), vp(outs[4]),
+                                                     ctypes.byref(loss), ctypes.byref(it), ctypes.byref(err),
+                                                     vp(t[0]), vp(t[2]), vp(t[1]), vp(t[3]), nn, nn, ss, self.reg, 1,
+                                                     self.L, 0.0, sp))
+
+        def timed(fn):
+            fn()
+            ts = []
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return float(np.median(ts))
+
+        b_ms = timed(batched)
+        bref = [[o.clone() for o in outs] for (_, outs, _, _) in keep]
+        s_ms = timed(one_by_one)
+        same = all(torch.equal(a, b) for (_, outs, _, _), br in zip(keep, bref) for a, b in zip(outs, br))
+        n = len(shapes)
+        return {"problems": n, "shapes": "N in {256, 512, 1024, 2048} x S in {4, 8, 16, 32}, log, gradient, L = 50",
+                "batched_solves_per_s": n / (b_ms / 1e3), "one_by_one_solves_per_s": n / (s_ms / 1e3),
+                "speedup": s_ms / b_ms, "bitwise_equal": bool(same)}
 
     def reference(self, args):
         threads = os.cpu_count() or 1

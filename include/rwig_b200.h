@@ -184,6 +184,45 @@ RWIG_API int rwig_barycenter_log_dev(double* F, double* G, double* b, double* gr
                                      int N, int S, double reg, int withgrad, int max_iter,
                                      double zero_tol, void* stream);
 
+/* Many independent barycenter problems in one call.  No counterpart in the
+ * reference (one barycenter per call).  Each problem has its own sizes,
+ * method (0 parallel, 1 log), regularisation and iteration control, and the
+ * argument meaning of rwig_barycenter_*_dev; all arrays are device pointers
+ * and the outputs X1 (U or F), X2 (V or G), b, grad_A, grad_w may be NULL.
+ * Problems with a fixed iteration count (zero_tol <= 0) are queued side by
+ * side on streams forked from `stream` (NULL = the engine's stream), so their
+ * small products share the GPU; problems with a stopping test (zero_tol > 0)
+ * read their error on the host every iteration and run one after another.
+ * out[i]: loss, err, iter and status (0 converged, 1 max_iter, 2 other, < 0
+ * an error of that problem alone).  Each result equals the single call's on
+ * the same problem bitwise.  Returns 0 once every output is written, or a
+ * negative error. */
+typedef struct rwig_bary_problem {
+  const double* A;     /* M x S */
+  const double* w;     /* S */
+  const double* C;     /* M x N */
+  const double* b_ext; /* N (withgrad) */
+  int M, N, S;
+  double reg;
+  int method;   /* 0 parallel, 1 log */
+  int withgrad;
+  int max_iter;
+  double zero_tol;
+  double* X1;     /* U (parallel) or F (log), M x S */
+  double* X2;     /* V or G, N x S */
+  double* b;      /* N */
+  double* grad_A; /* M x S */
+  double* grad_w; /* S */
+} rwig_bary_problem;
+
+typedef struct rwig_bary_result {
+  double loss, err;
+  int iter, status;
+} rwig_bary_result;
+
+RWIG_API int rwig_batch_barycenter_dev(const rwig_bary_problem* probs, int count, rwig_bary_result* out,
+                                       void* stream);
+
 /* Wasserstein dictionary learning.
  *
  * rwig_wdl replaces cuda_wdl (inst/include/cuda_interface.cuh:31-39, called

@@ -67,6 +67,18 @@ class Problem(ctypes.Structure):
                 ("zero_tol", _d), ("P", _vp), ("f", _vp), ("g", _vp), ("X", _vp), ("Y", _vp), ("d", _i)]
 
 
+class BaryProblem(ctypes.Structure):
+    """rwig_bary_problem (include/rwig_b200.h)."""
+    _fields_ = [("A", _vp), ("w", _vp), ("C", _vp), ("b_ext", _vp), ("M", _i), ("N", _i), ("S", _i), ("reg", _d),
+                ("method", _i), ("withgrad", _i), ("max_iter", _i), ("zero_tol", _d), ("X1", _vp), ("X2", _vp),
+                ("b", _vp), ("grad_A", _vp), ("grad_w", _vp)]
+
+
+class BaryResult(ctypes.Structure):
+    """rwig_bary_result (include/rwig_b200.h)."""
+    _fields_ = [("loss", _d), ("err", _d), ("iter", _i), ("status", _i)]
+
+
 class Result(ctypes.Structure):
     """rwig_result (include/rwig_b200.h)."""
     _fields_ = [("loss", _d), ("err", _d), ("iter", _i), ("status", _i), ("marg_l1_row", _d),
@@ -109,6 +121,7 @@ SIGNATURES = {
     "rwig_wdl_batch_grad_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _i, _i, _vp]),
     "rwig_batch_sinkhorn_log": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result)]),
     "rwig_batch_sinkhorn_log_dev": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result), _vp]),
+    "rwig_batch_barycenter_dev": (_i, [ctypes.POINTER(BaryProblem), _i, ctypes.POINTER(BaryResult), _vp]),
     "rwig_server_create": (_i, [ctypes.POINTER(_vp), _d, _d]),
     "rwig_server_submit": (_i, [_vp, ctypes.POINTER(Problem)]),
     "rwig_server_poll": (_i, [_vp, _i, ctypes.POINTER(Result)]),

@@ -177,6 +177,65 @@ def barycenter(A, C, w, b_ext=None, barycenter_control: dict | None = None) -> d
     return out
 
 
+def batch_barycenter(problems) -> list:
+    """Many barycenter problems in one call (rwig_batch_barycenter_dev):
+    `problems` is an iterable of dicts with A, C, w, optional b_ext and
+    optional control entries as in barycenter() (reg, method "log" or
+    "parallel", with_grad, max_iter, zero_tol).  Problems with a fixed
+    iteration count (zero_tol <= 0) run side by side on the GPU.  Returns one
+    dict per problem with the keys of barycenter()'s result."""
+    import torch
+    dev = torch.device("cuda", 0)
+    problems = list(problems)
+    n = len(problems)
+    arr = (_lib.BaryProblem * max(n, 1))()
+    res = (_lib.BaryResult * max(n, 1))()
+    keep, meta = [], []
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev) if x is not None else None  # noqa: E731
+    vp = lambda x: ctypes.c_void_p(x.data_ptr()) if x is not None else None  # noqa: E731
+    for i, q in enumerate(problems):
+        A = np.asfortranarray(np.asarray(q["A"], dtype=np.float64))
+        C = np.asfortranarray(np.asarray(q["C"], dtype=np.float64))
+        w = np.asarray(q["w"], dtype=np.float64).ravel()
+        ctrl = check_barycenter_args({k: v for k, v in q.items() if k not in ("A", "C", "w", "b_ext")})
+        method = ctrl["method"]
+        if method == "auto":
+            method = "log" if choose_sinkhorn_method(C, ctrl["reg"], ctrl["threshold"]) == "log" else "parallel"
+        wg = bool(ctrl["with_grad"])
+        if A.ndim != 2 or C.ndim != 2 or A.shape[0] != C.shape[0] or w.shape[0] != A.shape[1]:
+            raise ValueError(f"problem {i}: A (M x S), C (M x N) and w (S) don't match")
+        if wg and q.get("b_ext") is None:
+            raise ValueError(f"problem {i}: you must supply the `b_ext` with `with_grad = TRUE`!")
+        M, S = A.shape
+        N = C.shape[1]
+        tA, tC, tw = t(A.T), t(C.T), t(w)  # column-major on the device
+        tbe = t(np.asarray(q["b_ext"], dtype=np.float64).ravel()) if wg else None
+        X1 = torch.empty((S, M), dtype=torch.float64, device=dev)
+        X2 = torch.empty((S, N), dtype=torch.float64, device=dev)
+        b = torch.empty(N, dtype=torch.float64, device=dev)
+        gA = torch.empty((S, M), dtype=torch.float64, device=dev) if wg else None
+        gw = torch.empty(S, dtype=torch.float64, device=dev) if wg else None
+        keep.append((tA, tC, tw, tbe, X1, X2, b, gA, gw))
+        meta.append((method, wg))
+        arr[i] = _lib.BaryProblem(vp(tA), vp(tw), vp(tC), vp(tbe), M, N, S, float(ctrl["reg"]),
+                                  1 if method == "log" else 0, int(wg), int(ctrl["max_iter"]), float(ctrl["zero_tol"]),
+                                  vp(X1), vp(X2), vp(b), vp(gA), vp(gw))
+    _lib.check(_lib.load().rwig_batch_barycenter_dev(arr, n, res, None))
+    out = []
+    for i in range(n):
+        tA, tC, tw, tbe, X1, X2, b, gA, gw = keep[i]
+        method, wg = meta[i]
+        r = res[i]
+        names = ("F", "G") if method == "log" else ("U", "V")
+        d = {"b": b.cpu().numpy(), names[0]: np.asfortranarray(X1.cpu().numpy().T),
+             names[1]: np.asfortranarray(X2.cpu().numpy().T), "iter": r.iter, "err": r.err,
+             "return_status": r.status, "method": method}
+        if wg:
+            d.update(grad_A=np.asfortranarray(gA.cpu().numpy().T), grad_w=gw.cpu().numpy(), loss=r.loss)
+        out.append(d)
+    return out
+
+
 def wdl_cpp(Y, C, reg, S, batch_size, epochs, sinkhorn_mode=1, max_iter=1000, zero_tol=1e-6, optimizer=2,
             eta=0.001, gamma=0.01, beta1=0.9, beta2=0.999, eps=1e-8, verbose=False, seed=42, Alpha0=None,
             Lambda0=None, max_steps=0) -> dict:

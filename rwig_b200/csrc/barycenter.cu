@@ -364,6 +364,202 @@ enum {
   SB_T, SB_T2, SB_GA, SB_GWP, SB_GW, SB_A, SB_W, SB_C, SB_BEXT, SB_OUTU, SB_OUTV, SB_OUTB
 };
 
+// One barycenter solve: its device buffers (engine scratch slots, numbered
+// from `off` so that several solves can be enqueued side by side) and its
+// launch sequence.  All pointers on the device.
+struct Solve {
+  Context* ctx = nullptr;
+  bool logdomain = false;
+  double *X1 = nullptr, *X2 = nullptr, *b = nullptr, *gradA = nullptr, *gradw = nullptr;
+  const double *A = nullptr, *w = nullptr, *C = nullptr, *bext = nullptr;
+  int M = 0, N = 0, S = 0, withgrad = 0, L = 0;
+  double reg = 0.0, tol = 0.0;
+  size_t MS = 0, NS = 0;
+  long long ldk = 0, ldd = 0;
+  int H = 0, ngrp = 0;
+  // tol <= 0: the iteration count is fixed (L) and err is only needed after
+  // the last iteration, so the whole launch sequence is known up front
+  bool fixed = true;
+  double *K = nullptr, *Uh = nullptr, *Vh = nullptr, *Zh = nullptr, *Yh = nullptr, *Bh = nullptr;
+  double *logA = nullptr, *D = nullptr, *gram = nullptr, *bn = nullptr, *scal = nullptr;
+  double *T = nullptr, *T2 = nullptr, *gA = nullptr, *gwp = nullptr, *gw = nullptr;
+  int launches = 0, iter = 0;
+  double err = 1000.0;
+
+  double* slot(double* base, size_t sz, int l) const { return base + sz * (size_t)(withgrad ? l : (l & 1)); }
+
+  // Sizes from the arguments; buffers from scratch slots off + SB_*,
+  // allocated before anything is enqueued (a captured sequence must not
+  // allocate).
+  int alloc(int off) {
+    L = std::max(0, L);
+    MS = (size_t)M * S;
+    NS = (size_t)N * S;
+    ldk = ((M + 1) / 2) * 2;
+    ldd = ((M + 1) / 2) * 2;
+    // history depth: every iteration's state when gradients are needed, else two
+    H = withgrad ? L + 2 : 2;
+    ngrp = (N + 7) / 8;
+    fixed = !(tol > 0.0);
+    K = (double*)scratch(ctx, off + SB_K, sizeof(double) * ldk * N);
+    Uh = (double*)scratch(ctx, off + SB_UH, sizeof(double) * MS * H);
+    Vh = (double*)scratch(ctx, off + SB_VH, sizeof(double) * NS * H);
+    Zh = (double*)scratch(ctx, off + SB_ZH, sizeof(double) * NS * H);
+    Yh = (double*)scratch(ctx, off + SB_YH, sizeof(double) * MS * H);
+    Bh = (double*)scratch(ctx, off + SB_BH, sizeof(double) * (size_t)N * H);
+    logA = (double*)scratch(ctx, off + SB_LOGA, sizeof(double) * MS);
+    D = (double*)scratch(ctx, off + SB_D, sizeof(double) * ldd * S);
+    gram = (double*)scratch(ctx, off + SB_GRAM, sizeof(double) * (size_t)S * S);
+    bn = (double*)scratch(ctx, off + SB_BN, sizeof(double) * N);
+    scal = (double*)scratch(ctx, off + SB_SCAL, sizeof(double) * 8);
+    if (!K || !Uh || !Vh || !Zh || !Yh || !Bh || !logA || !D || !gram || !bn || !scal) return RWIG_E_NOMEM;
+    if (withgrad) {
+      T = (double*)scratch(ctx, off + SB_T, sizeof(double) * MS);
+      T2 = (double*)scratch(ctx, off + SB_T2, sizeof(double) * NS);
+      gA = (double*)scratch(ctx, off + SB_GA, sizeof(double) * MS);
+      gwp = (double*)scratch(ctx, off + SB_GWP, sizeof(double) * (size_t)ngrp * S);
+      gw = (double*)scratch(ctx, off + SB_GW, sizeof(double) * S);
+      if (!T || !T2 || !gA || !gwp || !gw) return RWIG_E_NOMEM;
+    }
+    return 0;
+  }
+
+  // err from the Gram matrix of the residual D: Frobenius (parallel, :134) or
+  // spectral (log, :252)
+  void err_from_gram(const double* G) {
+    if (logdomain) {
+      err = std::sqrt(lambda_max(std::vector<double>(G, G + (size_t)S * S), S));
+    } else {
+      double tr = 0.0;
+      for (int s = 0; s < S; ++s) tr += G[s + s * S];
+      err = std::sqrt(tr);
+    }
+  }
+
+  // The whole solve on stream q (with tol > 0 the stopping test reads err
+  // on the host after every iteration).
+  int enqueue(cudaStream_t q) {
+  launches = 0;
+  iter = 0;
+  err = 1000.0;
+  gibbs_kernel<<<grid_for(ctx, ldk * N), TPB, 0, q>>>(C, M, N, ldk, reg, K);  // K = exp(-C/reg)
+  log_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(A, MS, logA);
+  fill_kernel<<<grid_for(ctx, NS), TPB, 0, q>>>(slot(Vh, NS, 0), NS, 1.0);  // V_0 = 1
+  launches += 3;
+  // Y = K X (rows M, contraction N) and Z = K^T X (rows N, contraction M)
+  auto gemm_y = [&](const double* X, auto epi) -> int {
+    return dg::gemm<0>(ctx, dg::GemmArgs{K, ldk, M, N, S, X, N, 0}, epi, q, 0, &launches);
+  };
+  auto gemm_z = [&](const double* X, auto epi) -> int {
+    return dg::gemm<1>(ctx, dg::GemmArgs{K, ldk, N, M, S, X, M, 0}, epi, q, 0, &launches);
+  };
+  // Y_0 = K V_0, U_1 = A / Y_0
+  int rc = gemm_y(slot(Vh, NS, 0), EpiY{A, logA, nullptr, slot(Yh, MS, 0), slot(Uh, MS, 1), nullptr, M, S,
+                                        (int)ldd, logdomain ? 1 : 0});
+  if (rc) return rc;
+  while (iter < L && err >= tol) {
+    ++iter;
+    const int l = iter;
+    double* Ul = slot(Uh, MS, l);
+    // Z_l = K^T U_l; b_l; V_l = b_l / Z_l
+    rc = gemm_z(Ul, EpiZ{w, slot(Zh, NS, l), slot(Vh, NS, l), slot(Bh, N, l), N, S, logdomain ? 1 : 0});
+    if (rc) return rc;
+    // Y_l = K V_l; U_{l+1} = A / Y_l; residual when the stopping test needs it
+    const bool need_err = !fixed || (iter == L);
+    rc = gemm_y(slot(Vh, NS, l), EpiY{A, logA, Ul, slot(Yh, MS, l), slot(Uh, MS, l + 1),
+                                      need_err ? D : nullptr, M, S, (int)ldd, logdomain ? 1 : 0});
+    if (rc) return rc;
+    if (need_err) {
+      rc = dg::gemm<1>(ctx, dg::GemmArgs{D, ldd, S, M, S, D, ldd, 0}, dg::EpiStore{gram, S, S}, q, 0, &launches);
+      if (rc) return rc;
+      if (!fixed) {  // the stopping test needs err now
+        std::vector<double> G((size_t)S * S);
+        RWIG_CUDA_TRY(cudaMemcpyAsync(G.data(), gram, sizeof(double) * S * S, cudaMemcpyDeviceToHost, q));
+        RWIG_CUDA_TRY(cudaStreamSynchronize(q));
+        err_from_gram(G.data());
+      }
+    }
+  }
+  RWIG_CUDA_TRY(cudaGetLastError());
+
+  // normalised barycenter and loss (log: before the backward, :268-271;
+  // parallel: the backward uses the un-normalised b, :35-42)
+  if (iter > 0) {
+    normalise_b<<<1, 1024, 0, q>>>(slot(Bh, N, iter), N, logdomain, withgrad ? bext : nullptr, bn, scal);
+  } else {
+    // no iteration: parallel b = 0 / sum(0) (barycenter_impl_parallel.cpp:64, :39);
+    // log b = exp(0) / N (barycenter_impl_log.cpp:193, :268-269)
+    fill_kernel<<<grid_for(ctx, N), TPB, 0, q>>>(bn, N, logdomain ? 1.0 / N : NAN);
+  }
+  ++launches;
+
+  if (withgrad && iter > 0) {
+    RWIG_CUDA_TRY(cudaMemsetAsync(gA, 0, sizeof(double) * MS, q));
+    RWIG_CUDA_TRY(cudaMemsetAsync(gwp, 0, sizeof(double) * (size_t)ngrp * S, q));
+    for (int l = iter; l >= 1; --l) {
+      const bool seed = (l == iter);
+      const EpiB1 e1{slot(Zh, NS, l), slot(Vh, NS, l), w, slot(Bh, N, l), bn, bext, reg, N, S,
+                     logdomain ? 1 : 0, seed ? 1 : 0, T2, gwp};
+      if (seed) {
+        seed_b1<<<ngrp, dg::NTH, sizeof(double) * (S + 1) * 8, q>>>(e1, N);
+        ++launches;
+      } else {
+        rc = gemm_z(T, e1);  // K^T T
+        if (rc) return rc;
+      }
+      rc = gemm_y(T2, EpiB2{slot(Uh, MS, l), slot(Yh, MS, l - 1), A, M, S, logdomain ? 1 : 0, gA, T});  // K T2
+      if (rc) return rc;
+    }
+    reduce_gw<<<S, 256, 0, q>>>(gwp, ngrp, S, gw);
+    ++launches;
+    if (logdomain) {
+      scale_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(gA, MS, reg);  // :376
+      ++launches;
+    }
+    if (gradA) RWIG_CUDA_TRY(cudaMemcpyAsync(gradA, gA, sizeof(double) * MS, cudaMemcpyDeviceToDevice, q));
+    if (gradw) RWIG_CUDA_TRY(cudaMemcpyAsync(gradw, gw, sizeof(double) * S, cudaMemcpyDeviceToDevice, q));
+  }
+
+  // outputs: U, V (parallel) or F = eps log U, G = eps log V (log) of the last iteration
+  const double* Ufin = slot(Uh, MS, iter > 0 ? iter : 0);
+  const double* Vfin = slot(Vh, NS, iter);
+  if (iter == 0) {
+    fill_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(slot(Uh, MS, 0), MS, 1.0);  // U = 1 (:67)
+    ++launches;
+  }
+  if (X1) {
+    if (logdomain) {
+      log_scaled<<<grid_for(ctx, MS), TPB, 0, q>>>(Ufin, MS, reg, X1);
+      ++launches;
+    } else {
+      RWIG_CUDA_TRY(cudaMemcpyAsync(X1, Ufin, sizeof(double) * MS, cudaMemcpyDeviceToDevice, q));
+    }
+  }
+  if (X2) {
+    if (logdomain) {
+      log_scaled<<<grid_for(ctx, NS), TPB, 0, q>>>(Vfin, NS, reg, X2);
+      ++launches;
+    } else {
+      RWIG_CUDA_TRY(cudaMemcpyAsync(X2, Vfin, sizeof(double) * NS, cudaMemcpyDeviceToDevice, q));
+    }
+  }
+  if (b) RWIG_CUDA_TRY(cudaMemcpyAsync(b, bn, sizeof(double) * N, cudaMemcpyDeviceToDevice, q));
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+  }
+};
+
+// Checks of the arguments common to the single and batched entries.
+int check_args(const double* A, const double* w, const double* C, const double* bext, int M, int N, int S,
+               double reg, int withgrad) {
+  if (!A || !w || !C) return set_error(RWIG_E_INVALID, "A, w and C must be non-null");
+  if (M < 1 || N < 1 || S < 1) return set_error(RWIG_E_INVALID, "M, N and S must be >= 1");
+  if (S > 64) return set_error(RWIG_E_UNSUPPORTED, "more than 64 histograms");
+  if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
+  if (withgrad && !bext) return set_error(RWIG_E_INVALID, "b_ext is required with withgrad");
+  return 0;
+}
+
 // Core driver; all pointers on the device.  Outputs (any may be null):
 // U, V (parallel) or F, G (log) as X1, X2; b (normalised); grad_A, grad_w.
 int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, double* b, double* gradA,
@@ -371,169 +567,36 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
         const double* C, const double* bext, int M, int N, int S, double reg, int withgrad, int max_iter,
         double tol) {
   reset_report();
-  if (!A || !w || !C) return set_error(RWIG_E_INVALID, "A, w and C must be non-null");
-  if (M < 1 || N < 1 || S < 1) return set_error(RWIG_E_INVALID, "M, N and S must be >= 1");
-  if (S > 64) return set_error(RWIG_E_UNSUPPORTED, "more than 64 histograms");
-  if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
-  if (withgrad && !bext) return set_error(RWIG_E_INVALID, "b_ext is required with withgrad");
-  const int L = std::max(0, max_iter);
-  const size_t MS = (size_t)M * S, NS = (size_t)N * S;
-  const long long ldk = ((M + 1) / 2) * 2;
-  // history depth: every iteration's state when gradients are needed, else two
-  const int H = withgrad ? L + 2 : 2;
-  double* K = (double*)scratch(ctx, SB_K, sizeof(double) * ldk * N);
-  double* Uh = (double*)scratch(ctx, SB_UH, sizeof(double) * MS * H);
-  double* Vh = (double*)scratch(ctx, SB_VH, sizeof(double) * NS * H);
-  double* Zh = (double*)scratch(ctx, SB_ZH, sizeof(double) * NS * H);
-  double* Yh = (double*)scratch(ctx, SB_YH, sizeof(double) * MS * H);
-  double* Bh = (double*)scratch(ctx, SB_BH, sizeof(double) * (size_t)N * H);
-  double* logA = (double*)scratch(ctx, SB_LOGA, sizeof(double) * MS);
-  const long long ldd = ((M + 1) / 2) * 2;
-  double* D = (double*)scratch(ctx, SB_D, sizeof(double) * ldd * S);
-  double* gram = (double*)scratch(ctx, SB_GRAM, sizeof(double) * (size_t)S * S);
-  double* bn = (double*)scratch(ctx, SB_BN, sizeof(double) * N);
-  double* scal = (double*)scratch(ctx, SB_SCAL, sizeof(double) * 8);
-  if (!K || !Uh || !Vh || !Zh || !Yh || !Bh || !logA || !D || !gram || !bn || !scal) return RWIG_E_NOMEM;
-  auto slot = [&](double* base, size_t sz, int l) { return base + sz * (size_t)(withgrad ? l : (l & 1)); };
-  // backward buffers, allocated before anything is enqueued (a captured
-  // sequence must not allocate)
-  const int ngrp = (N + 7) / 8;
-  double *T = nullptr, *T2 = nullptr, *gA = nullptr, *gwp = nullptr, *gw = nullptr;
-  if (withgrad) {
-    T = (double*)scratch(ctx, SB_T, sizeof(double) * MS);
-    T2 = (double*)scratch(ctx, SB_T2, sizeof(double) * NS);
-    gA = (double*)scratch(ctx, SB_GA, sizeof(double) * MS);
-    gwp = (double*)scratch(ctx, SB_GWP, sizeof(double) * (size_t)ngrp * S);
-    gw = (double*)scratch(ctx, SB_GW, sizeof(double) * S);
-    if (!T || !T2 || !gA || !gwp || !gw) return RWIG_E_NOMEM;
-  }
-  // tol <= 0: the iteration count is fixed (L) and err is only needed after
-  // the last iteration, so the whole launch sequence is known up front
-  const bool fixed = !(tol > 0.0);
-  int launches = 0;
-  double err = 1000.0;
-  int iter = 0;
-
-  // err from the Gram matrix of the residual D: Frobenius (parallel, :134) or
-  // spectral (log, :252)
-  auto err_from_gram = [&](const std::vector<double>& G) {
-    if (logdomain) {
-      err = std::sqrt(lambda_max(G, S));
-    } else {
-      double tr = 0.0;
-      for (int s = 0; s < S; ++s) tr += G[s + s * S];
-      err = std::sqrt(tr);
-    }
-  };
-  auto enqueue = [&](cudaStream_t q) -> int {
-    launches = 0;
-    iter = 0;
-    err = 1000.0;
-    gibbs_kernel<<<grid_for(ctx, ldk * N), TPB, 0, q>>>(C, M, N, ldk, reg, K);  // K = exp(-C/reg)
-    log_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(A, MS, logA);
-    fill_kernel<<<grid_for(ctx, NS), TPB, 0, q>>>(slot(Vh, NS, 0), NS, 1.0);  // V_0 = 1
-    launches += 3;
-    // Y = K X (rows M, contraction N) and Z = K^T X (rows N, contraction M)
-    auto gemm_y = [&](const double* X, auto epi) -> int {
-      return dg::gemm<0>(ctx, dg::GemmArgs{K, ldk, M, N, S, X, N, 0}, epi, q, 0, &launches);
-    };
-    auto gemm_z = [&](const double* X, auto epi) -> int {
-      return dg::gemm<1>(ctx, dg::GemmArgs{K, ldk, N, M, S, X, M, 0}, epi, q, 0, &launches);
-    };
-    // Y_0 = K V_0, U_1 = A / Y_0
-    int rc = gemm_y(slot(Vh, NS, 0), EpiY{A, logA, nullptr, slot(Yh, MS, 0), slot(Uh, MS, 1), nullptr, M, S,
-                                          (int)ldd, logdomain ? 1 : 0});
-    if (rc) return rc;
-    while (iter < L && err >= tol) {
-      ++iter;
-      const int l = iter;
-      double* Ul = slot(Uh, MS, l);
-      // Z_l = K^T U_l; b_l; V_l = b_l / Z_l
-      rc = gemm_z(Ul, EpiZ{w, slot(Zh, NS, l), slot(Vh, NS, l), slot(Bh, N, l), N, S, logdomain ? 1 : 0});
-      if (rc) return rc;
-      // Y_l = K V_l; U_{l+1} = A / Y_l; residual when the stopping test needs it
-      const bool need_err = !fixed || (iter == L);
-      rc = gemm_y(slot(Vh, NS, l), EpiY{A, logA, Ul, slot(Yh, MS, l), slot(Uh, MS, l + 1),
-                                        need_err ? D : nullptr, M, S, (int)ldd, logdomain ? 1 : 0});
-      if (rc) return rc;
-      if (need_err) {
-        rc = dg::gemm<1>(ctx, dg::GemmArgs{D, ldd, S, M, S, D, ldd, 0}, dg::EpiStore{gram, S, S}, q, 0, &launches);
-        if (rc) return rc;
-        if (!fixed) {  // the stopping test needs err now
-          std::vector<double> G((size_t)S * S);
-          RWIG_CUDA_TRY(cudaMemcpyAsync(G.data(), gram, sizeof(double) * S * S, cudaMemcpyDeviceToHost, q));
-          RWIG_CUDA_TRY(cudaStreamSynchronize(q));
-          err_from_gram(G);
-        }
-      }
-    }
-    RWIG_CUDA_TRY(cudaGetLastError());
-
-    // normalised barycenter and loss (log: before the backward, :268-271;
-    // parallel: the backward uses the un-normalised b, :35-42)
-    if (iter > 0) {
-      normalise_b<<<1, 1024, 0, q>>>(slot(Bh, N, iter), N, logdomain, withgrad ? bext : nullptr, bn, scal);
-    } else {
-      // no iteration: parallel b = 0 / sum(0) (barycenter_impl_parallel.cpp:64, :39);
-      // log b = exp(0) / N (barycenter_impl_log.cpp:193, :268-269)
-      fill_kernel<<<grid_for(ctx, N), TPB, 0, q>>>(bn, N, logdomain ? 1.0 / N : NAN);
-    }
-    ++launches;
-
-    if (withgrad && iter > 0) {
-      RWIG_CUDA_TRY(cudaMemsetAsync(gA, 0, sizeof(double) * MS, q));
-      RWIG_CUDA_TRY(cudaMemsetAsync(gwp, 0, sizeof(double) * (size_t)ngrp * S, q));
-      for (int l = iter; l >= 1; --l) {
-        const bool seed = (l == iter);
-        const EpiB1 e1{slot(Zh, NS, l), slot(Vh, NS, l), w, slot(Bh, N, l), bn, bext, reg, N, S,
-                       logdomain ? 1 : 0, seed ? 1 : 0, T2, gwp};
-        if (seed) {
-          seed_b1<<<ngrp, dg::NTH, sizeof(double) * (S + 1) * 8, q>>>(e1, N);
-          ++launches;
-        } else {
-          rc = gemm_z(T, e1);  // K^T T
-          if (rc) return rc;
-        }
-        rc = gemm_y(T2, EpiB2{slot(Uh, MS, l), slot(Yh, MS, l - 1), A, M, S, logdomain ? 1 : 0, gA, T});  // K T2
-        if (rc) return rc;
-      }
-      reduce_gw<<<S, 256, 0, q>>>(gwp, ngrp, S, gw);
-      ++launches;
-      if (logdomain) {
-        scale_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(gA, MS, reg);  // :376
-        ++launches;
-      }
-      if (gradA) RWIG_CUDA_TRY(cudaMemcpyAsync(gradA, gA, sizeof(double) * MS, cudaMemcpyDeviceToDevice, q));
-      if (gradw) RWIG_CUDA_TRY(cudaMemcpyAsync(gradw, gw, sizeof(double) * S, cudaMemcpyDeviceToDevice, q));
-    }
-
-    // outputs: U, V (parallel) or F = eps log U, G = eps log V (log) of the last iteration
-    const double* Ufin = slot(Uh, MS, iter > 0 ? iter : 0);
-    const double* Vfin = slot(Vh, NS, iter);
-    if (iter == 0) {
-      fill_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(slot(Uh, MS, 0), MS, 1.0);  // U = 1 (:67)
-      ++launches;
-    }
-    if (X1) {
-      if (logdomain) {
-        log_scaled<<<grid_for(ctx, MS), TPB, 0, q>>>(Ufin, MS, reg, X1);
-        ++launches;
-      } else {
-        RWIG_CUDA_TRY(cudaMemcpyAsync(X1, Ufin, sizeof(double) * MS, cudaMemcpyDeviceToDevice, q));
-      }
-    }
-    if (X2) {
-      if (logdomain) {
-        log_scaled<<<grid_for(ctx, NS), TPB, 0, q>>>(Vfin, NS, reg, X2);
-        ++launches;
-      } else {
-        RWIG_CUDA_TRY(cudaMemcpyAsync(X2, Vfin, sizeof(double) * NS, cudaMemcpyDeviceToDevice, q));
-      }
-    }
-    if (b) RWIG_CUDA_TRY(cudaMemcpyAsync(b, bn, sizeof(double) * N, cudaMemcpyDeviceToDevice, q));
-    RWIG_CUDA_TRY(cudaGetLastError());
-    return 0;
-  };
+  if (int rc = check_args(A, w, C, bext, M, N, S, reg, withgrad)) return rc;
+  Solve sv;
+  sv.ctx = ctx;
+  sv.logdomain = logdomain;
+  sv.X1 = X1;
+  sv.X2 = X2;
+  sv.b = b;
+  sv.gradA = gradA;
+  sv.gradw = gradw;
+  sv.A = A;
+  sv.w = w;
+  sv.C = C;
+  sv.bext = bext;
+  sv.M = M;
+  sv.N = N;
+  sv.S = S;
+  sv.reg = reg;
+  sv.withgrad = withgrad;
+  sv.L = max_iter;
+  sv.tol = tol;
+  if (int rc = sv.alloc(0)) return rc;
+  const bool fixed = sv.fixed;
+  const int L = sv.L;
+  auto enqueue = [&](cudaStream_t q) { return sv.enqueue(q); };
+  int& launches = sv.launches;
+  int& iter = sv.iter;
+  double& err = sv.err;
+  const double *K = sv.K, *Uh = sv.Uh, *Vh = sv.Vh, *Zh = sv.Zh, *Yh = sv.Yh, *Bh = sv.Bh, *logA = sv.logA;
+  const double *D = sv.D, *gram = sv.gram, *bn = sv.bn, *scal = sv.scal;
+  const double *T = sv.T, *T2 = sv.T2, *gA = sv.gA, *gwp = sv.gwp, *gw = sv.gw;
 
   // A fixed sequence that repeats the previous call's arguments and buffers
   // is captured once into a CUDA graph and replayed from then on.
@@ -616,7 +679,7 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   }
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   RWIG_CUDA_TRY(cudaGetLastError());
-  if (fixed && iter > 0) err_from_gram(G);
+  if (fixed && iter > 0) sv.err_from_gram(G.data());
   if (loss) *loss = withgrad ? sc[1] : 0.0;
   if (iter_out) *iter_out = iter;
   if (err_out) *err_out = err;
@@ -634,6 +697,138 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   R.support_n = N;
   R.bary_norm = sc[0];
   return status;
+}
+
+// Side streams of the batched entry (created on first use, kept).
+constexpr int kSideStreams = 8;
+cudaStream_t side_stream(int i) {
+  static cudaStream_t pool[kSideStreams] = {};
+  if (!pool[i] && cudaStreamCreateWithFlags(&pool[i], cudaStreamNonBlocking) != cudaSuccess) {
+    (void)cudaGetLastError();
+    pool[i] = nullptr;
+  }
+  return pool[i];
+}
+
+// First scratch slot of the i-th solve of a batch (clear of every other
+// entry's slot numbers).
+constexpr int kBatchSlotBase = 1000, kBatchSlotStride = 32;
+
+// Many barycenter problems: those with a fixed iteration count enqueued
+// side by side on the side streams (each with its own scratch slots), their
+// Gram matrices and scalars copied to pinned memory, one wait at the end;
+// the others through run() one after another.
+int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int count, rwig_bary_result* out) {
+  reset_report();
+  std::vector<Solve> sv((size_t)count);
+  std::vector<int> fixed_ids, serial_ids;
+  for (int i = 0; i < count; ++i) {
+    const rwig_bary_problem& q = probs[i];
+    out[i] = rwig_bary_result{0.0, 0.0, 0, 0};
+    const int rc = (q.method == 0 || q.method == 1)
+                       ? check_args(q.A, q.w, q.C, q.b_ext, q.M, q.N, q.S, q.reg, q.withgrad)
+                       : set_error(RWIG_E_INVALID, "method must be 0 (parallel) or 1 (log)");
+    if (rc) {
+      out[i].status = rc;
+      continue;
+    }
+    if (q.zero_tol > 0.0) {
+      serial_ids.push_back(i);
+      continue;
+    }
+    Solve& s = sv[i];
+    s.ctx = ctx;
+    s.logdomain = q.method == 1;
+    s.X1 = q.X1;
+    s.X2 = q.X2;
+    s.b = q.b;
+    s.gradA = q.grad_A;
+    s.gradw = q.grad_w;
+    s.A = q.A;
+    s.w = q.w;
+    s.C = q.C;
+    s.bext = q.b_ext;
+    s.M = q.M;
+    s.N = q.N;
+    s.S = q.S;
+    s.reg = q.reg;
+    s.withgrad = q.withgrad;
+    s.L = q.max_iter;
+    s.tol = q.zero_tol;
+    const int rc2 = s.alloc(kBatchSlotBase + kBatchSlotStride * (int)fixed_ids.size());
+    if (rc2) {
+      out[i].status = rc2;
+      continue;
+    }
+    fixed_ids.push_back(i);
+  }
+  int launches = 0;
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
+  if (!fixed_ids.empty()) {
+    // pinned results: per solve the Gram matrix (S x S) and two scalars
+    size_t need = 0;
+    std::vector<size_t> at(fixed_ids.size());
+    for (size_t k = 0; k < fixed_ids.size(); ++k) {
+      at[k] = need;
+      need += (size_t)sv[fixed_ids[k]].S * sv[fixed_ids[k]].S + 2;
+    }
+    if (ctx->pinned_bytes < need * sizeof(double)) {
+      if (ctx->pinned) cudaFreeHost(ctx->pinned);
+      ctx->pinned = nullptr;
+      ctx->pinned_bytes = 0;
+      RWIG_CUDA_TRY(cudaHostAlloc(&ctx->pinned, need * sizeof(double), cudaHostAllocDefault));
+      ctx->pinned_bytes = need * sizeof(double);
+    }
+    double* hp = (double*)ctx->pinned;
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));  // inputs ready on the caller's stream
+    bool used[kSideStreams] = {};
+    for (size_t k = 0; k < fixed_ids.size(); ++k) {
+      Solve& s = sv[fixed_ids[k]];
+      const int si = (int)(k % kSideStreams);
+      cudaStream_t q = side_stream(si);
+      if (!q) return set_error(RWIG_E_CUDA, "could not create a side stream");
+      if (!used[si]) RWIG_CUDA_TRY(cudaStreamWaitEvent(q, ctx->evk, 0));
+      used[si] = true;
+      if (int rc = s.enqueue(q)) return rc;
+      launches += s.launches;
+      if (s.iter > 0) {
+        RWIG_CUDA_TRY(cudaMemcpyAsync(hp + at[k], s.gram, sizeof(double) * s.S * s.S, cudaMemcpyDeviceToHost, q));
+        RWIG_CUDA_TRY(cudaMemcpyAsync(hp + at[k] + (size_t)s.S * s.S, s.scal, sizeof(double) * 2,
+                                      cudaMemcpyDeviceToHost, q));
+      }
+    }
+    for (int si = 0; si < kSideStreams; ++si)
+      if (used[si]) RWIG_CUDA_TRY(cudaStreamSynchronize(side_stream(si)));
+    RWIG_CUDA_TRY(cudaGetLastError());
+    for (size_t k = 0; k < fixed_ids.size(); ++k) {
+      Solve& s = sv[fixed_ids[k]];
+      rwig_bary_result& r = out[fixed_ids[k]];
+      if (s.iter > 0) s.err_from_gram(hp + at[k]);
+      r.loss = (s.withgrad && s.iter > 0) ? hp[at[k] + (size_t)s.S * s.S + 1] : 0.0;
+      r.err = s.err;
+      r.iter = s.iter;
+      r.status = (s.err <= s.tol) ? 0 : (s.iter == s.L ? 1 : 2);
+    }
+  }
+  for (int i : serial_ids) {
+    const rwig_bary_problem& q = probs[i];
+    int it = 0;
+    double loss = 0.0, err = 0.0;
+    const int rc = run(ctx, st, q.method == 1, q.X1, q.X2, q.b, q.grad_A, q.grad_w, &loss, &it, &err, q.A, q.w, q.C,
+                       q.b_ext, q.M, q.N, q.S, q.reg, q.withgrad, q.max_iter, q.zero_tol);
+    launches += report().kernel_launches;
+    out[i] = rwig_bary_result{loss, err, it, rc};
+  }
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
+  RWIG_CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  reset_report();
+  rwig_report& R = report();
+  R.device_ms = ms;
+  R.kernel_ms = ms;
+  R.kernel_launches = launches;
+  return 0;
 }
 
 // Host-pointer wrapper: copies in, runs, copies out.
@@ -702,6 +897,16 @@ extern "C" int rwig_barycenter_parallel_dev(double* U, double* V, double* b, dou
   std::lock_guard<std::mutex> lk(ctx->mu);
   return bary::run(ctx, stream ? (cudaStream_t)stream : ctx->stream, false, U, V, b, grad_A, grad_w, loss, iter,
                    err, A, w, C, b_ext, M, N, S, reg, withgrad, max_iter, zero_tol);
+}
+
+extern "C" int rwig_batch_barycenter_dev(const rwig_bary_problem* probs, int count, rwig_bary_result* out,
+                                         void* stream) {
+  if (count < 0 || (count > 0 && (!probs || !out))) return set_error(RWIG_E_INVALID, "bad problem array");
+  if (count == 0) return 0;
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return bary::run_batch(ctx, stream ? (cudaStream_t)stream : ctx->stream, probs, count, out);
 }
 
 extern "C" int rwig_barycenter_log_dev(double* F, double* G, double* b, double* grad_A, double* grad_w,
