@@ -518,6 +518,9 @@ struct Solve {
     }
     if (gradA) RWIG_CUDA_TRY(cudaMemcpyAsync(gradA, gA, sizeof(double) * MS, cudaMemcpyDeviceToDevice, q));
     if (gradw) RWIG_CUDA_TRY(cudaMemcpyAsync(gradw, gw, sizeof(double) * S, cudaMemcpyDeviceToDevice, q));
+  } else if (withgrad) {  // no iteration to unroll: the gradient is zero
+    if (gradA) RWIG_CUDA_TRY(cudaMemsetAsync(gradA, 0, sizeof(double) * MS, q));
+    if (gradw) RWIG_CUDA_TRY(cudaMemsetAsync(gradw, 0, sizeof(double) * S, q));
   }
 
   // outputs: U, V (parallel) or F = eps log U, G = eps log V (log) of the last iteration

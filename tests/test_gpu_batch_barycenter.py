@@ -56,6 +56,8 @@ def test_batch_equals_single_calls():
         assert got[i]["err"] == ref["err"] or (np.isnan(got[i]["err"]) and np.isnan(ref["err"])), i
         if q["with_grad"]:
             assert got[i]["loss"] == ref["loss"], i
+        if q["with_grad"] and q["max_iter"] == 0:  # nothing unrolled: zero gradient
+            assert not got[i]["grad_A"].any() and not got[i]["grad_w"].any()
 
 
 def test_batch_against_oracle():
