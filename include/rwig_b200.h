@@ -351,9 +351,11 @@ RWIG_API int rwig_selftest_dgemm(const double* K, long long ldk, int trans, int 
  * library until exit; the call makes no device allocation.
  * Limits: M, N <= 4096, a and b strictly positive, M even, C 16-byte aligned
  * (column-major, leading dimension M); anything else returns
- * RWIG_E_UNSUPPORTED.  P, f, g are device outputs (any may be NULL); loss,
- * iter, err are host pointers; `stream` is a cudaStream_t (NULL: legacy
- * default stream).  All calls on a device share the block: calls that overlap
+ * RWIG_E_UNSUPPORTED; a negative max_iter returns RWIG_E_INVALID.  P, f, g
+ * are device outputs (any may be NULL); loss, iter, err are host pointers;
+ * `stream` is a cudaStream_t (NULL: legacy default stream).  The call waits
+ * for its work on `stream` before it returns (loss, iter and err are read
+ * back to the host).  All calls on a device share the block: calls that overlap
  * on the GPU race and must be serialised by the caller.  The first call on a
  * device looks up the block's address; make it before any stream capture. */
 RWIG_API int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double* loss, int* iter,

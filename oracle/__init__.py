@@ -35,16 +35,19 @@ def build(force: bool = False) -> str:
 
 
 _REF_GPU_PATH = os.path.join(_HERE, "_ref", "librwig_ref_gpu.so")
-_REF_SOURCES = os.environ.get("RWIG_REFERENCE_DIR", "/root/reference")
 _ref_gpu = None
 
 
-def build_ref_gpu() -> str | None:
-    """Compile rwig's own GPU vanilla Sinkhorn and parallel barycenter from the
-    reference's sources (``make -C oracle ref``) when those sources are present;
-    elsewhere the prebuilt library is used as is."""
-    if os.path.isdir(os.path.join(_REF_SOURCES, "src")):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={_REF_SOURCES}"], check=True)
+def build_ref_gpu(ref_dir: str | None = None) -> str | None:
+    """Compile rwig's own GPU vanilla Sinkhorn, parallel barycenter and WDL from
+    the reference's sources (``make -C oracle ref REF=<dir>``).  The source tree
+    is ``ref_dir`` or the environment variable ``RWIG_REFERENCE_DIR``; with
+    neither set nothing is built and the prebuilt library (if any) is used."""
+    src = ref_dir or os.environ.get("RWIG_REFERENCE_DIR")
+    if src:
+        if not os.path.isdir(os.path.join(src, "src")):
+            raise RuntimeError(f"not an rwig source tree (no src/): {src}")
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={src}"], check=True)
     return _REF_GPU_PATH if os.path.exists(_REF_GPU_PATH) else None
 
 
@@ -57,7 +60,7 @@ def ref_gpu():
     global _ref_gpu
     if _ref_gpu is None:
         if not os.path.exists(_REF_GPU_PATH):
-            raise RuntimeError(f"reference GPU library not built: {_REF_GPU_PATH} (make -C oracle ref)")
+            raise RuntimeError(f"reference GPU library not built: {_REF_GPU_PATH} (make -C oracle ref REF=...)")
         L = ctypes.CDLL(_REF_GPU_PATH)
         i, d = ctypes.c_int, ctypes.c_double
         L.ref_gpu_sinkhorn_vanilla.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, i, i, d, i, i, d]
@@ -65,8 +68,42 @@ def ref_gpu():
         L.ref_gpu_barycenter_parallel.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp,
                                                   i, i, i, d, i, i, d]
         L.ref_gpu_barycenter_parallel.restype = None
+        L.ref_gpu_wdl.argtypes = [_dp, _dp, _dp, _dp, _dp, i, i, i, d, i, d, i, i, i, d, d, d, d, d, i]
+        L.ref_gpu_wdl.restype = None
+        L.ref_gpu_wdl_batch_grad.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, i, i, i, d, i, i, i,
+                                             ctypes.POINTER(ctypes.c_float)]
+        L.ref_gpu_wdl_batch_grad.restype = i
         _ref_gpu = L
     return _ref_gpu
+
+
+def ref_gpu_wdl_batch_grad(A, WB, YB, K_or_C, reg, L, mode=0, reps=1):
+    """rwig's own unrolled GPU WDL batch gradient (wdl_batch, src/cuda_wdl.cu:385)
+    on D = WB.shape[1] documents, host buffers.  Returns (g_Alpha, g_lambda,
+    mean device ms of one wdl_batch call over `reps` calls)."""
+    A, WB, YB, K_or_C = _f64(A), _f64(WB), _f64(YB), _f64(K_or_C)
+    N, S = A.shape
+    D = WB.shape[1]
+    gA, gl = np.zeros((N, S), order="F"), np.zeros(S)
+    ms = ctypes.c_float()
+    rc = ref_gpu().ref_gpu_wdl_batch_grad(_ptr(gA), _ptr(gl), _ptr(A), _ptr(WB), _ptr(YB), _ptr(K_or_C), N, S, D,
+                                          float(reg), int(L), int(mode), int(reps), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference wdl_batch failed with CUDA error {rc}")
+    return gA, gl, ms.value
+
+
+def ref_gpu_wdl(Y, C, S, reg, max_iter, zero_tol, B, E, opt=1, eta=1e-3, gamma=0.01, beta1=0.9, beta2=0.999,
+                eps=1e-8, seed=1):
+    """rwig's own GPU WDL (cuda_wdl, src/cuda_wdl.cu:539): training from
+    mt19937(seed) logits, then inference.  Returns A, W, Yhat."""
+    Y, C = _f64(Y), _f64(C)
+    N, M = Y.shape
+    A, W, Yhat = np.zeros((N, S), order="F"), np.zeros((S, M), order="F"), np.zeros((N, M), order="F")
+    ref_gpu().ref_gpu_wdl(_ptr(A), _ptr(W), _ptr(Yhat), _ptr(Y), _ptr(C), N, M, S, float(reg), int(max_iter),
+                          float(zero_tol), int(B), int(E), int(opt), float(eta), float(gamma), float(beta1),
+                          float(beta2), float(eps), int(seed))
+    return dict(A=A, W=W, Yhat=Yhat)
 
 
 def ref_gpu_sinkhorn_vanilla(a, b, C, reg, max_iter=1000, zero_tol=1e-6):

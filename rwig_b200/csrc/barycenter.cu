@@ -484,13 +484,14 @@ struct Solve {
 
   // normalised barycenter and loss (log: before the backward, :268-271;
   // parallel: the backward uses the un-normalised b, :35-42)
-  if (iter > 0) {
-    normalise_b<<<1, 1024, 0, q>>>(slot(Bh, N, iter), N, logdomain, withgrad ? bext : nullptr, bn, scal);
-  } else {
-    // no iteration: parallel b = 0 / sum(0) (barycenter_impl_parallel.cpp:64, :39);
-    // log b = exp(0) / N (barycenter_impl_log.cpp:193, :268-269)
-    fill_kernel<<<grid_for(ctx, N), TPB, 0, q>>>(bn, N, logdomain ? 1.0 / N : NAN);
+  if (iter == 0) {
+    // no iteration: the initial b is 0 (parallel, barycenter_impl_parallel.cpp:64)
+    // or log b = 0 (log, barycenter_impl_log.cpp:193), normalised as below to
+    // 0 / 0 = NaN or 1/N, and the loss taken against b_ext all the same
+    fill_kernel<<<grid_for(ctx, N), TPB, 0, q>>>(slot(Bh, N, 0), N, 0.0);
+    ++launches;
   }
+  normalise_b<<<1, 1024, 0, q>>>(slot(Bh, N, iter), N, logdomain, withgrad ? bext : nullptr, bn, scal);
   ++launches;
 
   if (withgrad && iter > 0) {
@@ -674,7 +675,7 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   }
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   double sc[2] = {0.0, 0.0};
-  if (iter > 0) RWIG_CUDA_TRY(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
   std::vector<double> G;
   if (fixed && iter > 0) {
     G.resize((size_t)S * S);
@@ -702,19 +703,21 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   return status;
 }
 
-// Side streams of the batched entry (created on first use, kept).
-constexpr int kSideStreams = 8;
-cudaStream_t side_stream(int i) {
-  static cudaStream_t pool[kSideStreams] = {};
-  if (!pool[i] && cudaStreamCreateWithFlags(&pool[i], cudaStreamNonBlocking) != cudaSuccess) {
+// Side stream i of the batched entry on this context's device, created on
+// first use (the caller holds ctx->mu and has ctx->device current).
+constexpr int kSideStreams = Context::kSideStreams;
+cudaStream_t side_stream(Context* ctx, int i) {
+  cudaStream_t& q = ctx->side[i];
+  if (!q && cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess) {
     (void)cudaGetLastError();
-    pool[i] = nullptr;
+    q = nullptr;
   }
-  return pool[i];
+  return q;
 }
 
-// First scratch slot of the i-th solve of a batch (clear of every other
-// entry's slot numbers).
+// First scratch slot of the solves enqueued on side stream i (clear of every
+// other entry's slot numbers).  Solves on one stream run in stream order, so
+// they share one slot set, grown to the largest of them.
 constexpr int kBatchSlotBase = 1000, kBatchSlotStride = 32;
 
 // Many barycenter problems: those with a fixed iteration count enqueued
@@ -758,12 +761,18 @@ int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int
     s.withgrad = q.withgrad;
     s.L = q.max_iter;
     s.tol = q.zero_tol;
-    const int rc2 = s.alloc(kBatchSlotBase + kBatchSlotStride * (int)fixed_ids.size());
+    const int rc2 = s.alloc(kBatchSlotBase + kBatchSlotStride * (int)(fixed_ids.size() % kSideStreams));
     if (rc2) {
       out[i].status = rc2;
       continue;
     }
     fixed_ids.push_back(i);
+  }
+  // a later, larger solve on the same stream may have regrown a slot: take
+  // every solve's pointers again now that the slots have their final sizes
+  for (size_t k = 0; k < fixed_ids.size(); ++k) {
+    Solve& s = sv[fixed_ids[k]];
+    if (const int rc = s.alloc(kBatchSlotBase + kBatchSlotStride * (int)(k % kSideStreams))) return rc;
   }
   int launches = 0;
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
@@ -785,29 +794,38 @@ int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int
     double* hp = (double*)ctx->pinned;
     RWIG_CUDA_TRY(cudaEventRecord(ctx->evk, st));  // inputs ready on the caller's stream
     bool used[kSideStreams] = {};
+    // on an error part-way, wait for what was enqueued (it writes the
+    // caller's outputs and the pinned buffer) and mark the rest as failed
+    auto fail_from = [&](size_t k0, int rc) -> int {
+      for (int si = 0; si < kSideStreams; ++si)
+        if (used[si]) cudaStreamSynchronize(ctx->side[si]);
+      for (size_t k = k0; k < fixed_ids.size(); ++k) out[fixed_ids[k]].status = rc;
+      return rc;
+    };
     for (size_t k = 0; k < fixed_ids.size(); ++k) {
       Solve& s = sv[fixed_ids[k]];
       const int si = (int)(k % kSideStreams);
-      cudaStream_t q = side_stream(si);
-      if (!q) return set_error(RWIG_E_CUDA, "could not create a side stream");
-      if (!used[si]) RWIG_CUDA_TRY(cudaStreamWaitEvent(q, ctx->evk, 0));
+      cudaStream_t q = side_stream(ctx, si);
+      if (!q) return fail_from(k, set_error(RWIG_E_CUDA, "could not create a side stream"));
+      if (!used[si] && cudaStreamWaitEvent(q, ctx->evk, 0) != cudaSuccess)
+        return fail_from(k, set_error(RWIG_E_CUDA, "cudaStreamWaitEvent on a side stream failed"));
       used[si] = true;
-      if (int rc = s.enqueue(q)) return rc;
+      if (int rc = s.enqueue(q)) return fail_from(k, rc);
       launches += s.launches;
-      if (s.iter > 0) {
-        RWIG_CUDA_TRY(cudaMemcpyAsync(hp + at[k], s.gram, sizeof(double) * s.S * s.S, cudaMemcpyDeviceToHost, q));
-        RWIG_CUDA_TRY(cudaMemcpyAsync(hp + at[k] + (size_t)s.S * s.S, s.scal, sizeof(double) * 2,
-                                      cudaMemcpyDeviceToHost, q));
-      }
+      if (cudaMemcpyAsync(hp + at[k], s.gram, sizeof(double) * s.S * s.S, cudaMemcpyDeviceToHost, q) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(hp + at[k] + (size_t)s.S * s.S, s.scal, sizeof(double) * 2, cudaMemcpyDeviceToHost,
+                          q) != cudaSuccess)
+        return fail_from(k, set_error(RWIG_E_CUDA, "result copy of a batched barycenter failed"));
     }
     for (int si = 0; si < kSideStreams; ++si)
-      if (used[si]) RWIG_CUDA_TRY(cudaStreamSynchronize(side_stream(si)));
+      if (used[si]) RWIG_CUDA_TRY(cudaStreamSynchronize(ctx->side[si]));
     RWIG_CUDA_TRY(cudaGetLastError());
     for (size_t k = 0; k < fixed_ids.size(); ++k) {
       Solve& s = sv[fixed_ids[k]];
       rwig_bary_result& r = out[fixed_ids[k]];
       if (s.iter > 0) s.err_from_gram(hp + at[k]);
-      r.loss = (s.withgrad && s.iter > 0) ? hp[at[k] + (size_t)s.S * s.S + 1] : 0.0;
+      r.loss = s.withgrad ? hp[at[k] + (size_t)s.S * s.S + 1] : 0.0;
       r.err = s.err;
       r.iter = s.iter;
       r.status = (s.err <= s.tol) ? 0 : (s.iter == s.L ? 1 : 2);

@@ -148,6 +148,11 @@ extern "C" void rwig_shutdown(void) {
     cudaEventDestroy(c->evk);
     cudaEventDestroy(c->evs0);
     cudaEventDestroy(c->evs1);
+    for (cudaStream_t& q : c->side)
+      if (q) {
+        cudaStreamSynchronize(q);
+        cudaStreamDestroy(q);
+      }
     cudaStreamDestroy(c->stream);
     c.reset();
   }

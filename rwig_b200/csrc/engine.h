@@ -35,6 +35,10 @@ struct Context {
   size_t pinned_bytes = 0;
   GraphEntry graphs[kGraphSites];
   std::vector<unsigned long long> seen[kGraphSites];  // key of the previous call per site
+  // side streams of the batched barycenter entry, created on this device on
+  // first use (under mu) and destroyed by rwig_shutdown
+  static constexpr int kSideStreams = 8;
+  cudaStream_t side[kSideStreams] = {};
 };
 
 // Returns the context of the current (or first) device, initialising it on

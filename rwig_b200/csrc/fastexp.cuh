@@ -83,10 +83,14 @@ __device__ __forceinline__ double exp_tbl(double x, const double* tbl) {
 }  // namespace rwig
 
 namespace rwig {
-// 1/x to within 2 ulp for normal positive x: single-precision seed refined by
-// two Newton-Raphson steps y <- y + y (1 - x y) in FP64 (each step squares the
-// relative error: 2^-22 -> 2^-44 -> below 2^-53).
+// 1/x to within 2 ulp: for |x| in [2^-120, 2^120] a single-precision seed
+// refined by two Newton-Raphson steps y <- y + y (1 - x y) in FP64 (each step
+// squares the relative error: 2^-22 -> 2^-44 -> below 2^-53).  Outside that
+// range (where the float seed would be 0, inf or subnormal), and for 0, inf
+// and NaN, the IEEE division 1.0 / x.
 __device__ __forceinline__ double rcp_nr(double x) {
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-120 && ax <= 0x1p120)) return 1.0 / x;
   double y = (double)(1.0f / (float)x);
   double e = fma(-x, y, 1.0);
   y = fma(y, e, y);

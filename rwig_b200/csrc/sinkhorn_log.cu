@@ -1321,6 +1321,7 @@ extern "C" int rwig_sinkhorn_log_noalloc(double* P, double* f, double* g, double
   if (!a || !b || !C) return set_error(RWIG_E_INVALID, "a, b and C must be non-null");
   if (M < 1 || N < 1) return set_error(RWIG_E_INVALID, "M and N must be >= 1");
   if (!(reg > 0.0) || !std::isfinite(reg)) return set_error(RWIG_E_INVALID, "reg must be finite and > 0");
+  if (max_iter < 0) return set_error(RWIG_E_INVALID, "max_iter must be >= 0");
   if (M > kMaxM || N > kMaxN)
     return set_error(RWIG_E_UNSUPPORTED,
                      "problem exceeds the no-allocation limit of M <= 4096 and N <= 4096; "

@@ -151,7 +151,9 @@ __global__ void __launch_bounds__(NTT, 1) scaled_kernel(ScaledParams p) {
         if (c == lane) mine_s = sum[c];
       const bool owner = lane < nc;
       const int jl = jb - ring.c0 + lane;
-      const double v_l = owner ? (init ? 1.0 : cb[jl] * rcp_nr(mine_s)) : 0.0;
+      // vanilla: v = b / (K^T u) by IEEE division, as the reference
+      // (sinkhorn_impl_vanilla.cpp:133), also where K^T u is subnormal or 0
+      const double v_l = owner ? (init ? 1.0 : (VAN ? cb[jl] / mine_s : cb[jl] * rcp_nr(mine_s))) : 0.0;
       double v[CW];
 #pragma unroll
       for (int c = 0; c < CW; ++c) v[c] = __shfl_sync(0xffffffffu, v_l, c);

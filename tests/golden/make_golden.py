@@ -90,7 +90,9 @@ def extract(ref_root: str) -> dict:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RWIG_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_golden.py <rwig source tree>  (or set RWIG_REFERENCE_DIR)")
     data = extract(ref)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tinytest_golden.json")
     with open(dst, "w") as fh:

@@ -129,3 +129,23 @@ def test_graph_replay_is_bitwise_identical(method):
     ref = rw.barycenter(A2, C, w, be, dict(ctrl, max_iter=13))  # a different sequence, eager
     assert got["iter"] == 12 and ref["iter"] == 13
     _compare(method, A2, C, w, be, 0.1, max_iter=12, zero_tol=0.0)
+
+
+@pytest.mark.parametrize("method", ["parallel", "log"])
+def test_zero_iterations(method):
+    """max_iter = 0 with gradient: b is the initial b normalised (0/0 = NaN for
+    parallel, 1/N for log) and the loss is taken against b_ext all the same
+    (barycenter_impl_parallel.cpp:39-42, barycenter_impl_log.cpp:268-271);
+    nothing is unrolled, so the gradients are zero."""
+    A, C, w, be = synth.barycenter_config(n=50, S=3, dim=3, salt=4)
+    f = oracle.barycenter_log if method == "log" else oracle.barycenter_parallel
+    ref = f(A, C, w, be, 0.1, with_grad=True, max_iter=0, zero_tol=1e-6)
+    got = rw.barycenter(A, C, w, be, {"reg": 0.1, "method": method, "with_grad": True, "max_iter": 0,
+                                      "zero_tol": 1e-6})
+    assert got["iter"] == ref["iter"] == 0 and got["return_status"] == ref["return_status"]
+    assert rel_err(got["b"], ref["b"]) <= PARITY_TOL
+    if method == "parallel":
+        assert np.isnan(ref["loss"]) and np.isnan(got["loss"])
+    else:
+        assert abs(got["loss"] - ref["loss"]) <= PARITY_TOL * abs(ref["loss"])
+    assert not got["grad_A"].any() and not got["grad_w"].any()

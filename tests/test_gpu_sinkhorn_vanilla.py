@@ -79,3 +79,30 @@ def test_device_entry_matches_host_entry():
     assert r["iter"] == host["iter"]
     assert np.array_equal(P.cpu().numpy().T, host["P"])
     assert np.array_equal(u.cpu().numpy(), host["u"]) and np.array_equal(v.cpu().numpy(), host["v"])
+
+
+def _outlier_problem(m, n, seed, far):
+    """Sources and targets in [0, 0.1]^2 except `far` targets near (1, 1):
+    with the cost normalised by its maximum, K^T u at those targets is about
+    exp(-1/eps) times the other column sums."""
+    g = np.random.default_rng(seed)
+    x = g.random((m, 2)) * 0.1
+    y = g.random((n, 2)) * 0.1
+    y[:far] = 1.0 - 0.01 * g.random((far, 2))
+    C = synth.sq_euclid_cost(x, y)
+    a = g.gamma(1.0, size=m)
+    b = g.gamma(1.0, size=n)
+    return a / a.sum(), b / b.sum(), C
+
+
+@pytest.mark.parametrize("m,n,reg,seed,far", [(256, 256, 0.01, 1, 1), (300, 200, 0.01, 4, 4),
+                                              (256, 256, 0.012, 3, 2)])
+def test_column_sums_below_float_range(m, n, reg, seed, far):
+    """Column sums K^T u far below FLT_MIN (1e-40 at eps = 0.01): v = b / K^T u
+    must be the IEEE quotient, as sinkhorn_impl_vanilla.cpp:133 computes it."""
+    a, b, C = _outlier_problem(m, n, seed, far)
+    got, ref = _compare(a, b, C, reg, max_iter=2000)
+    ktu = b / ref["v"]
+    if reg == 0.01:
+        assert ktu.min() < 1e-38
+    assert np.isfinite(got["P"]).all() and np.isfinite(got["v"]).all()

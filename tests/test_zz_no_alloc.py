@@ -81,3 +81,10 @@ def test_rejects_sizes_beyond_the_limit():
     with pytest.raises(_lib.RwigError) as ei:
         _call("noalloc", prob)
     assert ei.value.code == -6 and "4096" in str(ei.value)
+
+
+def test_rejects_negative_max_iter():
+    prob = _dev_buffers(64, 64, salt=24, reg=0.05)
+    with pytest.raises(_lib.RwigError) as ei:
+        _call("noalloc", prob, max_iter=-1)
+    assert ei.value.code == -1 and "max_iter" in str(ei.value)
