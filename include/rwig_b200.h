@@ -50,7 +50,8 @@ typedef struct rwig_report {
   double kernel_ms;      /* device time of the solver kernels (first launch to last) */
   double sweep_ms;       /* device time of the launches that ran scaled-form iterations */
   int sweep_iters;       /* iterations run by those launches */
-  int fallback_events;   /* sweeps re-run with exact per-row / per-column minima */
+  int fallback_events;   /* sweeps re-run with exact per-row / per-column minima
+                            (log barycenter: 1 when the log-domain kernels ran) */
   int kernel_launches;   /* engine kernels launched by the call */
   int support_m;         /* rows kept after dropping zero-mass entries of a */
   int support_n;         /* columns kept after dropping zero-mass entries of b */
@@ -95,7 +96,12 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *   "wdl.infer_docs": documents per stacked-column chunk of WDL inference
  *       (default 1024);
  *   "dgemm.kshape", "dgemm.tile": DMMA instruction shape (k = 4, 8 or 16)
- *       and tile height (0 automatic, 64, 128) of rwig_selftest_dgemm only.
+ *       and tile height (0 automatic, 64, 128) of rwig_selftest_dgemm only;
+ *   "barycenter.log_path": the log barycenter's route: 0 (default) the
+ *       scaling form on K = exp(-C/reg) with a range check, re-run by the
+ *       log-domain kernels when K has subnormal entries or the sums leave
+ *       [1e-290, 1e290]; 1 the log-domain kernels always; -1 the scaling
+ *       form only.
  * The batch.* options change team shapes and therefore the summation order
  * of a batched result (within rounding); a result is the same alone and in
  * any mix under the same options.  A NaN value clears the option (its

@@ -22,6 +22,16 @@
 // with the seeds of step L as in the reference.  The history U_l, V_l, Z_l,
 // Y_l, b_l of every iteration is kept on the device (the backward reads it
 // once, newest first); all reductions run in a fixed order.
+//
+// The scaling form equals the log-domain updates only while every K_ij is a
+// normal double and the products stay well inside the double range.  For the
+// log method the Gibbs kernel and the epilogues check this as they go (K_ij
+// normal and finite; every entry of Y = K V and Z = K^T U in [1e-290,
+// 1e290]; the adjoint operands finite) and raise a flag word; a flagged solve
+// is re-run by the log-domain kernels of barycenter_log.cu, which follow the
+// reference's soft-min sweeps over C - F and C - G directly.  With Y, Z >=
+// 1e-290 and normal K the products lost to underflow change each sum by
+// less than N 2^-1074 / 1e-290, far below rounding.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -38,12 +48,24 @@ namespace bary {
 
 constexpr int TPB = 256;
 
-__global__ void gibbs_kernel(const double* C, int M, int N, long long ldk, double reg, double* K) {
+// Range checks of the scaling form (log method): a value outside the range
+// sets *flag (the solve is then re-run in the log domain).
+constexpr double kRangeLo = 1e-290, kRangeHi = 1e290;
+__device__ __forceinline__ void check_range(double* flag, double x) {
+  if (flag && !(x >= kRangeLo && x <= kRangeHi)) *flag = 1.0;
+}
+__device__ __forceinline__ void check_finite(double* flag, double x) {
+  if (flag && !(fabs(x) <= 1.79e308)) *flag = 1.0;
+}
+
+__global__ void gibbs_kernel(const double* C, int M, int N, long long ldk, double reg, double* K, double* flag) {
   const long long total = ldk * (long long)N;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
        k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k % ldk), j = (int)(k / ldk);
-    K[k] = (i < M) ? exp(-C[i + (long long)j * M] / reg) : 0.0;  // exp(-C / reg)
+    const double v = (i < M) ? exp(-C[i + (long long)j * M] / reg) : 0.0;  // exp(-C / reg)
+    K[k] = v;
+    if (flag && i < M && !(v >= 2.2250738585072014e-308 && v <= 1.79e308)) *flag = 1.0;  // subnormal, 0, inf
   }
 }
 
@@ -66,12 +88,14 @@ struct EpiZ {
   double* V;
   double* bl;
   int N, S, logdomain;
+  double* flag;
   __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double* ws) const {
     if (nr <= 0) return;
     const int n = nr * S;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
       const int r = e % nr, s = e / nr;
       const double z = t[s * ldt + r];
+      check_range(flag, z);
       ws[s * ldt + r] = logdomain ? w[s] * log(z) : pow(z, w[s]);
     }
     __syncthreads();
@@ -102,12 +126,14 @@ struct EpiY {
   double* Unext;
   double* D;
   int M, S, ldd, logdomain;
+  double* flag;
   __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double*) const {
     if (nr <= 0) return;
     for (int e = threadIdx.x; e < nr * S; e += blockDim.x) {
       const int r = e % nr, s = e / nr, i = r0 + r;
       const size_t k = (size_t)i + (size_t)s * M;
       const double y = t[s * ldt + r];
+      check_range(flag, y);
       Y[k] = y;
       if (Unext) Unext[k] = A[k] / y;
       if (D) D[i + (size_t)s * ldd] = logdomain ? log(Ucur[k] * y) - logA[k] : Ucur[k] * y - A[k];
@@ -131,6 +157,7 @@ struct EpiB1 {
   int N, S, logdomain, seed;
   double* T2;
   double* gw_part;
+  double* flag;
   __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double* ws) const {
     if (nr <= 0) return;
     const int n = nr * S;
@@ -171,6 +198,7 @@ struct EpiB1 {
         double y = (w[s] / eps) * c;
         if (!seed) y -= -V[k] * t[s * ldt + r];
         T2[k] = y / Z[k];
+        check_finite(flag, T2[k]);
         ws[s * ldt + r] = lz * c;
       }
     }
@@ -193,6 +221,7 @@ struct EpiB2 {
   int M, S, logdomain;
   double* gradA;
   double* Tnext;
+  double* flag;
   __device__ void operator()(int r0, int nr, int, int, double* t, int ldt, double*) const {
     if (nr <= 0) return;
     for (int e = threadIdx.x; e < nr * S; e += blockDim.x) {
@@ -206,6 +235,8 @@ struct EpiB2 {
         const double fbar = Ul[k] * y;  // U_l o K(...)
         gradA[k] += fbar / A[k];
         Tnext[k] = fbar / Yprev[k];  // Fbar / (K V_{l-1})
+        check_finite(flag, Tnext[k]);
+        check_finite(flag, gradA[k]);
       }
     }
   }
@@ -385,6 +416,7 @@ struct Solve {
   double *T = nullptr, *T2 = nullptr, *gA = nullptr, *gwp = nullptr, *gw = nullptr;
   int launches = 0, iter = 0;
   double err = 1000.0;
+  bool needs_log = false;  // the range flag was seen set during the solve (tol > 0)
 
   double* slot(double* base, size_t sz, int l) const { return base + sz * (size_t)(withgrad ? l : (l & 1)); }
 
@@ -438,11 +470,16 @@ struct Solve {
 
   // The whole solve on stream q (with tol > 0 the stopping test reads err
   // on the host after every iteration).
+  // Log method: the range flag of the scaling form (scal[2]), else null.
+  double* flag() const { return logdomain ? scal + 2 : nullptr; }
+
   int enqueue(cudaStream_t q) {
   launches = 0;
   iter = 0;
   err = 1000.0;
-  gibbs_kernel<<<grid_for(ctx, ldk * N), TPB, 0, q>>>(C, M, N, ldk, reg, K);  // K = exp(-C/reg)
+  needs_log = false;
+  RWIG_CUDA_TRY(cudaMemsetAsync(scal + 2, 0, sizeof(double), q));
+  gibbs_kernel<<<grid_for(ctx, ldk * N), TPB, 0, q>>>(C, M, N, ldk, reg, K, flag());  // K = exp(-C/reg)
   log_kernel<<<grid_for(ctx, MS), TPB, 0, q>>>(A, MS, logA);
   fill_kernel<<<grid_for(ctx, NS), TPB, 0, q>>>(slot(Vh, NS, 0), NS, 1.0);  // V_0 = 1
   launches += 3;
@@ -455,27 +492,32 @@ struct Solve {
   };
   // Y_0 = K V_0, U_1 = A / Y_0
   int rc = gemm_y(slot(Vh, NS, 0), EpiY{A, logA, nullptr, slot(Yh, MS, 0), slot(Uh, MS, 1), nullptr, M, S,
-                                        (int)ldd, logdomain ? 1 : 0});
+                                        (int)ldd, logdomain ? 1 : 0, flag()});
   if (rc) return rc;
   while (iter < L && err >= tol) {
     ++iter;
     const int l = iter;
     double* Ul = slot(Uh, MS, l);
     // Z_l = K^T U_l; b_l; V_l = b_l / Z_l
-    rc = gemm_z(Ul, EpiZ{w, slot(Zh, NS, l), slot(Vh, NS, l), slot(Bh, N, l), N, S, logdomain ? 1 : 0});
+    rc = gemm_z(Ul, EpiZ{w, slot(Zh, NS, l), slot(Vh, NS, l), slot(Bh, N, l), N, S, logdomain ? 1 : 0, flag()});
     if (rc) return rc;
     // Y_l = K V_l; U_{l+1} = A / Y_l; residual when the stopping test needs it
     const bool need_err = !fixed || (iter == L);
     rc = gemm_y(slot(Vh, NS, l), EpiY{A, logA, Ul, slot(Yh, MS, l), slot(Uh, MS, l + 1),
-                                      need_err ? D : nullptr, M, S, (int)ldd, logdomain ? 1 : 0});
+                                      need_err ? D : nullptr, M, S, (int)ldd, logdomain ? 1 : 0, flag()});
     if (rc) return rc;
     if (need_err) {
       rc = dg::gemm<1>(ctx, dg::GemmArgs{D, ldd, S, M, S, D, ldd, 0}, dg::EpiStore{gram, S, S}, q, 0, &launches);
       if (rc) return rc;
       if (!fixed) {  // the stopping test needs err now
-        std::vector<double> G((size_t)S * S);
+        std::vector<double> G((size_t)S * S + 1);
         RWIG_CUDA_TRY(cudaMemcpyAsync(G.data(), gram, sizeof(double) * S * S, cudaMemcpyDeviceToHost, q));
+        RWIG_CUDA_TRY(cudaMemcpyAsync(G.data() + (size_t)S * S, scal + 2, sizeof(double), cudaMemcpyDeviceToHost, q));
         RWIG_CUDA_TRY(cudaStreamSynchronize(q));
+        if (G[(size_t)S * S] != 0.0) {  // out of the scaling form's range: stop, re-run in the log domain
+          needs_log = true;
+          return 0;
+        }
         err_from_gram(G.data());
       }
     }
@@ -500,7 +542,7 @@ struct Solve {
     for (int l = iter; l >= 1; --l) {
       const bool seed = (l == iter);
       const EpiB1 e1{slot(Zh, NS, l), slot(Vh, NS, l), w, slot(Bh, N, l), bn, bext, reg, N, S,
-                     logdomain ? 1 : 0, seed ? 1 : 0, T2, gwp};
+                     logdomain ? 1 : 0, seed ? 1 : 0, T2, gwp, flag()};
       if (seed) {
         seed_b1<<<ngrp, dg::NTH, sizeof(double) * (S + 1) * 8, q>>>(e1, N);
         ++launches;
@@ -508,7 +550,7 @@ struct Solve {
         rc = gemm_z(T, e1);  // K^T T
         if (rc) return rc;
       }
-      rc = gemm_y(T2, EpiB2{slot(Uh, MS, l), slot(Yh, MS, l - 1), A, M, S, logdomain ? 1 : 0, gA, T});  // K T2
+      rc = gemm_y(T2, EpiB2{slot(Uh, MS, l), slot(Yh, MS, l - 1), A, M, S, logdomain ? 1 : 0, gA, T, flag()});  // K T2
       if (rc) return rc;
     }
     reduce_gw<<<S, 256, 0, q>>>(gwp, ngrp, S, gw);
@@ -566,12 +608,52 @@ int check_args(const double* A, const double* w, const double* C, const double* 
 
 // Core driver; all pointers on the device.  Outputs (any may be null):
 // U, V (parallel) or F, G (log) as X1, X2; b (normalised); grad_A, grad_w.
+// Option "barycenter.log_path" for the log method: 0 (default) the scaling
+// form with its range check, re-run in the log domain when it fails; 1 the
+// log-domain kernels always; -1 the scaling form only.
+int log_path_option() { return (int)option("barycenter.log_path", 0.0); }
+
+// run_log with the call's report filled (device time from ev0 on `st`).
+int run_log_reported(Context* ctx, cudaStream_t st, double* X1, double* X2, double* b, double* gradA,
+                     double* gradw, double* loss, int* iter_out, double* err_out, const double* A, const double* w,
+                     const double* C, const double* bext, int M, int N, int S, double reg, int withgrad,
+                     int max_iter, double tol, int prior_launches) {
+  int nl = 0, it = 0;
+  double er = 0.0;
+  const int status = run_log(ctx, st, X1, X2, b, gradA, gradw, loss, &it, &er, A, w, C, bext, M, N, S, reg,
+                             withgrad, max_iter, tol, &nl);
+  if (status < 0) return status;
+  RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
+  RWIG_CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (iter_out) *iter_out = it;
+  if (err_out) *err_out = er;
+  rwig_report& R = report();
+  R.iter = it;
+  R.status = status;
+  R.err = er;
+  R.device_ms = ms;
+  R.kernel_ms = ms;
+  R.kernel_launches = prior_launches + nl;
+  R.fallback_events = 1;
+  R.support_m = M;
+  R.support_n = N;
+  return status;
+}
+
 int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, double* b, double* gradA,
         double* gradw, double* loss, int* iter_out, double* err_out, const double* A, const double* w,
         const double* C, const double* bext, int M, int N, int S, double reg, int withgrad, int max_iter,
         double tol) {
   reset_report();
   if (int rc = check_args(A, w, C, bext, M, N, S, reg, withgrad)) return rc;
+  const int lp = logdomain ? log_path_option() : 0;
+  if (lp == 1) {
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
+    return run_log_reported(ctx, st, X1, X2, b, gradA, gradw, loss, iter_out, err_out, A, w, C, bext, M, N, S,
+                            reg, withgrad, max_iter, tol, 0);
+  }
   Solve sv;
   sv.ctx = ctx;
   sv.logdomain = logdomain;
@@ -674,7 +756,7 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
     if (fixed) ctx->seen[site] = key;
   }
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
-  double sc[2] = {0.0, 0.0};
+  double sc[3] = {0.0, 0.0, 0.0};
   RWIG_CUDA_TRY(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
   std::vector<double> G;
   if (fixed && iter > 0) {
@@ -683,6 +765,9 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   }
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   RWIG_CUDA_TRY(cudaGetLastError());
+  if (logdomain && lp == 0 && (sv.needs_log || sc[2] != 0.0))
+    return run_log_reported(ctx, st, X1, X2, b, gradA, gradw, loss, iter_out, err_out, A, w, C, bext, M, N, S,
+                            reg, withgrad, max_iter, tol, launches);
   if (fixed && iter > 0) sv.err_from_gram(G.data());
   if (loss) *loss = withgrad ? sc[1] : 0.0;
   if (iter_out) *iter_out = iter;
@@ -738,7 +823,7 @@ int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int
       out[i].status = rc;
       continue;
     }
-    if (q.zero_tol > 0.0) {
+    if (q.zero_tol > 0.0 || (q.method == 1 && log_path_option() == 1)) {
       serial_ids.push_back(i);
       continue;
     }
@@ -782,7 +867,7 @@ int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int
     std::vector<size_t> at(fixed_ids.size());
     for (size_t k = 0; k < fixed_ids.size(); ++k) {
       at[k] = need;
-      need += (size_t)sv[fixed_ids[k]].S * sv[fixed_ids[k]].S + 2;
+      need += (size_t)sv[fixed_ids[k]].S * sv[fixed_ids[k]].S + 3;
     }
     if (ctx->pinned_bytes < need * sizeof(double)) {
       if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -814,16 +899,31 @@ int run_batch(Context* ctx, cudaStream_t st, const rwig_bary_problem* probs, int
       launches += s.launches;
       if (cudaMemcpyAsync(hp + at[k], s.gram, sizeof(double) * s.S * s.S, cudaMemcpyDeviceToHost, q) !=
               cudaSuccess ||
-          cudaMemcpyAsync(hp + at[k] + (size_t)s.S * s.S, s.scal, sizeof(double) * 2, cudaMemcpyDeviceToHost,
+          cudaMemcpyAsync(hp + at[k] + (size_t)s.S * s.S, s.scal, sizeof(double) * 3, cudaMemcpyDeviceToHost,
                           q) != cudaSuccess)
         return fail_from(k, set_error(RWIG_E_CUDA, "result copy of a batched barycenter failed"));
     }
     for (int si = 0; si < kSideStreams; ++si)
       if (used[si]) RWIG_CUDA_TRY(cudaStreamSynchronize(ctx->side[si]));
     RWIG_CUDA_TRY(cudaGetLastError());
+    // log problems whose scaling form left its range: re-run in the log domain
+    const int lp = log_path_option();
+    for (size_t k = 0; k < fixed_ids.size(); ++k) {
+      Solve& s = sv[fixed_ids[k]];
+      if (!(s.logdomain && lp == 0 && hp[at[k] + (size_t)s.S * s.S + 2] != 0.0)) continue;
+      const rwig_bary_problem& q = probs[fixed_ids[k]];
+      rwig_bary_result& r = out[fixed_ids[k]];
+      int nl = 0;
+      const int rc = run_log(ctx, st, q.X1, q.X2, q.b, q.grad_A, q.grad_w, &r.loss, &r.iter, &r.err, q.A, q.w, q.C,
+                             q.b_ext, q.M, q.N, q.S, q.reg, q.withgrad, q.max_iter, q.zero_tol, &nl);
+      launches += nl;
+      r.status = rc;
+      s.iter = -1;  // done
+    }
     for (size_t k = 0; k < fixed_ids.size(); ++k) {
       Solve& s = sv[fixed_ids[k]];
       rwig_bary_result& r = out[fixed_ids[k]];
+      if (s.iter < 0) continue;
       if (s.iter > 0) s.err_from_gram(hp + at[k]);
       r.loss = s.withgrad ? hp[at[k] + (size_t)s.S * s.S + 1] : 0.0;
       r.err = s.err;

@@ -149,3 +149,111 @@ def test_zero_iterations(method):
     else:
         assert abs(got["loss"] - ref["loss"]) <= PARITY_TOL * abs(ref["loss"])
     assert not got["grad_A"].any() and not got["grad_w"].any()
+
+
+class _LogPath:
+    """Sets the engine option barycenter.log_path for a block (NaN restores the default)."""
+
+    def __init__(self, value):
+        self.value = value
+
+    def __enter__(self):
+        rw.load().rwig_set_option(b"barycenter.log_path", float(self.value))
+
+    def __exit__(self, *exc):
+        rw.load().rwig_set_option(b"barycenter.log_path", float("nan"))
+
+
+@pytest.mark.parametrize("n,S,dim,reg,L,tol,scale", [
+    (200, 5, 3, 1e-3, 20, 0.0, 1.0),     # max C / eps = 1000 on a max-normalised cost
+    (256, 8, 10, 1e-3, 15, 0.0, 1.0),
+    (180, 6, 3, 0.05, 20, 0.0, 100.0),   # un-normalised cost, max C = 100: max C / eps = 2000
+    (300, 4, 2, 0.05, 25, 0.0, 100.0),
+    (150, 3, 2, 1e-3, 200, 1.0, 1.0),    # with a stopping test (stops at iteration 78)
+])
+def test_log_barycenter_where_the_gibbs_kernel_underflows(n, S, dim, reg, L, tol, scale):
+    """exp(-C/eps) has entries that underflow to zero: the scaling form's range
+    check fails and the solve runs in the log domain, as the reference's
+    compute_log does (barycenter_impl_log.cpp:189-382), with its gradients."""
+    A, C, w, be = synth.barycenter_config(n=n, S=S, dim=dim, salt=n + S)
+    C = C * scale
+    assert (np.exp(-C / reg) == 0).any()
+    got, ref = _compare("log", A, C, w, be, reg, max_iter=L, zero_tol=tol)
+    assert rw.last_report()["fallback_events"] == 1
+    assert np.isfinite(got["grad_A"]).all() and np.isfinite(got["F"]).all()
+
+
+def test_log_barycenter_scaling_form_kept_in_range():
+    """Within range (max C / eps = 20) the scaling form's result stands."""
+    A, C, w, be = synth.barycenter_config(n=256, S=8, dim=10, salt=5)
+    _compare("log", A, C, w, be, 0.05, max_iter=30, zero_tol=0.0)
+    assert rw.last_report()["fallback_events"] == 0
+
+
+@pytest.mark.parametrize("n,m,S,reg,L,tol", [
+    (64, 64, 4, 0.1, 1000, 1e-9), (200, 150, 7, 0.1, 30, 0.0), (256, 256, 32, 0.05, 50, 0.0),
+    (513, 300, 3, 0.2, 40, 0.0), (2, 2, 2, 0.1, 5, 0.0), (90, 700, 17, 0.02, 12, 0.0), (1000, 64, 64, 0.1, 6, 0.0),
+])
+def test_log_domain_kernels_against_oracle(n, m, S, reg, L, tol):
+    """The log-domain kernels forced on (barycenter.log_path = 1) at ordinary
+    regularisation, rectangular costs and S up to 64."""
+    g = synth.rng(41, n + m + S)
+    x, y = g.random((n, 3)), g.random((m, 3))
+    C = synth.sq_euclid_cost(x, y)
+    A = synth.dirichlet(g, 0.5, n, S)
+    w = synth.dirichlet(g, 1.0, S)
+    be = synth.dirichlet(g, 1.0, m)
+    with _LogPath(1):
+        got, ref = _compare("log", A, C, w, be, reg, max_iter=L, zero_tol=tol)
+        assert rw.last_report()["fallback_events"] == 1
+        again = rw.barycenter(A, C, w, be, {"reg": reg, "method": "log", "with_grad": True, "max_iter": L,
+                                            "zero_tol": tol})
+    for k in ("b", "F", "G", "grad_A", "grad_w"):  # fixed-order reductions: repeatable bit for bit
+        assert np.array_equal(again[k], got[k]), k
+
+
+def test_log_domain_gradient_finite_differences():
+    """Central differences (h = 1e-6) of ||b - b_ext||^2 with the normaliser held
+    at its value, through the log-domain kernels (forced on)."""
+    A, C, w, be = synth.barycenter_config(n=120, S=4, dim=3, salt=8)
+    L, reg = 15, 0.05
+    ctrl = {"reg": reg, "method": "log", "with_grad": True, "max_iter": L, "zero_tol": 0.0}
+    with _LogPath(1):
+        _fd_check(A, C, w, be, ctrl)
+
+
+def _fd_check(A, C, w, be, ctrl):
+    r = rw.barycenter(A, C, w, be, ctrl)
+    assert rw.last_report()["fallback_events"] == 1
+    Z0 = rw.last_report()["bary_norm"]
+
+    def obj(A_, w_):
+        q = rw.barycenter(A_, C, w_, be, ctrl)
+        braw = q["b"] * rw.last_report()["bary_norm"] / Z0
+        return float((braw - be) @ (braw - be))
+
+    gw = _fd(lambda x: obj(A, x), w, range(w.size))
+    assert np.abs(gw - r["grad_w"]).max() <= 1e-5 * max(1.0, np.abs(gw).max())
+    g = np.random.default_rng(1)
+    idx = [k for k in g.choice(A.size, 30, replace=False) if A.flat[k] > 1e-3]
+    gA = _fd(lambda X: obj(X, w), A, idx)
+    assert np.abs(gA - r["grad_A"].flat[idx]).max() <= 1e-5 * max(1.0, np.abs(gA).max())
+
+
+def test_batched_log_barycenter_falls_back_per_problem():
+    """In a batch, only the problems whose scaling form leaves its range are
+    re-run in the log domain; every result equals the single call's."""
+    probs = []
+    for i, (n, S, reg, scale) in enumerate([(150, 4, 1e-3, 1.0), (160, 5, 0.1, 1.0), (170, 3, 0.05, 100.0)]):
+        A, C, w, be = synth.barycenter_config(n=n, S=S, dim=3, salt=60 + i)
+        probs.append({"A": A, "C": C * scale, "w": w, "b_ext": be, "reg": reg, "method": "log",
+                      "with_grad": True, "max_iter": 10, "zero_tol": 0.0})
+    got = rw.batch_barycenter(probs)
+    for i, q in enumerate(probs):
+        ref = rw.barycenter(q["A"], q["C"], q["w"], q["b_ext"],
+                            {k: q[k] for k in ("reg", "method", "with_grad", "max_iter", "zero_tol")})
+        for k in ("b", "F", "G", "grad_A", "grad_w"):
+            assert np.array_equal(got[i][k], ref[k]), (i, k)
+        o = oracle.barycenter_log(q["A"], q["C"], q["w"], q["b_ext"], q["reg"], with_grad=True, max_iter=10,
+                                  zero_tol=0.0)
+        assert rel_err(got[i]["grad_A"], o["grad_A"]) <= PARITY_TOL
