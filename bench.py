@@ -1,25 +1,32 @@
 """Benchmark of the rwig_b200 engine.
 
-Default workload (the headline): log-stabilised Sinkhorn, one 4096 x 4096 FP64
-problem per solve, a, b ~ Dirichlet(0.5), support points uniform in [0,1]^2,
-squared-Euclidean cost normalised by its max, eps = 0.01, max_iter = 2000,
-zero_tol = 1e-9; outputs plan P, potentials f, g, loss.  Other workloads:
+Default workload (the headline, --workload stream): the serving stream of 200
+mixed-size log-Sinkhorn requests (n, m log-uniform in [64, 8192], eps from
+{0.01, 0.05, 0.1}, Dirichlet(1) histograms, points uniform in [0,1]^d with d
+from {2, 3, 64}, squared-Euclidean cost / max, tol 1e-9, max_iter 2000).  One
+step = one batched call over the whole stream with device-resident inputs;
+`value` = requests solved per second.  The same line carries the plain
+per-call path on the same stream ("plain"), the end-to-end batched call on
+pinned host buffers ("e2e"), the continuous-batching server's p50/p99
+latency under Poisson arrivals at 50/80/100 % of its capacity ("latency"),
+the autotuned batched call, and the WDL training workload ("wdl": V = 5000,
+K = 16 topics, batch 64, L = 20, Adam; engine steps/s, FP64-tensor fraction,
+and one batched adjoint step against the reference's own unrolled GPU step).
+Other workloads, one JSON line each:
+--workload log4096 (log-Sinkhorn 4096 x 4096, eps = 0.01, Dirichlet(0.5)),
 --workload vanilla256 (vanilla Sinkhorn 256 x 256, eps = 0.1, Dirichlet(1)),
 --workload barycenter2048 (log barycenter + gradient, N = 2048, S = 32, L = 50),
 --workload wdl5000 (WDL training steps, V = 5000, K = 16, batch 64, L = 20, Adam),
---workload stream (200 mixed-size log-Sinkhorn requests, batched vs per call),
 --workload sinkgrad2048 (log-Sinkhorn 2048 x 2048 with its gradient w.r.t. a, L = 100).
 Synthetic, seeded inputs (rwig_b200.synth); no dataset.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload W]
 
-One step = one full solve.  `value` = solves/s over all ranks with inputs
-already resident in HBM (CUDA events on the launching stream, L2 flushed
-between steps); `e2e` = the same through the host-pointer C ABI
-(rwig_sinkhorn_log) with pinned host buffers, copies included.  With N > 1
-each rank solves its own replica (the path has no exchange step).
+Timing: CUDA events on the launching stream, max over ranks; `e2e` through
+the host-pointer C ABI with pinned host buffers, copies included.  With N > 1
+each rank runs its own replica (the path has no exchange step).
 --impl reference times the reference algorithm's CPU implementation (the C++
-restatement in oracle/) on this host's cores.
+restatement in oracle/) on this host's cores, whole solves.
 """
 from __future__ import annotations
 
@@ -38,7 +45,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-DEFAULT_WORKLOAD = "log4096"
+DEFAULT_WORKLOAD = "stream"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -49,6 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="stream workload: requests per arrival rate of the serving run")
+    ap.add_argument("--no-wdl", action="store_true", help="stream: leave out the WDL block")
     ap.add_argument("--no-autotune", action="store_true",
                     help="stream workload: skip tuning the batch.* options on the stream")
     # profiling entry point: one warm-up and one measured solve of a chosen size
@@ -166,9 +174,9 @@ class SinkhornWorkload:
         from rwig_b200 import synth
         return synth.sinkhorn_problem(self.m, self.n, self.alpha, 2)
 
-    def cpu_seconds(self, threads, iters_full):
-        """CPU port time of one solve: bounded runs at two iteration counts,
-        extrapolated to the solve's iteration count."""
+    def cpu_seconds(self, threads, iters_full=None):
+        """CPU port time of one whole solve of the problem, timed (vanilla:
+        repeated whole solves for at least 2 s, 1 thread)."""
         import oracle
         a, b, C = self.inputs()
         if self.method == "vanilla":
@@ -182,18 +190,12 @@ class SinkhornWorkload:
                     break
             secs = (time.perf_counter() - t0) / k
             return secs, threads, f"{k} full solves of the same problem, 1 thread"
-        lo, hi = 2, 8
-        t = {}
-        for it in (lo, hi):
-            t0 = time.perf_counter()
-            oracle.sinkhorn_log(a, b, C, self.reg, max_iter=it, zero_tol=0.0, n_threads=threads, want_P=True)
-            t[it] = time.perf_counter() - t0
-        per_iter = max((t[hi] - t[lo]) / (hi - lo), 1e-9)
-        fixed = max(t[lo] - lo * per_iter, 0.0)
-        secs = fixed + iters_full * per_iter
-        sample = (f"{lo}- and {hi}-iteration runs of the same {self.m}x{self.n} problem ({threads} threads), "
-                  f"extrapolated to a {iters_full}-iteration solve: {per_iter * 1e3:.1f} ms/iteration, "
-                  f"{fixed * 1e3:.0f} ms fixed")
+        t0 = time.perf_counter()
+        r = oracle.sinkhorn_log(a, b, C, self.reg, max_iter=self.max_iter, zero_tol=self.tol, n_threads=threads,
+                                want_P=True)
+        secs = time.perf_counter() - t0
+        sample = (f"one whole {r['iter']}-iteration solve of the same {self.m}x{self.n} problem with the plan "
+                  f"({threads} threads): {secs:.1f} s")
         return secs, threads, sample
 
     def reference_iters(self):
@@ -304,7 +306,7 @@ class SinkhornWorkload:
                 "all_kernels_ms_per_solve": kms}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1, int(round(it_mean)))
+            secs, cores, sample = self.cpu_seconds(os.cpu_count() or 1)
             cpu = {"value": 1.0 / secs, "unit": self.unit, "cores": cores, "kind": "port", "sample": sample}
         ref_gpu = None
         if self.method == "vanilla" and world == 1:
@@ -324,13 +326,12 @@ class SinkhornWorkload:
                 "clocks": clocks.summary()}
 
     def reference(self, args):
+        """Each step one whole solve on all host threads (one untimed solve first)."""
         threads = os.cpu_count() or 1
-        iters = self.reference_iters()
-        for _ in range(args.warmup):
-            self.cpu_seconds(threads, iters)
+        self.cpu_seconds(threads)
         secs, cores, sample = [], 1, ""
         for _ in range(args.steps):
-            s_, cores, sample = self.cpu_seconds(threads, iters)
+            s_, cores, sample = self.cpu_seconds(threads)
             secs.append(s_)
         return sum(secs), cores, sample
 
@@ -708,19 +709,33 @@ def device_cost(x, y, dev):
 
 
 class StreamWorkload:
-    """A stream of mixed-size log-Sinkhorn requests, solved by the batched
-    launch (value) and, for comparison, one rwig_sinkhorn_log_dev call per
-    request on the same device-resident inputs."""
+    """The serving stream of mixed-size log-Sinkhorn requests (the headline).
+
+    One step = one batched call (rwig_batch_sinkhorn_log_dev) over the whole
+    200-request stream with device-resident inputs; `value` = requests solved
+    per second over the K timed calls.  Beside it on the same line: the plain
+    per-call path (one rwig_sinkhorn_log_dev call per request), the end-to-end
+    batched call with pinned host buffers, the continuous-batching server's
+    p50/p99 latency under Poisson arrivals, the autotuned batched call, and the
+    WDL training step (engine vs the reference's own unrolled GPU step)."""
 
     higher_is_better = True
 
     def __init__(self, R=200, max_iter=2000, tol=1e-9):
         self.R, self.max_iter, self.tol = R, max_iter, tol
         self.unit = "solves/s"
-        self.metric = "batched log-Sinkhorn solves/s on the mixed-size request stream (FP64)"
+        self.metric = "batched vs plain solves/s, p50/p99 latency @err<1e-10 FP64; WDL steps/s"
         self.desc = (f"{R} log-Sinkhorn requests: n, m log-uniform in [64, 8192], eps from {{0.01, 0.05, 0.1}}, "
                      f"Dirichlet(1) histograms, points uniform in [0,1]^d with d from {{2, 3, 64}}, "
                      f"squared-Euclidean cost / max, tol {tol:g}, max_iter {max_iter}, outputs f, g, loss")
+
+    def config(self, world):
+        """The same dict on the engine and the reference arm."""
+        from rwig_b200 import synth
+        gb = sum(q["m"] * q["n"] for q in synth.stream_requests(self.R)) * 8 / 1e9
+        return {"workload": self.desc, "parallelism": f"replicas x{world}",
+                "step": f"one batched call over the whole {self.R}-request stream (value counts requests)",
+                "l2": f"no flush: the stream's cost matrices ({gb:.1f} GB) exceed L2"}
 
     def build(self, dev):
         import torch
@@ -759,19 +774,27 @@ class StreamWorkload:
         sp = ctypes.c_void_p(stream.cuda_stream)
         probs = self.problems(data)
         res = (_lib.Result * R)()
-        # warm-up: the whole batched call (sizes the engine's scratch arena)
+        # warm-up: whole batched calls (the first sizes the engine's scratch arena)
         for _ in range(max(1, args.warmup)):
             _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
         torch.cuda.synchronize()
+        launches = 0
         with clocks_cls(dev.index) as clocks:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
             torch.cuda.synchronize()
-            e0.record(stream)
-            _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
-            e1.record(stream)
-            e1.synchronize()
-            batch_ms = e0.elapsed_time(e1)
-        launches = rw.last_report()["kernel_launches"]
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            for e0, e1 in evs:
+                e0.record(stream)
+                _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, R, res, sp))
+                e1.record(stream)
+                launches += rw.last_report()["kernel_launches"]
+            torch.cuda.synchronize()
+            step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
+        total_ms = max_over_ranks(sum(step_ms), world, dev)
+        batch_ms = total_ms / args.steps
         bres = [res[i].as_dict() for i in range(R)]
         bf = [d["f"].cpu().numpy() for d in data]
         # the per-call path on the same inputs; one untimed pass first sizes its
@@ -804,22 +827,31 @@ class StreamWorkload:
             assert bres[i]["iter"] == piters[i], (i, bres[i]["iter"], piters[i])
             pf = d["f"].cpu().numpy()
             worst = max(worst, float(np.abs(bf[i] - pf).max() / max(np.abs(pf).max(), 1e-300)))
-        # end to end: host inputs through rwig_batch_sinkhorn_log
-        hC = [d["C"].cpu().numpy() for d in data]  # (n, m) row-major = column-major m x n
-        harr = (_lib.Problem * R)()
-        keep = []
+        assert worst <= 1e-10, worst
+        # end to end: pinned host inputs through rwig_batch_sinkhorn_log (copies in and out every call)
+        hC, harr, keep = [], (_lib.Problem * R)(), []
         for i, d in enumerate(data):
             q = d["q"]
-            f, g = np.zeros(q["m"]), np.zeros(q["n"])
-            keep.append((f, g))
-            hv = lambda x: ctypes.c_void_p(x.ctypes.data)  # noqa: E731
-            harr[i] = _lib.Problem(hv(d["ha"]), hv(d["hb"]), hv(hC[i]), q["m"], q["n"], q["eps"], self.max_iter,
-                                   self.tol, None, hv(f), hv(g))
-        t0 = time.perf_counter()
+            pc = torch.empty(d["C"].shape, dtype=torch.float64, pin_memory=True)
+            pc.copy_(d["C"])
+            ha = torch.from_numpy(d["ha"]).pin_memory()
+            hb = torch.from_numpy(d["hb"]).pin_memory()
+            f = torch.zeros(q["m"], dtype=torch.float64, pin_memory=True)
+            g = torch.zeros(q["n"], dtype=torch.float64, pin_memory=True)
+            keep.append((pc, ha, hb, f, g))
+            hC.append(pc.numpy())  # (n, m) row-major = column-major m x n
+            hp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+            harr[i] = _lib.Problem(hp(ha), hp(hb), hp(pc), q["m"], q["n"], q["eps"], self.max_iter, self.tol, None,
+                                   hp(f), hp(g))
+        n_e2e = max(1, min(args.steps, 3))
         _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
-        e2e_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            _lib.check(L.rwig_batch_sinkhorn_log(harr, R, res))
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / n_e2e, world, dev)
         serving = self.serve(data, hC, R / (batch_ms / 1e3), args.serve_requests)
         tuned = None if args.no_autotune else self.autotuned(data, hC, probs, res, sp, stream)
+        wdl = None if args.no_wdl else self.wdl_block(args, dev)
         if rank != 0:
             return None
         hbm, src = measured_peaks()
@@ -828,26 +860,27 @@ class StreamWorkload:
         achieved = alg / (batch_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "peak_source": src,
-                "kernel": "service_kernel (a team of CTAs per problem)",
-                "alg_bytes": alg, "note": "K read once per iteration plus the K build and final passes; "
-                                           "small problems stay in L2, so frac may exceed 1"}
+                "kernel": "service_kernel (a team of CTAs per problem), whole batched call",
+                "alg_bytes_per_step": alg,
+                "note": "K read once per iteration plus the K build and final passes per request; strips of "
+                        "small problems stay in shared memory or L2, so this is the stream's effective rate"}
         in_kernel = sum(1 for r in bres if r["path"] == 0)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = self.cpu_baseline(data, bres)
-        return {"value": R * world / (batch_ms / 1e3), "ms_per_step": batch_ms / R,
-                "config": {"workload": self.desc, "parallelism": f"replicas x{world}",
-                           "step": "one request; the whole stream is one batched call",
-                           "requests_in_batched_kernel": in_kernel,
-                           "l2": "no flush (the stream itself is the workload)"},
+            cpu = self.cpu_baseline(budget_s=15.0)
+        cfg = self.config(world)
+        cfg["requests_in_batched_kernel"] = in_kernel
+        return {"value": R * args.steps * world / (total_ms / 1e3), "ms_per_step": batch_ms,
+                "config": cfg,
                 "plain": {"value": R / (plain_ms / 1e3), "unit": self.unit,
                           "path": "one rwig_sinkhorn_log_dev call per request, device-resident inputs",
                           "speedup_batched_over_plain": plain_ms / batch_ms,
-                          "max_rel_diff_f_vs_batched": worst},
+                          "max_rel_diff_f_vs_batched": worst, "iterations_equal": True},
                 "e2e": {"value": R / e2e_s, "unit": self.unit,
-                        "h2d_bytes_per_step": sum((e + d["q"]["m"] + d["q"]["n"]) * 8 for e, d in zip(elems, data)) / R,
-                        "d2h_bytes_per_step": sum((d["q"]["m"] + d["q"]["n"]) * 8 for d in data) / R},
-                "serving": serving, "autotuned": tuned,
+                        "h2d_bytes_per_step": sum((e + d["q"]["m"] + d["q"]["n"]) * 8 for e, d in zip(elems, data)),
+                        "d2h_bytes_per_step": sum((d["q"]["m"] + d["q"]["n"]) * 8 + 16 * 8 for d in data),
+                        "call": f"rwig_batch_sinkhorn_log on pinned host buffers, mean of {n_e2e} calls"},
+                "latency": serving, "autotuned": tuned, "wdl": wdl,
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
 
     def autotuned(self, data, hC, probs, res, sp, stream):
@@ -964,32 +997,93 @@ class StreamWorkload:
                                   "p99_ms": ms(plat, 99)}}
         return out
 
-    def cpu_baseline(self, data, bres):
-        """The oracle (all host threads) on the three smallest requests, scaled
-        to the stream by element-iterations."""
-        import oracle
-        order = sorted(range(len(data)), key=lambda i: data[i]["q"]["m"] * data[i]["q"]["n"])[:3]
-        t = 0.0
-        work = 0.0
-        for i in order:
-            d = data[i]
-            C = d["C"].cpu().numpy().T
-            t0 = time.perf_counter()
-            r = oracle.sinkhorn_log(d["ha"], d["hb"], C, d["q"]["eps"], max_iter=self.max_iter, zero_tol=self.tol,
-                                    n_threads=os.cpu_count() or 1, want_P=False)
-            t += time.perf_counter() - t0
-            work += (r["iter"] + 2) * d["q"]["m"] * d["q"]["n"]
-        total = sum((bres[i]["iter"] + 2) * data[i]["q"]["m"] * data[i]["q"]["n"] for i in range(len(data)))
-        secs = t * total / work
-        return {"value": len(data) / secs, "unit": self.unit, "cores": os.cpu_count() or 1, "kind": "port",
-                "sample": f"3 smallest requests solved by the oracle ({t:.2f} s), scaled by element-iterations"}
+    def wdl_block(self, args, dev):
+        """The WDL training workload (V = 5000, K = 16 topics, batch 64, L = 20,
+        Adam) beside the stream: engine training steps through rwig_wdl (device
+        time inside the call), and one batched adjoint step -- the engine's
+        rwig_wdl_batch_grad_dev against the reference's own unrolled GPU step
+        (wdl_batch, src/cuda_wdl.cu:385, compiled from its sources into
+        oracle/_ref) on the same device-resident batch, both timed with CUDA
+        events, their gradients compared."""
+        import torch
 
-    def reference(self, args):
-        """The oracle (all host threads) on the three smallest requests, timed in
-        full, scaled to the whole stream by element-iterations; the stream's
-        per-request iteration counts come from tests/golden/stream_iters.json
-        (tests/golden/make_stream_iters.py).  Returns the time of `steps`
-        requests at the stream's mean cost per request."""
+        import oracle
+        import rwig_b200 as rw
+        from rwig_b200 import _lib
+        wl = WdlWorkload()
+        Y, C, A0, L0 = wl.data()
+        L = _lib.load()
+        N, M, S, B = wl.V, wl.M, wl.S, wl.B
+        A = np.zeros((N, S), order="F")
+        W = np.zeros((S, M), order="F")
+        dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+        steps, warm = 6, 2
+
+        def train(k):
+            _lib.check(L.rwig_wdl(dp(A), dp(W), None, dp(Y), dp(C), N, M, S, wl.reg, wl.L, 1e-6, B, 1000, 1,
+                                  wl.lr, 0.01, 0.9, 0.999, 1e-8, 42, 0, dp(A0), dp(L0), int(k)))
+            return rw.last_report()
+
+        train(warm)
+        rep = train(steps)
+        tf_peak = measured_dgemm_tflops(dev)
+        achieved = wl.step_flops() * steps / (rep["device_ms"] / 1e3) / 1e12
+        out = {"workload": wl.desc, "steps_per_s": steps / (rep["device_ms"] / 1e3), "unit": "steps/s",
+               "steps_timed": steps, "ms_per_step": rep["device_ms"] / steps,
+               "roofline": {"bound": "tensor", "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
+                            "frac": achieved / tf_peak, "flops_per_step": wl.step_flops(),
+                            "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU"},
+               "gpu_launches_per_step": rep["kernel_launches"] / steps}
+        # one batched adjoint step on batch 0, device-resident K: engine vs the reference's wdl_batch
+        Ah = oracle.col_softmax(A0)
+        Wh = oracle.col_softmax(L0)[:, :B].copy(order="F")
+        Yb = np.asfortranarray(Y[:, :B])
+        K = np.asfortranarray(np.exp(-C / wl.reg))
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)  # noqa: E731  column-major on device
+        dA, dW, dY, dK = t(Ah), t(Wh), t(Yb), t(K)
+        gA = torch.empty((S, N), dtype=torch.float64, device=dev)
+        gl = torch.empty(S, dtype=torch.float64, device=dev)
+        stream = torch.cuda.current_stream()
+        vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+
+        def engine_step():
+            _lib.check(L.rwig_wdl_batch_grad_dev(vp(gA), vp(gl), vp(dA), vp(dW), vp(dY), vp(dK), N, S, B, wl.reg,
+                                                 wl.L, 0, ctypes.c_void_p(stream.cuda_stream)))
+
+        engine_step()
+        ts = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            engine_step()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        eng_ms = float(np.mean(ts))
+        adj = {"batch": f"batch 0: {B} documents, K given (mode 0)", "engine_ms": eng_ms,
+               "engine_call": "rwig_wdl_batch_grad_dev, mean of 3 after 1 untimed"}
+        if oracle.ref_gpu_available():
+            rgA, rgl, ref_ms = oracle.ref_gpu_wdl_batch_grad(Ah, Wh, Yb, K, wl.reg, wl.L, mode=0, reps=3)
+            egA = gA.cpu().numpy().T
+            rel = float(np.abs(egA - rgA).max() / np.abs(rgA).max())
+            adj.update(reference_ms=ref_ms, speedup_engine_over_reference=ref_ms / eng_ms,
+                       reference_call="wdl_batch (src/cuda_wdl.cu:385) built from the reference's sources, cuBLAS "
+                                      "DGEMMs, mean of 3 calls (CUDA events on its stream)",
+                       max_rel_diff_g_alpha=rel)
+        out["adjoint_step"] = adj
+        return out
+
+    def _work(self, reqs, iters):
+        return [(iters[i] + 2) * reqs[i]["m"] * reqs[i]["n"] for i in range(len(reqs))]
+
+    def cpu_sample(self, budget_s=None, steps=None):
+        """Whole log-Sinkhorn solves of the stream's requests by the oracle (all
+        host threads), timed one by one: requests taken in the stream's order
+        among those of at most 2^24 elements (each seconds, not minutes, on the
+        host), until `steps` solves or `budget_s` seconds.  Returns a list of
+        (seconds, element-iterations) per solve and the stream's mean
+        element-iterations per request, from the per-request iteration counts
+        in tests/golden/stream_iters.json (tests/golden/make_stream_iters.py)."""
         import oracle
         from rwig_b200 import synth
         path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "stream_iters.json")
@@ -998,27 +1092,48 @@ class StreamWorkload:
         reqs = synth.stream_requests(self.R)
         if len(iters) != len(reqs):
             raise RuntimeError("stream_iters.json does not match the stream")
-        elems = [q["m"] * q["n"] for q in reqs]
-        order = sorted(range(len(reqs)), key=lambda i: elems[i])[:3]
+        work = self._work(reqs, iters)
+        mean_work = sum(work) / len(work)
+        pick = [i for i, q in enumerate(reqs) if q["m"] * q["n"] <= (1 << 24)]
         threads = os.cpu_count() or 1
-        secs = []
-        for _ in range(max(1, args.warmup) + args.steps):
-            t, work = 0.0, 0.0
-            for i in order:
-                q = reqs[i]
-                a, b, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
-                C = synth.sq_euclid_cost(x, y)
-                t0 = time.perf_counter()
-                r = oracle.sinkhorn_log(a, b, C, q["eps"], max_iter=self.max_iter, zero_tol=self.tol,
-                                        n_threads=threads, want_P=False)
-                t += time.perf_counter() - t0
-                work += (r["iter"] + 2) * elems[i]
-            total = sum((iters[i] + 2) * elems[i] for i in range(len(reqs)))
-            secs.append(t * total / work / len(reqs))  # mean seconds per request
-        per = secs[max(1, args.warmup):]
-        sample = (f"the 3 smallest requests solved by the oracle ({threads} threads), scaled to the 200-request "
-                  f"stream by element-iterations")
-        return sum(per), threads, sample
+        out, k, t_all = [], 0, 0.0
+        while (steps is not None and len(out) < steps) or (budget_s is not None and t_all < budget_s):
+            q = reqs[pick[k % len(pick)]]
+            k += 1
+            a, b, x, y = synth.stream_request_data(q["m"], q["n"], q["d"], q["salt"])
+            C = synth.sq_euclid_cost(x, y)
+            t0 = time.perf_counter()
+            r = oracle.sinkhorn_log(a, b, C, q["eps"], max_iter=self.max_iter, zero_tol=self.tol,
+                                    n_threads=threads, want_P=False)
+            dt = time.perf_counter() - t0
+            t_all += dt
+            out.append((dt, (r["iter"] + 2) * q["m"] * q["n"]))
+        return out, mean_work, threads, len(pick)
+
+    def cpu_baseline(self, budget_s=15.0):
+        solves, mean_work, threads, npick = self.cpu_sample(budget_s=budget_s)
+        t = sum(s for s, _ in solves)
+        w = sum(x for _, x in solves)
+        value = (w / mean_work) / t
+        return {"value": value, "unit": self.unit, "cores": threads, "kind": "port",
+                "sample": f"{len(solves)} whole solves ({t:.1f} s) of the stream's requests of <= 2^24 elements "
+                          f"({npick} of {self.R}) by the oracle on {threads} threads; value = stream-mean requests "
+                          f"per second, the solves' element-iterations divided by the stream's mean per request "
+                          f"({mean_work:.3g})"}
+
+    def reference(self, args):
+        """--impl reference: each step one whole solve of a stream request (the
+        oracle on all host threads, as cpu_sample); value in stream-mean
+        requests per second (element-iteration weighted)."""
+        solves, mean_work, threads, npick = self.cpu_sample(steps=max(1, args.warmup) + args.steps)
+        timed = solves[max(1, args.warmup):]
+        t = sum(s for s, _ in timed)
+        w = sum(x for _, x in timed)
+        sample = (f"each step one whole log-Sinkhorn solve of a stream request of <= 2^24 elements ({npick} of "
+                  f"{self.R}, in stream order) by the oracle on {threads} threads; value = the solves' "
+                  f"element-iterations / the stream's mean per request ({mean_work:.3g}) per second")
+        return {"seconds": t, "value": (w / mean_work) / t, "cores": threads, "sample": sample,
+                "requests_per_step": (w / mean_work) / len(timed)}
 
 
 class GradWorkload:
@@ -1201,14 +1316,23 @@ def base_line(wl, args, world):
 
 
 def run_reference(args):
+    """The reference's CPU path (the oracle port, all host threads) on the same
+    workload; rank 0 alone runs and prints, the other ranks exit."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     wl = WORKLOADS[args.workload]
-    tot, cores, sample = wl.reference(args)
-    value = args.steps / tot
+    r = wl.reference(args)
+    extra = {}
+    if isinstance(r, dict):
+        tot, cores, sample, value = r["seconds"], r["cores"], r["sample"], r["value"]
+        extra["requests_per_step"] = r["requests_per_step"]
+    else:
+        tot, cores, sample = r
+        value = args.steps / tot
+    cfg = wl.config(args.gpus) if hasattr(wl, "config") else {"workload": wl.desc, "parallelism": "cpu"}
     line = {"impl": "reference", **base_line(wl, args, args.gpus), "value": value,
-            "ms_per_step": tot / args.steps * 1e3, "config": {"workload": wl.desc, "parallelism": "cpu"},
+            "ms_per_step": tot / args.steps * 1e3, "config": cfg, **extra,
             "cpu_baseline": {"value": value, "unit": wl.unit, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
