@@ -1050,18 +1050,37 @@ class StreamWorkload:
             _lib.check(L.rwig_wdl_batch_grad_dev(vp(gA), vp(gl), vp(dA), vp(dW), vp(dY), vp(dK), N, S, B, wl.reg,
                                                  wl.L, 0, ctypes.c_void_p(stream.cuda_stream)))
 
-        engine_step()
-        ts = []
-        for _ in range(3):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+        def timed_step():
             engine_step()
-            e1.record(stream)
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        eng_ms = float(np.mean(ts))
+            ts = []
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                engine_step()
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return float(np.mean(ts))
+
+        eng_ms = timed_step()
+        full_gA = gA.cpu().numpy()
         adj = {"batch": f"batch 0: {B} documents, K given (mode 0)", "engine_ms": eng_ms,
                "engine_call": "rwig_wdl_batch_grad_dev, mean of 3 after 1 untimed"}
+        # checkpointed adjoint (wdl.checkpoint = k): history footprint and step time
+        NW, ND = N * S * B * 8, N * B * 8
+        ck = {}
+        for kk in (wl.L, 5, 4, 1):
+            L.rwig_set_option(b"wdl.checkpoint", float(kk))
+            try:
+                ms_k = timed_step()
+                same = bool(np.array_equal(gA.cpu().numpy(), full_gA))
+            finally:
+                L.rwig_set_option(b"wdl.checkpoint", float("nan"))
+            nseg = -(-wl.L // kk)
+            hist = (nseg + 4 * kk + 3) * NW + (kk + 1) * ND
+            ck[f"k{kk}"] = {"ms": ms_k, "history_bytes": hist, "products": wl.products() + 2 * (wl.L - kk),
+                            "gradient_bitwise_equal_to_full_history": same}
+        adj["checkpointing"] = ck
         if oracle.ref_gpu_available():
             rgA, rgl, ref_ms = oracle.ref_gpu_wdl_batch_grad(Ah, Wh, Yb, K, wl.reg, wl.L, mode=0, reps=3)
             egA = gA.cpu().numpy().T

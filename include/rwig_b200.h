@@ -95,6 +95,12 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       over by later ones that fit the free CTAs (default 5000);
  *   "wdl.infer_docs": documents per stacked-column chunk of WDL inference
  *       (default 1024);
+ *   "wdl.checkpoint": k > 0 keeps the WDL forward state only every k-th
+ *       iteration plus one segment of k iterations and recomputes the other
+ *       segments during the backward (same gradient bits; 2 (L - k) more
+ *       products; ceil(L/k) + 4k + 3 history slots of N x S D doubles
+ *       instead of 4 (L + 1)); 0 (default) or k >= L keeps every
+ *       iteration;
  *   "dgemm.kshape", "dgemm.tile": DMMA instruction shape (k = 4, 8 or 16)
  *       and tile height (0 automatic, 64, 128) of rwig_selftest_dgemm only;
  *   "barycenter.log_path": the log barycenter's route: 0 (default) the

@@ -327,6 +327,43 @@ def wdl_batch_grad_dp(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0, group=None, gr
     return np.asfortranarray(out[:N * S].reshape((N, S), order="F")), out[N * S:].copy()
 
 
+def wdl_batch_grad_dp_dev(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0, group=None, stream=None):
+    """Data-parallel batched WDL gradient on device buffers (one process per
+    GPU, torch.distributed group).  Matrices are contiguous float64 CUDA
+    tensors in column-major order, i.e. an R x C matrix is a (C, R) tensor:
+    A (S, N), W_B (D, S), Y_B (D, N) and K_or_C (N, N), the last resident on
+    the device for as long as the caller keeps it (it is not copied per call).
+    Rank r computes the mean gradient of documents [r D / R, (r + 1) D / R)
+    with rwig_wdl_batch_grad_dev straight into one device buffer, scales it by
+    its shard size, and one all-reduce of that buffer (g_Alpha then g_lambda,
+    N S + S doubles) on the device gives every rank the whole batch's mean
+    (src/wdl_impl.cpp:236-243).  Returns device tensors (g_Alpha as (S, N),
+    g_lambda (S,)); nothing passes through host memory."""
+    import torch
+    import torch.distributed as dist
+    S, N = A.shape
+    D = W_B.shape[0]
+    if W_B.shape[1] != S or Y_B.shape != (D, N) or K_or_C.shape != (N, N):
+        raise ValueError("A (S, N), W_B (D, S), Y_B (D, N) and K_or_C (N, N) do not match")
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    lo, hi = rank * D // world, (rank + 1) * D // world
+    buf = torch.zeros(N * S + S, dtype=torch.float64, device=A.device)
+    st = stream if stream is not None else torch.cuda.current_stream(A.device)
+    st.wait_stream(torch.cuda.current_stream(A.device))  # buf zeroed, inputs written
+    if hi > lo:
+        gA, gl = buf[:N * S], buf[N * S:]
+        rc = _lib.load().rwig_wdl_batch_grad_dev(_ptr(gA), _ptr(gl), _ptr(A), _ptr(W_B[lo:hi]), _ptr(Y_B[lo:hi]),
+                                                 _ptr(K_or_C), N, S, hi - lo, float(reg), int(L), int(mode),
+                                                 ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc)
+        with torch.cuda.stream(st):
+            buf.mul_(float(hi - lo))
+    with torch.cuda.stream(st):
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+        buf.div_(float(D))
+    return buf[:N * S].view(S, N), buf[N * S:]
+
+
 def _cost_or_points(q):
     """(C, None, None) from q["C"], or (None, X, Y) from point clouds q["x"]
     (M x d), q["y"] (N x d), column-major; sizes checked against a, b."""

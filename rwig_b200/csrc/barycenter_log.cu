@@ -345,7 +345,7 @@ __global__ void finish_b(const double* logb, int N, const double* bext, double* 
 }
 
 enum {
-  SL_FH = 140, SL_GH, SL_MH, SL_RH, SL_LB, SL_LOGA, SL_D, SL_GRAM, SL_PMAX, SL_PSUM, SL_FBAR, SL_Y, SL_GA,
+  SL_FH = 300, SL_GH, SL_MH, SL_RH, SL_LB, SL_LOGA, SL_D, SL_GRAM, SL_PMAX, SL_PSUM, SL_FBAR, SL_Y, SL_GA,
   SL_GWP, SL_GW, SL_BN, SL_SCAL
 };
 

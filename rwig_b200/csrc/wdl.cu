@@ -342,7 +342,7 @@ __global__ void opt_step(double* th, double* m, double* v, const double* g, int 
 enum {
   SW_UH = 120, SW_VH, SW_KVH, SW_KTH, SW_BH, SW_T, SW_T2, SW_AB, SW_GWP, SW_DOT, SW_WBAR, SW_K,
   SW_Y, SW_C, SW_ALPHA, SW_LAMBDA, SW_A, SW_W, SW_MA, SW_VA, SW_ML, SW_VL, SW_GA, SW_GL, SW_YHAT,
-  SW_HA, SW_HW, SW_HY, SW_HK, SW_HOUT, SW_IU, SW_IV, SW_IKV, SW_IKT, SW_IB, SW_IERR, SW_IST
+  SW_HA, SW_HW, SW_HY, SW_HK, SW_HOUT, SW_IU, SW_IV, SW_IKV, SW_IKT, SW_IB, SW_IERR, SW_IST, SW_VCK
 };
 
 // Columns per GEMM tile: whole documents, at most 64.
@@ -543,6 +543,17 @@ int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const
 
 // Batched gradient on device buffers: K padded (ldk), A (N x S), Wb (S x D),
 // Yb (N x D); outputs gA (N x S) and gl (S).
+//
+// Checkpointing (option "wdl.checkpoint" = k, 0 or >= L: none).  The state
+// the backward step l reads -- KVB_{l-1}, UB_l, KTUB_l, VB_l, bB_l -- is what
+// forward iteration l-1 writes from VB_{l-1} alone.  The forward keeps VB at
+// every k-th iteration (VB_0, VB_k, ...) and the full state of one segment of
+// k iterations; the backward runs the segments newest first, recomputing each
+// earlier segment's states from its checkpoint into the segment buffers
+// before unrolling it.  The recomputation runs the same products on the same
+// inputs, so the gradient is bitwise that of the full history; it costs
+// 2 (L - k') extra products (k' the last segment's length) and holds
+// ceil(L / k) + 4 k + 3 state slots of N x S D doubles instead of 4 (L + 1).
 int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const double* A, const double* Wb,
                const double* Yb, const double* K, long long ldk, int N, int S, int D, int L, int* launches) {
   const int SD = S * D;
@@ -552,53 +563,67 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
     RWIG_CUDA_TRY(cudaMemsetAsync(gl, 0, sizeof(double) * S, st));
     return 0;
   }
+  const int kopt = (int)option("wdl.checkpoint", 0.0);
+  const int k = (kopt <= 0 || kopt >= L) ? L : kopt;  // segment length
+  const int nseg = (L + k - 1) / k;
   const int ngrp = (N + 7) / 8;
-  double* Uh = (double*)scratch(ctx, SW_UH, sizeof(double) * NW * (L + 1));
-  double* Vh = (double*)scratch(ctx, SW_VH, sizeof(double) * NW * (L + 1));
-  double* KVh = (double*)scratch(ctx, SW_KVH, sizeof(double) * NW * (L + 1));
-  double* KTh = (double*)scratch(ctx, SW_KTH, sizeof(double) * NW * (L + 1));
-  double* Bh = (double*)scratch(ctx, SW_BH, sizeof(double) * ND * (L + 1));
+  // segment buffers, local index t = l - j k (t = 0..k); V's slot 0 is the checkpoint
+  double* Us = (double*)scratch(ctx, SW_UH, sizeof(double) * NW * (k + 1));
+  double* Vs = (double*)scratch(ctx, SW_VH, sizeof(double) * NW * (k + 1));
+  double* KVs = (double*)scratch(ctx, SW_KVH, sizeof(double) * NW * k);
+  double* KTs = (double*)scratch(ctx, SW_KTH, sizeof(double) * NW * (k + 1));
+  double* Bs = (double*)scratch(ctx, SW_BH, sizeof(double) * ND * (k + 1));
+  double* Vck = (double*)scratch(ctx, SW_VCK, sizeof(double) * NW * nseg);  // VB_{j k}
   double* T = (double*)scratch(ctx, SW_T, sizeof(double) * NW);
   double* T2 = (double*)scratch(ctx, SW_T2, sizeof(double) * NW);
   double* AB = (double*)scratch(ctx, SW_AB, sizeof(double) * NW);
   double* gwp = (double*)scratch(ctx, SW_GWP, sizeof(double) * (size_t)ngrp * SD);
   double* dot = (double*)scratch(ctx, SW_DOT, sizeof(double) * SD);
   double* wbar = (double*)scratch(ctx, SW_WBAR, sizeof(double) * SD);
-  if (!Uh || !Vh || !KVh || !KTh || !Bh || !T || !T2 || !AB || !gwp || !dot || !wbar) return RWIG_E_NOMEM;
-  auto U = [&](int l) { return Uh + NW * l; };
-  auto V = [&](int l) { return Vh + NW * l; };
-  auto KV = [&](int l) { return KVh + NW * l; };
-  auto KT = [&](int l) { return KTh + NW * l; };
-  auto Bb = [&](int l) { return Bh + ND * l; };
+  if (!Us || !Vs || !KVs || !KTs || !Bs || !Vck || !T || !T2 || !AB || !gwp || !dot || !wbar) return RWIG_E_NOMEM;
+  auto U = [&](int t) { return Us + NW * t; };
+  auto V = [&](int j, int t) { return t == 0 ? Vck + NW * j : Vs + NW * t; };
+  auto KV = [&](int t) { return KVs + NW * t; };
+  auto KT = [&](int t) { return KTs + NW * t; };
+  auto Bb = [&](int t) { return Bs + ND * t; };
+  auto seg_len = [&](int j) { return std::min(k, L - j * k); };
   const int tc = tile_cols(S, SD);
   auto gemm = [&](int trans, const double* X, auto epi) -> int {
     const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
     return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
   };
-  fill<<<grid_for(ctx, NW), TPB, 0, st>>>(V(0), NW, 1.0);
+  // forward iterations j k .. j k + len - 1 (wdl_impl.cpp:124-160)
+  auto forward_segment = [&](int j) -> int {
+    for (int t = 0; t < seg_len(j); ++t) {
+      if (int rc = gemm(0, V(j, t), EpiY{A, N, S, SD, KV(t), U(t + 1)})) return rc;
+      if (int rc = gemm(1, U(t + 1), EpiZ{Wb, N, S, SD, KT(t + 1), V(j, t + 1), Bb(t + 1)})) return rc;
+    }
+    return 0;
+  };
+  fill<<<grid_for(ctx, NW), TPB, 0, st>>>(V(0, 0), NW, 1.0);
   ++*launches;
   int rc;
-  for (int l = 0; l < L; ++l) {  // wdl_impl.cpp:124-160
-    rc = gemm(0, V(l), EpiY{A, N, S, SD, KV(l), U(l + 1)});
-    if (rc) return rc;
-    rc = gemm(1, U(l + 1), EpiZ{Wb, N, S, SD, KT(l + 1), V(l + 1), Bb(l + 1)});
-    if (rc) return rc;
+  for (int j = 0; j < nseg; ++j) {
+    if ((rc = forward_segment(j))) return rc;
+    if (j + 1 < nseg)  // VB_{(j+1) k}, the next segment's checkpoint
+      RWIG_CUDA_TRY(cudaMemcpyAsync(V(j + 1, 0), V(j, k), sizeof(double) * NW, cudaMemcpyDeviceToDevice, st));
   }
   RWIG_CUDA_TRY(cudaMemsetAsync(AB, 0, sizeof(double) * NW, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(gwp, 0, sizeof(double) * (size_t)ngrp * SD, st));
-  for (int l = L; l >= 1; --l) {  // :169-218
-    const bool seed = (l == L);
-    const EpiB1 e1{KT(l), V(l), Wb, Bb(l), Yb, N, S, SD, seed ? 1 : 0, T2, gwp};
-    if (seed) {
-      dim3 grid(ngrp, (SD + tc - 1) / tc);
-      seed_b1<<<grid, TPB, sizeof(double) * 2 * tc * 8, st>>>(e1, N, tc);
-      ++*launches;
-    } else {
-      rc = gemm(1, T, e1);  // K^T T
-      if (rc) return rc;
+  for (int j = nseg - 1; j >= 0; --j) {  // :169-218, segments newest first
+    if (j != nseg - 1 && (rc = forward_segment(j))) return rc;  // recompute from VB_{j k}
+    for (int t = seg_len(j); t >= 1; --t) {
+      const bool seed = (j * k + t == L);
+      const EpiB1 e1{KT(t), V(j, t), Wb, Bb(t), Yb, N, S, SD, seed ? 1 : 0, T2, gwp};
+      if (seed) {
+        dim3 grid(ngrp, (SD + tc - 1) / tc);
+        seed_b1<<<grid, TPB, sizeof(double) * 2 * tc * 8, st>>>(e1, N, tc);
+        ++*launches;
+      } else {
+        if ((rc = gemm(1, T, e1))) return rc;  // K^T T
+      }
+      if ((rc = gemm(0, T2, EpiB2{U(t), KV(t - 1), N, SD, AB, T}))) return rc;  // K T2
     }
-    rc = gemm(0, T2, EpiB2{U(l), KV(l - 1), N, SD, AB, T});  // K T2
-    if (rc) return rc;
   }
   col_dots<<<SD, TPB, 0, st>>>(A, AB, N, S, dot);
   alpha_grad<<<grid_for(ctx, (long long)N * S), TPB, 0, st>>>(A, AB, dot, N, S, D, gA);

@@ -127,3 +127,42 @@ def test_batched_inference_chunks_and_per_document_stops():
         for o in outs:
             assert rel_err(o["Yhat"][:, m], r["b"]) <= 1e-9, (m, rel_err(o["Yhat"][:, m], r["b"]))
     assert len(iters) > 1, iters  # the documents stopped at different iterations
+
+
+class _Option:
+    def __init__(self, name, value):
+        self.name, self.value = name.encode(), value
+
+    def __enter__(self):
+        rw.load().rwig_set_option(self.name, float(self.value))
+
+    def __exit__(self, *exc):
+        rw.load().rwig_set_option(self.name, float("nan"))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 6, 7])
+def test_checkpointed_adjoint_is_bitwise_full_history(k):
+    """wdl.checkpoint = k keeps the forward state every k-th iteration and
+    recomputes the segments in the backward: the same gradient bits as the
+    full history (L = 7, so k = 2, 3 leave a short last segment)."""
+    reg, L = 0.1, 7
+    Y, C, K, A, W = _batch(230, 6, 5, 8, reg, salt=17)
+    full = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+    with _Option("wdl.checkpoint", k):
+        got = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        launches = rw.last_report()["kernel_launches"]
+    assert np.array_equal(got[0], full[0]) and np.array_equal(got[1], full[1])
+    ref_gA, ref_gl = oracle.wdl_batch_grad(A, W, Y, K, L)
+    assert rel_err(got[0], ref_gA) <= PARITY_TOL
+    assert launches > 0
+
+
+def test_checkpointed_training_matches_full_history():
+    N, M, S, B, E, L, reg = 120, 21, 4, 8, 2, 5, 0.1
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=6, salt=41)
+    full = rw.wdl_cpp(Y, C, reg, S, B, E, max_iter=L, zero_tol=1e-6, optimizer=1, eta=1e-2, Alpha0=A0, Lambda0=L0)
+    with _Option("wdl.checkpoint", 2):
+        got = rw.wdl_cpp(Y, C, reg, S, B, E, max_iter=L, zero_tol=1e-6, optimizer=1, eta=1e-2, Alpha0=A0,
+                         Lambda0=L0)
+    for k in ("A", "W", "Yhat"):
+        assert np.array_equal(got[k], full[k]), k
