@@ -257,3 +257,50 @@ def test_batched_log_barycenter_falls_back_per_problem():
         o = oracle.barycenter_log(q["A"], q["C"], q["w"], q["b_ext"], q["reg"], with_grad=True, max_iter=10,
                                   zero_tol=0.0)
         assert rel_err(got[i]["grad_A"], o["grad_A"]) <= PARITY_TOL
+
+
+def _bary2048():
+    import os
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "bary2048_oracle.npz"))
+    A, C, w, be = synth.barycenter_config(n=2048, S=32, dim=50)
+    return ref, A, C, w, be
+
+
+def test_full_size_against_oracle_fixture():
+    """The log-barycenter benchmark workload at full size (N = 2048, S = 32,
+    eps = 0.05, L = 50, with gradient) against the CPU oracle's solve
+    (tests/golden/bary2048_oracle.npz, made by tests/golden/make_fullsize.py)."""
+    ref, A, C, w, be = _bary2048()
+    got = rw.barycenter(A, C, w, be, {"reg": 0.05, "method": "log", "with_grad": True, "max_iter": 50,
+                                      "zero_tol": 0.0})
+    assert got["iter"] == int(ref["iter"]) == 50 and got["return_status"] == int(ref["return_status"])
+    for k in ("b", "grad_A", "grad_w"):
+        assert rel_err(got[k], ref[k]) <= PARITY_TOL, (k, rel_err(got[k], ref[k]))
+    sc = dual_scale(ref["F4"], ref["G4"])
+    assert rel_err(got["F"][::4], ref["F4"], sc) <= PARITY_TOL
+    assert rel_err(got["G"][::4], ref["G4"], sc) <= PARITY_TOL
+    assert abs(got["loss"] - float(ref["loss"])) <= PARITY_TOL * abs(float(ref["loss"]))
+    assert abs(got["err"] - float(ref["err"])) <= 1e-8 * abs(float(ref["err"]))
+
+
+def test_full_size_gradient_finite_differences():
+    """Central differences (h = 1e-6) of the full-size workload's objective
+    ||b - b_ext||^2 (normaliser held at its value, as the reference's backward
+    differentiates it) on 20 entries of A and every entry of w."""
+    _, A, C, w, be = _bary2048()
+    ctrl = {"reg": 0.05, "method": "log", "with_grad": True, "max_iter": 50, "zero_tol": 0.0}
+    r = rw.barycenter(A, C, w, be, ctrl)
+    Z0 = rw.last_report()["bary_norm"]
+    fctrl = dict(ctrl, with_grad=False)
+
+    def obj(A_, w_):
+        q = rw.barycenter(A_, C, w_, None, fctrl)
+        braw = q["b"] * rw.last_report()["bary_norm"] / Z0
+        return float((braw - be) @ (braw - be))
+
+    gw = _fd(lambda x: obj(A, x), w, range(w.size))
+    assert np.abs(gw - r["grad_w"]).max() <= 1e-6 * max(1.0, np.abs(gw).max()), np.abs(gw - r["grad_w"]).max()
+    g = np.random.default_rng(2)
+    idx = [k for k in g.choice(A.size, 200, replace=False) if A.flat[k] > 1e-3][:20]
+    gA = _fd(lambda X: obj(X, w), A, idx)
+    assert np.abs(gA - r["grad_A"].flat[idx]).max() <= 1e-6 * max(1.0, np.abs(gA).max())

@@ -90,3 +90,26 @@ def test_batch_equals_per_call_path():
     assert o["iter"] == r["iter"]
     sc = dual_scale(r["f"], r["g"])
     assert rel_err(o["f"], r["f"], sc) <= PARITY_TOL and rel_err(o["g"], r["g"], sc) <= PARITY_TOL
+
+
+def test_streamed_8192_against_oracle_fixture():
+    """One 8192 x 8192 request of the serving stream's kind through the batched
+    kernel, where its K (512 MB) is streamed from memory in strips every
+    iteration (it cannot stay in the shared memory of a team), alone and
+    beside small problems, against the CPU oracle's full solve
+    (tests/golden/sink8192_oracle.npz, made by tests/golden/make_fullsize.py)."""
+    import os
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "sink8192_oracle.npz"))
+    a, b, x, y = synth.stream_request_data(8192, 8192, 3, 777)
+    C = synth.sq_euclid_cost(x, y)
+    big = {"a": a, "b": b, "C": C, "reg": 0.05, "max_iter": 2000, "zero_tol": 1e-9}
+    alone = rw.batch_sinkhorn_log([big])[0]
+    mixed = rw.batch_sinkhorn_log([_problem(300, 200, 0.05, salt=1), big, _problem(64, 900, 0.1, salt=2)])[1]
+    for got in (alone, mixed):
+        assert got["path"] == 0
+        assert got["iter"] == int(ref["iter"]) and got["return_status"] == int(ref["return_status"])
+        sc = dual_scale(ref["f"], ref["g"])
+        assert rel_err(got["f"], ref["f"], sc) <= PARITY_TOL, rel_err(got["f"], ref["f"], sc)
+        assert rel_err(got["g"], ref["g"], sc) <= PARITY_TOL, rel_err(got["g"], ref["g"], sc)
+        assert abs(got["loss"] - float(ref["loss"])) <= PARITY_TOL * abs(float(ref["loss"]))
+    assert np.array_equal(alone["f"], mixed["f"]) and np.array_equal(alone["g"], mixed["g"])
