@@ -354,6 +354,20 @@ RWIG_API int rwig_selftest_dgemm(const double* K, long long ldk, int trans, int 
                                  const double* X, long long ldx, double* Y, long long ldy, int splits,
                                  void* stream);
 
+/* Self-check of the INT8 tensor-core GEMM behind the emulated FP64 products
+ * (no counterpart in the reference): D (M x N, column-major int32) = A B^T for
+ * A (M x Kd) and B (N x Kd) row-major int8 (values as signed char), Kd <=
+ * 65536; all device pointers. */
+RWIG_API int rwig_selftest_i8gemm(const signed char* A, const signed char* B, int M, int N, int Kd, int* D,
+                                  void* stream);
+
+/* Self-check of the FP64 product emulated on the INT8 tensor cores (no
+ * counterpart in the reference): Y (n x W, ldy) = op(K) X with op(K) = K
+ * (trans = 0) or K^T (trans = 1), K n x n (ldk), X n x W (ldx), n <= 8192;
+ * all device pointers.  Returns 0 or a negative error. */
+RWIG_API int rwig_selftest_ozaki(const double* K, long long ldk, int trans, int n, const double* X, long long ldx,
+                                 int W, double* Y, long long ldy, void* stream);
+
 /* Allocation-free log-Sinkhorn.  No counterpart in the reference: it exists for
  * callers that cannot let a library allocate device memory (a host framework
  * that owns the GPU's memory pool, a process under a hard device-memory quota,

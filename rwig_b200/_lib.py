@@ -114,6 +114,9 @@ SIGNATURES = {
     "rwig_selftest_exp": (_i, [_vp, _vp, _vp, _i, _vp]),
     "rwig_selftest_dgemm": (_i, [_vp, ctypes.c_longlong, _i, _i, _i, _i, _vp, ctypes.c_longlong, _vp,
                                  ctypes.c_longlong, _i, _vp]),
+    "rwig_selftest_i8gemm": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp]),
+    "rwig_selftest_ozaki": (_i, [_vp, ctypes.c_longlong, _i, _i, _vp, ctypes.c_longlong, _i, _vp, ctypes.c_longlong,
+                                 _vp]),
     "rwig_sinkhorn_log_noalloc": (_i, [_vp, _vp, _vp, _dp, _ip, _dp, _vp, _vp, _vp, _i, _i, _d, _i, _d, _vp]),
     "rwig_wdl": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _d, _i, _d, _i, _i, _i, _d, _d, _d, _d, _d, _i, _i,
                       _dp, _dp, _i]),

@@ -1,0 +1,626 @@
+// ozaki.cu -- the INT8 tensor-core half of the emulated FP64 products
+// (ozaki.cuh): reconstruction constants, scaling exponents, residues, and
+// the tcgen05 kind::i8 GEMM of the residue planes.
+//
+// GEMM kernel (one CTA per 128 x ntile output tile of one modulus, 128
+// threads):
+//   * operands are K-major int8 planes [T][rows][Kpad]; TMA (3-D tensor maps,
+//     128-byte swizzle) copies 128 x 128-byte A tiles and ntile x 128-byte B
+//     tiles into a 4-stage shared-memory ring, full / empty mbarriers;
+//   * thread 0 issues the copies, thread 32 the MMAs: per stage four
+//     tcgen05.mma.cta_group::1.kind::i8 of K = 32 (the shared-memory
+//     descriptors advanced by 32 bytes inside the swizzle atom) into an int32
+//     accumulator in tensor memory, then tcgen05.commit frees the stage;
+//   * the four warps read the accumulator back (tcgen05.ld 32x32b, warp w
+//     owns lanes 32w..32w+31 = rows), reduce it modulo p_t and store one byte
+//     per entry.
+// Every wait is bounded (2 s): a wait that runs out sets the error word and
+// the kernel winds down (the MMA thread still commits what it issued, the
+// tensor memory is freed), and the host reports RWIG_E_TIMEOUT.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+#include "ozaki.cuh"
+
+namespace rwig {
+namespace oz {
+
+// ---------------------------------------------------------------------------
+// reconstruction constants (host, little-endian 32-bit limbs)
+// ---------------------------------------------------------------------------
+namespace {
+
+using Big = std::vector<uint32_t>;
+
+void trim(Big& a) {
+  while (a.size() > 1 && a.back() == 0) a.pop_back();
+}
+Big mul_small(const Big& a, uint32_t m) {
+  Big r(a.size() + 1, 0);
+  uint64_t carry = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    const uint64_t v = (uint64_t)a[i] * m + carry;
+    r[i] = (uint32_t)v;
+    carry = v >> 32;
+  }
+  r[a.size()] = (uint32_t)carry;
+  trim(r);
+  return r;
+}
+Big div_small(const Big& a, uint32_t d) {
+  Big r(a.size(), 0);
+  uint64_t rem = 0;
+  for (size_t i = a.size(); i-- > 0;) {
+    const uint64_t cur = (rem << 32) | a[i];
+    r[i] = (uint32_t)(cur / d);
+    rem = cur % d;
+  }
+  trim(r);
+  return r;
+}
+uint32_t mod_small(const Big& a, uint32_t d) {
+  uint64_t rem = 0;
+  for (size_t i = a.size(); i-- > 0;) rem = ((rem << 32) | a[i]) % d;
+  return (uint32_t)rem;
+}
+int cmp(const Big& a, const Big& b) {
+  if (a.size() != b.size()) return a.size() < b.size() ? -1 : 1;
+  for (size_t i = a.size(); i-- > 0;)
+    if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+  return 0;
+}
+void sub_in(Big& a, const Big& b) {  // a -= b, a >= b
+  int64_t borrow = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    int64_t v = (int64_t)a[i] - borrow - (i < b.size() ? (int64_t)b[i] : 0);
+    borrow = v < 0;
+    if (v < 0) v += (int64_t)1 << 32;
+    a[i] = (uint32_t)v;
+  }
+  trim(a);
+}
+void shl1(Big& a) {
+  uint32_t carry = 0;
+  for (uint32_t& x : a) {
+    const uint32_t nc = x >> 31;
+    x = (x << 1) | carry;
+    carry = nc;
+  }
+  if (carry) a.push_back(carry);
+}
+
+Crt make_crt() {
+  // the 24 largest pairwise coprime integers up to 256
+  static const int mods[kT] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211,
+                               199, 197, 193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
+  Crt c{};
+  Big P{1};
+  for (int t = 0; t < kT; ++t) P = mul_small(P, (uint32_t)mods[t]);
+  double Pd = 0.0;
+  for (size_t i = P.size(); i-- > 0;) Pd = Pd * 4294967296.0 + (double)P[i];
+  c.P = Pd;
+  for (int t = 0; t < kT; ++t) {
+    const uint32_t p = (uint32_t)mods[t];
+    c.p[t] = (int)p;
+    c.invp[t] = 1.0 / (double)p;
+    const Big Mt = div_small(P, p);
+    const uint32_t mt = mod_small(Mt, p);
+    uint32_t inv = 0;
+    for (uint32_t x = 1; x < p; ++x)
+      if ((uint64_t)mt * x % p == 1) {
+        inv = x;
+        break;
+      }
+    Big e = mul_small(Mt, inv);  // e_t = M_t (M_t^-1 mod p_t) < P
+    // F_t = floor(2^256 e_t / P): 256 fraction bits by long division
+    unsigned long long F[4] = {0, 0, 0, 0};
+    for (int k = 255; k >= 0; --k) {
+      shl1(e);
+      if (cmp(e, P) >= 0) {
+        sub_in(e, P);
+        F[k / 64] |= 1ull << (k % 64);
+      }
+    }
+    for (int l = 0; l < 4; ++l) c.F[t][l] = F[l];
+  }
+  return c;
+}
+
+}  // namespace
+
+const Crt& crt_constants() {
+  static const Crt c = make_crt();
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// scaling exponents and residues
+// ---------------------------------------------------------------------------
+struct Mods {
+  int p[kT];
+  double invp[kT];
+};
+
+Mods mods_of(const Crt& c) {
+  Mods m;
+  for (int t = 0; t < kT; ++t) {
+    m.p[t] = c.p[t];
+    m.invp[t] = c.invp[t];
+  }
+  return m;
+}
+
+__device__ __forceinline__ int scale_exp(double mx) { return mx > 0.0 ? kQ - 1 - ilogb(mx) : 0; }
+
+// v mod p for an integer-valued double 0 <= v < 2^53, exactly.
+__device__ __forceinline__ int mod_exact(double v, int p, double invp) {
+  const double q = floor(v * invp);
+  int r = (int)fma(-q, (double)p, v);
+  if (r < 0) r += p;
+  if (r >= p) r -= p;
+  return r;
+}
+
+constexpr int kPw = 64;  // 2^s mod p_t for s < kPw (the scaled shift is at most kQ - 53)
+
+__device__ void load_pow2(int* pw, const Mods& m) {
+  for (int t = threadIdx.x + blockDim.x * threadIdx.y; t < kT; t += blockDim.x * blockDim.y) {
+    int v = 1 % m.p[t];
+    for (int s = 0; s < kPw; ++s) {
+      pw[t * kPw + s] = v;
+      v = (v * 2) % m.p[t];
+    }
+  }
+}
+
+// Symmetric residues of trunc(x 2^sc) for every modulus into out[t * plane].
+__device__ __forceinline__ void residues(double x, int sc, const int* pw, const Mods& m, int8_t* out, size_t plane) {
+  if (!(x != 0.0)) {
+#pragma unroll 4
+    for (int t = 0; t < kT; ++t) out[t * plane] = 0;
+    return;
+  }
+  const double ax = fabs(x);
+  const int e = ilogb(ax);
+  const double mant = ldexp(ax, 52 - e);  // integer in [2^52, 2^53)
+  const int sh = e - 52 + sc;             // trunc(|x| 2^sc) = mant 2^sh
+  const double base = sh >= 0 ? mant : (sh > -64 ? trunc(ldexp(mant, sh)) : 0.0);
+  const int s = sh >= 0 ? min(sh, kPw - 1) : 0;
+#pragma unroll 4
+  for (int t = 0; t < kT; ++t) {
+    const int p = m.p[t];
+    int r = mod_exact(base, p, m.invp[t]);
+    if (s) r = (r * pw[t * kPw + s]) % p;
+    if (x < 0.0 && r) r = p - r;
+    out[t * plane] = (int8_t)(r > (p - 1) / 2 ? r - p : r);
+  }
+}
+
+// alpha[i] from max_k |K[i + k ldk]| (rows of K), one thread per row.
+__global__ void exp_rows(const double* K, long long ldk, int n, int* alpha) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double mx = 0.0;
+    for (int k = 0; k < n; ++k) mx = fmax(mx, fabs(K[i + (long long)k * ldk]));
+    alpha[i] = scale_exp(mx);
+  }
+}
+
+// e[j] from max_k |X[k + j ldx]| (columns), one block per column.
+__global__ void exp_cols(const double* X, long long ldx, int Kd, int* e) {
+  __shared__ double sh[256];
+  const int j = blockIdx.x;
+  double mx = 0.0;
+  for (int k = threadIdx.x; k < Kd; k += blockDim.x) mx = fmax(mx, fabs(X[k + (long long)j * ldx]));
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) e[j] = scale_exp(sh[0]);
+}
+
+// Row r of the operand is column r of src (A(r, k) = src[k + r ld]):
+// out[t][r][k] for r < rows_pad, k < Kpad (zero outside rows x Kd).
+__global__ void res_cols(const double* src, long long ld, int Kd, int rows, const int* ex, int Kpad, int rows_pad,
+                         Mods m, int8_t* out) {
+  __shared__ int pw[kT * kPw];
+  load_pow2(pw, m);
+  __syncthreads();
+  const int r = blockIdx.y;
+  const size_t plane = (size_t)rows_pad * Kpad;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Kpad; k += gridDim.x * blockDim.x) {
+    const double x = (r < rows && k < Kd) ? src[k + (long long)r * ld] : 0.0;
+    residues(x, r < rows ? ex[r] : 0, pw, m, out + (size_t)r * Kpad + k, plane);
+  }
+}
+
+// Row i of the operand is row i of K (A(i, k) = K[i + k ldk]): 32 x 32 tiles
+// transposed through shared memory, out[t][i][k].
+__global__ void res_rows(const double* K, long long ldk, int n, const int* alpha, int Kpad, int Mpad, Mods m,
+                         int8_t* out) {
+  __shared__ int pw[kT * kPw];
+  __shared__ double tile[32][33];
+  load_pow2(pw, m);
+  const int i0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + threadIdx.x, k = k0 + r;
+    tile[r][threadIdx.x] = (i < n && k < n) ? K[i + (long long)k * ldk] : 0.0;
+  }
+  __syncthreads();
+  const size_t plane = (size_t)Mpad * Kpad;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, k = k0 + threadIdx.x;
+    if (i < Mpad && k < Kpad) residues(tile[threadIdx.x][r], i < n ? alpha[i] : 0, pw, m, out + (size_t)i * Kpad + k, plane);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the tcgen05 INT8 GEMM
+// ---------------------------------------------------------------------------
+constexpr int kStages = 4;
+constexpr int kAStage = kTileM * kBk;  // 16 KB
+constexpr int kBStage = 256 * kBk;     // room for ntile <= 256: 32 KB
+constexpr size_t kGemmSmem = 1024 + (size_t)kStages * (kAStage + kBStage) + 256;
+
+struct I8Args {
+  int Mpad, Wpad, Kpad, ntile, nk;
+  uint8_t* cres;  // residue planes [T][Wpad][Mpad]
+  int* raw;       // RAW: the int32 product [Wpad][Mpad]
+  unsigned* err;
+  Mods m;
+};
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile in the 128-byte swizzle
+// layout: start address >> 4, leading byte offset 16 (unused by this
+// layout), stride byte offset 1024 (eight 128-byte rows), descriptor version
+// 1, base offset 0 (tiles are 1024-byte aligned), layout type 2 (128B).
+__device__ __forceinline__ uint64_t sw128_desc(const void* p) {
+  const uint32_t a = smem_u32(p);
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor of kind::i8: int32 accumulator, signed A and B,
+// both K-major, N = ntile, M = 128.
+__host__ __device__ constexpr uint32_t i8_idesc(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u; }
+
+template <bool RAW>
+__global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtensorMap ta,
+                                                  const __grid_constant__ CUtensorMap tb, I8Args g) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = base;
+  uint8_t* sB = base + (size_t)kStages * kAStage;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sB + (size_t)kStages * kBStage);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * g.ntile, m0 = blockIdx.y * kTileM, z = blockIdx.z;
+  const uint32_t ncols = tmem_cols(g.ntile);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t stage_bytes = (uint32_t)(kAStage + g.ntile * kBk);
+
+  if (warp == 0 && lane == 0) {  // copies
+    int issued = 0;
+    for (int kb = 0; kb < g.nk; ++kb) {
+      const int s = kb % kStages;
+      if (kb >= kStages && !mbar_wait_bounded(empty + s, ((kb / kStages) - 1) & 1)) {
+        atomicOr(g.err, KERR_MBAR_TIMEOUT);
+        break;
+      }
+      mbar_arrive_expect_tx(full + s, stage_bytes);
+      tma_load_3d(sA + (size_t)s * kAStage, &ta, kb * kBk, m0, z, full + s);
+      tma_load_3d(sB + (size_t)s * kBStage, &tb, kb * kBk, n0, z, full + s);
+      ++issued;
+    }
+    // copies still in flight when the loop stopped early complete before exit
+    for (int kb = std::max(0, issued - kStages); kb < issued; ++kb)
+      if (issued < g.nk && !mbar_wait_bounded(full + kb % kStages, (kb / kStages) & 1)) atomicOr(g.err, KERR_MBAR_TIMEOUT);
+  } else if (warp == 1 && lane == 0) {  // MMAs
+    const uint32_t idesc = i8_idesc(g.ntile);
+    for (int kb = 0; kb < g.nk; ++kb) {
+      const int s = kb % kStages;
+      if (!mbar_wait_bounded(full + s, (kb / kStages) & 1)) {
+        atomicOr(g.err, KERR_MBAR_TIMEOUT);
+        break;
+      }
+      tc_fence_after();
+      const uint8_t* a = sA + (size_t)s * kAStage;
+      const uint8_t* b = sB + (size_t)s * kBStage;
+#pragma unroll
+      for (int kk = 0; kk < kBk / 32; ++kk)
+        tc_mma(tmem, sw128_desc(a + kk * 32), sw128_desc(b + kk * 32), idesc, (kb | kk) != 0);
+      tc_commit(empty + s);  // the stage is free once these MMAs have read it
+    }
+    tc_commit(done);  // everything issued has completed
+  }
+  __syncwarp();
+
+  const bool have = mbar_wait_bounded(done, 0);
+  tc_fence_after();
+  if (!have) {
+    if (threadIdx.x == 0) atomicOr(g.err, KERR_MBAR_TIMEOUT);
+  } else if ((*(volatile unsigned*)g.err & KERR_MBAR_TIMEOUT) == 0) {
+    const int i = m0 + warp * 32 + lane;  // accumulator lane = output row
+    const int p = RAW ? 1 : g.m.p[z];
+    const double invp = RAW ? 1.0 : g.m.invp[z];
+    for (int c = 0; c < g.ntile; c += 32) {
+      uint32_t v[32];
+      tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        if (c + q >= g.ntile) break;  // columns of the last load beyond the tile
+        const int j = n0 + c + q;
+        const int d = (int)v[q];
+        if (RAW) {
+          g.raw[(size_t)j * g.Mpad + i] = d;
+        } else {
+          int r = d - (int)floor((double)d * invp) * p;
+          if (r < 0) r += p;
+          if (r >= p) r -= p;
+          g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)r;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    (void)cudaGetLastError();
+  }
+  return fn;
+}
+
+// 3-D map over int8 planes [planes][rows][Kpad], boxes of 128 bytes x box_rows x 1.
+int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(RWIG_E_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[3] = {(cuuint64_t)Kpad, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)Kpad, (cuuint64_t)Kpad * (cuuint64_t)rows};
+  const cuuint32_t box[3] = {(cuuint32_t)kBk, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(RWIG_E_CUDA, "cuTensorMapEncodeTiled failed");
+  return 0;
+}
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+int pick_ntile(int W) { return std::min(256, round_up(std::max(W, 16), 16)); }
+
+enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_BRES, SO_BETA, SO_CRES, SO_ERR, SO_TA, SO_TB, SO_TD };
+
+// The kT (or, RAW, one) planes of A (Mpad x Kpad) and B (Wpad x Kpad): the
+// int8 products into cres (or raw).
+template <bool RAW>
+int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad, int Kpad, int ntile, int planes,
+              uint8_t* cres, int* raw, cudaStream_t st) {
+  CUtensorMap ta, tb;
+  if (int rc = make_map(&ta, A, Kpad, Mpad, planes, kTileM)) return rc;
+  if (int rc = make_map(&tb, B, Kpad, Wpad, planes, ntile)) return rc;
+  unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);
+  if (!err) return RWIG_E_NOMEM;
+  RWIG_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), st));
+  I8Args g{};
+  g.Mpad = Mpad;
+  g.Wpad = Wpad;
+  g.Kpad = Kpad;
+  g.ntile = ntile;
+  g.nk = Kpad / kBk;
+  g.cres = cres;
+  g.raw = raw;
+  g.err = err;
+  g.m = mods_of(crt_constants());
+  static bool attr = false;
+  if (!attr) {
+    RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    attr = true;
+  }
+  const dim3 grid(Wpad / ntile, Mpad / kTileM, planes);
+  i8_gemm<RAW><<<grid, 128, kGemmSmem, st>>>(ta, tb, g);
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int check_err(Context* ctx, cudaStream_t st) {
+  unsigned h = 0;
+  unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);
+  RWIG_CUDA_TRY(cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) return set_error(RWIG_E_TIMEOUT, "INT8 tensor-core GEMM: a bounded wait ran out");
+  return 0;
+}
+
+}  // namespace
+
+bool available(Context* ctx) { return ctx && ctx->smem_optin >= (int)kGemmSmem && encode_fn() != nullptr; }
+
+int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches) {
+  if (n < 1 || n > kMaxKd) return set_error(RWIG_E_UNSUPPORTED, "INT8 product path: size above 8192");
+  if (!available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 product path unavailable on this device");
+  pr->K = K;
+  pr->ldk = ldk;
+  pr->Mo = pr->Kd = n;
+  pr->Mpad = round_up(n, kTileM);
+  pr->Kpad = round_up(n, kBk);
+  const size_t planes = (size_t)kT * pr->Mpad * pr->Kpad;
+  const Mods m = mods_of(crt_constants());
+  for (int tr = 0; tr < 2; ++tr) {
+    pr->ares[tr] = (int8_t*)scratch(ctx, SO_ARES0 + tr, planes);
+    pr->alpha[tr] = (int*)scratch(ctx, SO_ALPHA0 + tr, sizeof(int) * n);
+    if (!pr->ares[tr] || !pr->alpha[tr]) return RWIG_E_NOMEM;
+  }
+  // trans = 0: rows of K
+  exp_rows<<<std::max(1, (n + 255) / 256), 256, 0, st>>>(K, ldk, n, pr->alpha[0]);
+  res_rows<<<dim3(pr->Kpad / 32, pr->Mpad / 32), dim3(32, 8), 0, st>>>(K, ldk, n, pr->alpha[0], pr->Kpad, pr->Mpad, m,
+                                                                        pr->ares[0]);
+  // trans = 1: columns of K
+  exp_cols<<<n, 256, 0, st>>>(K, ldk, n, pr->alpha[1]);
+  res_cols<<<dim3((pr->Kpad + 255) / 256, pr->Mpad), 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m,
+                                                                    pr->ares[1]);
+  if (launches) *launches += 4;
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int products(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, cudaStream_t st,
+             const uint8_t** cres, const int** beta, int* Wpad_out, int* launches) {
+  if (W < 1 || !X) return set_error(RWIG_E_INVALID, "INT8 product path: empty operand");
+  const int ntile = pick_ntile(W);
+  const int Wpad = round_up(W, ntile);
+  int8_t* bres = (int8_t*)scratch(ctx, SO_BRES, (size_t)kT * Wpad * pr.Kpad);
+  int* be = (int*)scratch(ctx, SO_BETA, sizeof(int) * W);
+  uint8_t* cr = (uint8_t*)scratch(ctx, SO_CRES, (size_t)kT * Wpad * pr.Mpad);
+  if (!bres || !be || !cr) return RWIG_E_NOMEM;
+  const Mods m = mods_of(crt_constants());
+  exp_cols<<<W, 256, 0, st>>>(X, ldx, pr.Kd, be);
+  res_cols<<<dim3((pr.Kpad + 255) / 256, Wpad), 256, 0, st>>>(X, ldx, pr.Kd, W, be, pr.Kpad, Wpad, m, bres);
+  if (int rc = launch_i8<false>(ctx, pr.ares[trans], pr.Mpad, bres, Wpad, pr.Kpad, ntile, kT, cr, nullptr, st)) return rc;
+  if (launches) *launches += 3;
+  *cres = cr;
+  *beta = be;
+  *Wpad_out = Wpad;
+  return 0;
+}
+
+// Bounded-wait status of the last products() launches (a host read).
+int status(Context* ctx, cudaStream_t st) { return check_err(ctx, st); }
+
+}  // namespace oz
+}  // namespace rwig
+
+using namespace rwig;
+
+// Self-check of the INT8 tensor-core GEMM (no counterpart in the reference):
+// D (M x N, column-major, int32) = A B^T for A (M x Kd) and B (N x Kd) int8,
+// both row-major (K-major); all device pointers.
+extern "C" int rwig_selftest_i8gemm(const signed char* A, const signed char* B, int M, int N, int Kd, int* D,
+                                    void* stream) {
+  if (!A || !B || !D || M < 1 || N < 1 || Kd < 1 || Kd > (1 << 16))
+    return set_error(RWIG_E_INVALID, "bad INT8 GEMM arguments");
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!oz::available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 tensor-core GEMM unavailable");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const int ntile = oz::pick_ntile(N), Mpad = oz::round_up(M, oz::kTileM), Npad = oz::round_up(N, ntile);
+  const int Kpad = oz::round_up(Kd, oz::kBk);
+  int8_t* a = (int8_t*)scratch(ctx, oz::SO_TA, (size_t)Mpad * Kpad);
+  int8_t* b = (int8_t*)scratch(ctx, oz::SO_TB, (size_t)Npad * Kpad);
+  int* d = (int*)scratch(ctx, oz::SO_TD, sizeof(int) * (size_t)Mpad * Npad);
+  if (!a || !b || !d) return RWIG_E_NOMEM;
+  RWIG_CUDA_TRY(cudaMemsetAsync(a, 0, (size_t)Mpad * Kpad, st));
+  RWIG_CUDA_TRY(cudaMemsetAsync(b, 0, (size_t)Npad * Kpad, st));
+  RWIG_CUDA_TRY(cudaMemcpy2DAsync(a, Kpad, A, Kd, Kd, M, cudaMemcpyDeviceToDevice, st));
+  RWIG_CUDA_TRY(cudaMemcpy2DAsync(b, Kpad, B, Kd, Kd, N, cudaMemcpyDeviceToDevice, st));
+  if (int rc = oz::launch_i8<true>(ctx, a, Mpad, b, Npad, Kpad, ntile, 1, nullptr, d, st)) return rc;
+  RWIG_CUDA_TRY(cudaMemcpy2DAsync(D, sizeof(int) * M, d, sizeof(int) * Mpad, sizeof(int) * M, N,
+                                  cudaMemcpyDeviceToDevice, st));
+  return oz::check_err(ctx, st);
+}
+
+// Self-check of the emulated FP64 product (no counterpart in the reference):
+// Y (n x W, ldy) = op(K) X, op(K) = K (trans = 0) or K^T (trans = 1), K
+// n x n (ldk), X n x W (ldx); all device pointers.
+extern "C" int rwig_selftest_ozaki(const double* K, long long ldk, int trans, int n, const double* X, long long ldx,
+                                   int W, double* Y, long long ldy, void* stream) {
+  if (!K || !X || !Y || n < 1 || W < 1 || (trans != 0 && trans != 1) || ldk < n || ldx < n || ldy < n)
+    return set_error(RWIG_E_INVALID, "bad emulated-product arguments");
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  oz::Prepared pr;
+  int launches = 0;
+  if (int rc = oz::prepare(ctx, K, ldk, n, &pr, st, &launches)) return rc;
+  if (int rc = oz::gemm(ctx, pr, trans, X, ldx, W, oz::kCrtCols, dg::EpiStore{Y, ldy, W}, st, &launches)) return rc;
+  return oz::status(ctx, st);
+}

@@ -1,0 +1,168 @@
+// ozaki.cuh -- FP64 matrix products op(K) X on the INT8 tensor cores
+// (tcgen05 kind::i8), exact integer products recombined by the Chinese
+// remainder theorem: the scheme of Y. Uchino, K. Ozaki and T. Imamura,
+// "Performance enhancement of the Ozaki Scheme on integer matrix
+// multiplication unit" (Ozaki scheme II, 2024/2025), written here for the
+// skinny products of the WDL step.
+//
+//   1. Scaling.  Row i of A = op(K) is scaled by 2^alpha_i and column j of X
+//      by 2^beta_j (powers of two: exact) so that the largest magnitude of the
+//      row / column is just below 2^q; truncation toward zero gives integer
+//      matrices Ah, Xh with |entries| < 2^q (an entry loses bits only where it
+//      is below 2^(53-q) of its row's / column's largest).
+//   2. Residues.  For T pairwise coprime moduli p_t <= 256 the symmetric
+//      residues Ah mod p_t, Xh mod p_t fit in int8.
+//   3. Products.  D_t = (Ah mod p_t)(Xh mod p_t) is exact in the tensor
+//      cores' int32 accumulators (|D_t| <= Kd 2^14 < 2^31 for Kd <= 2^16);
+//      c_t = D_t mod p_t in [0, p_t) (ozaki.cu).
+//   4. Reconstruction.  With P = prod p_t, M_t = P / p_t and e_t = M_t
+//      (M_t^-1 mod p_t), Ch = Ah Xh is the representative in (-P/2, P/2) of
+//      sum_t c_t e_t mod P.  Here frac(sum_t c_t e_t / P) is accumulated in
+//      256-bit fixed point from F_t = floor(2^256 e_t / P) (the mod-1
+//      reduction is the fixed point's overflow), read as a signed fraction s,
+//      and Ch = s P; the result is 2^-(alpha_i + beta_j) Ch, rounded once.
+//      Sizes keep Kd 2^(2q) < P / 2, so Ch is the exact integer product.
+//
+// With T = 24 moduli (log2 P = 184.09) and q = 85 the product is exact for
+// the truncated inputs; the only errors are the truncation of entries far
+// below their row's / column's maximum (relative 2^-85 of that maximum) and
+// the final rounding.  The reconstruction kernel hands each output tile to
+// the same epilogue functors as the DMMA GEMM (dgemm.cuh contract).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dgemm.cuh"
+#include "engine.h"
+
+namespace rwig {
+namespace oz {
+
+constexpr int kT = 24;        // moduli
+constexpr int kQ = 85;        // bits of the scaled integers
+constexpr int kMaxKd = 8192;  // contraction length for which kQ is safe: Kd 2^(2 kQ) < P / 2
+constexpr int kTileM = 128;   // UMMA M
+constexpr int kBk = 128;      // bytes of K per pipeline stage (one 128-byte swizzle atom)
+constexpr int kCrtRows = 64;  // rows per reconstruction tile
+constexpr int kCrtCols = 64;  // most columns per reconstruction tile (the DMMA GEMM's widest tile)
+constexpr int kCrtThreads = 256;
+
+// Reconstruction constants, passed by value to the kernels.
+struct Crt {
+  int p[kT];
+  double invp[kT];
+  unsigned long long F[kT][4];  // floor(2^256 e_t / P), little-endian 64-bit limbs
+  double P;                     // P rounded to double
+};
+
+// Host: the moduli and reconstruction constants (computed once).
+const Crt& crt_constants();
+
+// op(K) as the tensor cores' A operand: residues [kT][Mpad][Kpad] (K-major
+// int8) and the row exponents alpha (Mo ints), for trans = 0 (K, rows of K)
+// and trans = 1 (K^T, columns of K).
+struct Prepared {
+  const double* K = nullptr;
+  long long ldk = 0;
+  int Mo = 0, Kd = 0, Mpad = 0, Kpad = 0;
+  int8_t* ares[2] = {nullptr, nullptr};
+  int* alpha[2] = {nullptr, nullptr};
+};
+
+// Residues and exponents of op(K) for trans = 0 and 1 (square K: Mo = Kd),
+// into engine scratch slots.  Returns 0 or an engine error.
+int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches);
+
+// X's residues and the kT integer products: cres[t][j][i] = (A_t X_t)_ij mod
+// p_t for i < Mo, j < W (pitch Mpad per column, Wpad columns per modulus),
+// beta (W ints).  Returns 0 or an engine error.
+int products(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, cudaStream_t st,
+             const uint8_t** cres, const int** beta, int* Wpad, int* launches);
+
+// Status of the bounded waits of the INT8 GEMMs enqueued so far on `st`
+// (synchronises): 0 or RWIG_E_TIMEOUT.
+int status(Context* ctx, cudaStream_t st);
+
+// Whether the INT8 tensor-core path can run: sm_100 class device with the
+// driver's tensor-map entry point.
+bool available(Context* ctx);
+
+// Reconstruction of one kCrtRows x tc output tile, then the epilogue.
+template <class Epi>
+__global__ void __launch_bounds__(kCrtThreads) crt_kernel(Crt c, const uint8_t* __restrict__ cres, int Mpad, int Wpad,
+                                                          const int* __restrict__ alpha, const int* __restrict__ beta,
+                                                          int Mo, int W, int tc, Epi epi) {
+  extern __shared__ double sm[];
+  constexpr int ldt = kCrtRows + 1;
+  double* tile = sm;                            // [tc][ldt]
+  double* ws = sm + (size_t)kCrtCols * ldt;      // 2 (BN + 1) ldt doubles
+  const int r0 = blockIdx.x * kCrtRows, c0 = blockIdx.y * tc;
+  const int nr = min(kCrtRows, Mo - r0);
+  const size_t plane = (size_t)Wpad * Mpad;
+  for (int e = threadIdx.x; e < kCrtRows * tc; e += blockDim.x) {
+    const int r = e % kCrtRows, cc = e / kCrtRows, i = r0 + r, j = c0 + cc;
+    double v = 0.0;
+    if (r < nr && j < W) {
+      const uint8_t* q = cres + (size_t)j * Mpad + i;
+      unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll 4
+      for (int t = 0; t < kT; ++t) {
+        const unsigned long long ct = q[(size_t)t * plane];
+        unsigned __int128 x = (unsigned __int128)ct * c.F[t][0] + a0;
+        a0 = (unsigned long long)x;
+        x = (unsigned __int128)ct * c.F[t][1] + a1 + (unsigned long long)(x >> 64);
+        a1 = (unsigned long long)x;
+        x = (unsigned __int128)ct * c.F[t][2] + a2 + (unsigned long long)(x >> 64);
+        a2 = (unsigned long long)x;
+        a3 = a3 + ct * c.F[t][3] + (unsigned long long)(x >> 64);
+      }
+      // frac(sum / P) as a signed fraction in [-1/2, 1/2)
+      const bool neg = (a3 >> 63) != 0;
+      if (neg) {  // two's complement negation of the 256-bit value
+        a0 = ~a0;
+        a1 = ~a1;
+        a2 = ~a2;
+        a3 = ~a3;
+        if (++a0 == 0 && ++a1 == 0 && ++a2 == 0) ++a3;
+      }
+      const double mag = ldexp((double)a3, -64) + ldexp((double)a2, -128) + ldexp((double)a1, -192);
+      const double ch = mag * c.P;  // |Ah Xh|_ij
+      v = ldexp(neg ? -ch : ch, -(alpha[i] + beta[j]));
+    }
+    tile[cc * ldt + r] = v;
+  }
+  __syncthreads();
+  epi(r0, nr, c0, tc, tile, ldt, ws);
+}
+
+inline size_t crt_smem_bytes() { return sizeof(double) * (size_t)(kCrtCols + 2 * (kCrtCols + 1)) * (kCrtRows + 1); }
+
+// Y = op(K) X through the INT8 tensor cores, each output tile handed to
+// `epi` (the dgemm.cuh epilogue contract, tiles of kCrtRows rows and tc
+// columns).  *launches += the kernels launched.
+template <class Epi>
+int gemm(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, int tc, const Epi& epi,
+         cudaStream_t st, int* launches) {
+  const uint8_t* cres = nullptr;
+  const int* beta = nullptr;
+  int Wpad = 0;
+  if (int rc = products(ctx, pr, trans, X, ldx, W, st, &cres, &beta, &Wpad, launches)) return rc;
+  if (tc <= 0 || tc > kCrtCols) tc = kCrtCols;
+  static bool attr = false;  // once per instantiation (callers hold the context lock)
+  const size_t smem = crt_smem_bytes();
+  if (!attr) {
+    RWIG_CUDA_TRY(cudaFuncSetAttribute(crt_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  const dim3 grid((pr.Mo + kCrtRows - 1) / kCrtRows, (W + tc - 1) / tc);
+  crt_kernel<Epi><<<grid, kCrtThreads, smem, st>>>(crt_constants(), cres, pr.Mpad, Wpad, pr.alpha[trans], beta,
+                                                    pr.Mo, W, tc, epi);
+  if (launches) ++*launches;
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace oz
+}  // namespace rwig

@@ -1,0 +1,66 @@
+"""FP64 products emulated on the INT8 tensor cores (ozaki.cu / ozaki.cuh).
+
+* The tcgen05 kind::i8 GEMM itself (rwig_selftest_i8gemm) is exact: its
+  int32 products equal numpy's int64 products bit for bit, on tile-aligned
+  and ragged shapes.
+* The emulated FP64 product (rwig_selftest_ozaki: scaling, 24 residue planes,
+  CRT reconstruction) agrees with an exactly rounded reference computed in
+  extended precision (numpy longdouble sums of the FP64 products) to a few
+  ulp, for K and K^T, positive and mixed-sign operands, wide dynamic range."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from rwig_b200 import _lib, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("M,N,Kd", [(128, 16, 128), (256, 256, 512), (200, 40, 300), (1000, 300, 5000),
+                                    (5000, 1024, 256), (130, 257, 129)])
+def test_int8_gemm_is_exact(M, N, Kd):
+    import torch
+    g = np.random.default_rng(M + N + Kd)
+    A = g.integers(-128, 128, size=(M, Kd), dtype=np.int8)
+    B = g.integers(-128, 128, size=(N, Kd), dtype=np.int8)
+    d = torch.device("cuda:0")
+    tA, tB = torch.from_numpy(A).to(d), torch.from_numpy(B).to(d)
+    tD = torch.zeros((N, M), dtype=torch.int32, device=d)
+    _lib.check(_lib.load().rwig_selftest_i8gemm(_vp(tA), _vp(tB), M, N, Kd, _vp(tD), None))
+    ref = A.astype(np.int64) @ B.astype(np.int64).T
+    assert np.array_equal(tD.cpu().numpy().T.astype(np.int64), ref)
+
+
+def _exact(K, X):
+    """K X with every product and sum in extended precision, then rounded."""
+    return (K.astype(np.longdouble) @ X.astype(np.longdouble)).astype(np.float64)
+
+
+@pytest.mark.parametrize("n,W,trans,signed", [(500, 64, 0, False), (500, 64, 1, False), (777, 40, 0, True),
+                                              (2048, 300, 1, True), (5000, 1024, 0, False)])
+def test_emulated_fp64_product(n, W, trans, signed):
+    import torch
+    g = np.random.default_rng(n + W)
+    x = g.standard_normal((n, 16))
+    C = synth.sq_euclid_cost(x, x)
+    K = np.asfortranarray(np.exp(-C / 0.05))  # entries from 1 down to e^-20
+    X = np.asfortranarray(np.exp(g.uniform(-8, 8, size=(n, W))))  # column dynamic range e^16
+    if signed:
+        X *= np.where(g.random((n, W)) < 0.5, -1.0, 1.0)
+    d = torch.device("cuda:0")
+    tK = torch.from_numpy(np.ascontiguousarray(K.T)).to(d)
+    tX = torch.from_numpy(np.ascontiguousarray(X.T)).to(d)
+    tY = torch.zeros((W, n), dtype=torch.float64, device=d)
+    _lib.check(_lib.load().rwig_selftest_ozaki(_vp(tK), n, trans, n, _vp(tX), n, W, _vp(tY), n, None))
+    Y = tY.cpu().numpy().T
+    op = K.T if trans else K
+    ref = _exact(op, X) if n <= 800 else op @ X
+    err = np.abs(Y - ref) / (np.abs(op) @ np.abs(X))  # relative to the FP64 GEMM error scale sum |K||X|
+    assert err.max() <= 1e-14, err.max()
+    if not signed:  # positive operands: no cancellation, relative to each entry
+        assert (np.abs(Y - ref) / np.abs(ref)).max() <= 1e-13
