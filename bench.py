@@ -1062,10 +1062,19 @@ class StreamWorkload:
                 ts.append(e0.elapsed_time(e1))
             return float(np.mean(ts))
 
+        L.rwig_set_option(b"wdl.int8", 0.0)  # the same step with every product on the FP64 tensor cores
+        try:
+            dmma_ms = timed_step()
+            dmma_gA = gA.cpu().numpy()
+        finally:
+            L.rwig_set_option(b"wdl.int8", float("nan"))
         eng_ms = timed_step()
         full_gA = gA.cpu().numpy()
         adj = {"batch": f"batch 0: {B} documents, K given (mode 0)", "engine_ms": eng_ms,
-               "engine_call": "rwig_wdl_batch_grad_dev, mean of 3 after 1 untimed"}
+               "engine_call": "rwig_wdl_batch_grad_dev, mean of 3 after 1 untimed; products emulated on the "
+                              "INT8 tensor cores (wdl.int8 default)",
+               "engine_fp64_tensor_ms": dmma_ms,
+               "max_rel_diff_int8_vs_fp64_tensor": float(np.abs(full_gA - dmma_gA).max() / np.abs(dmma_gA).max())}
         # checkpointed adjoint (wdl.checkpoint = k): history footprint and step time
         NW, ND = N * S * B * 8, N * B * 8
         ck = {}

@@ -95,6 +95,11 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       over by later ones that fit the free CTAs (default 5000);
  *   "wdl.infer_docs": documents per stacked-column chunk of WDL inference
  *       (default 1024);
+ *   "wdl.int8": where the WDL products run: 1 (default) on the INT8 tensor
+ *       cores for N >= 1024 (each FP64 product emulated exactly by 24
+ *       modular integer products and CRT reconstruction), else on the FP64
+ *       tensor cores; 2 on the INT8 tensor cores whenever N <= 8192; 0
+ *       always on the FP64 tensor cores;
  *   "wdl.checkpoint": k > 0 keeps the WDL forward state only every k-th
  *       iteration plus one segment of k iterations and recomputes the other
  *       segments during the backward (same gradient bits; 2 (L - k) more

@@ -56,7 +56,7 @@ const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "
                                    "batch.strip_kb", "batch.max_team", "batch.redundant_rows",
                                    "batch.l2_keep_mb", "batch.max_elems", "batch.resident_team",
                                    "batch.stream_strip_kb", "batch.backfill_us",
-                                   "wdl.infer_docs", "wdl.checkpoint", "dgemm.kshape", "dgemm.tile", "barycenter.log_path"};
+                                   "wdl.infer_docs", "wdl.checkpoint", "wdl.int8", "dgemm.kshape", "dgemm.tile", "barycenter.log_path"};
 }  // namespace
 
 double option(const char* name, double dflt) {

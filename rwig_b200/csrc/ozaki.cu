@@ -127,7 +127,10 @@ Crt make_crt() {
         F[k / 64] |= 1ull << (k % 64);
       }
     }
-    for (int l = 0; l < 4; ++l) c.F[t][l] = F[l];
+    for (int l = 0; l < 4; ++l) {
+      c.F32[t][2 * l] = (unsigned)(F[l] & 0xffffffffu);
+      c.F32[t][2 * l + 1] = (unsigned)(F[l] >> 32);
+    }
   }
   return c;
 }
@@ -142,64 +145,41 @@ const Crt& crt_constants() {
 // ---------------------------------------------------------------------------
 // scaling exponents and residues
 // ---------------------------------------------------------------------------
+constexpr int kChunks = 5;  // 20-bit chunks of a scaled integer (100 bits >= kQ)
+
+// Per-modulus constants, passed by value (uniform across a launch): p, 1/p,
+// the reduction multiplier ceil(2^32 / p) and the chunk weights 2^(20 b) mod p.
 struct Mods {
   int p[kT];
   double invp[kT];
+  unsigned mg[kT];
+  unsigned w[kT][kChunks];
 };
 
 Mods mods_of(const Crt& c) {
   Mods m;
   for (int t = 0; t < kT; ++t) {
+    const unsigned long long p = (unsigned long long)c.p[t];
     m.p[t] = c.p[t];
     m.invp[t] = c.invp[t];
+    m.mg[t] = (unsigned)((0x100000000ull + p - 1) / p);
+    unsigned long long v = 1 % p;
+    for (int b = 0; b < kChunks; ++b) {
+      m.w[t][b] = (unsigned)v;
+      v = (v << 20) % p;
+    }
   }
   return m;
 }
 
 __device__ __forceinline__ int scale_exp(double mx) { return mx > 0.0 ? kQ - 1 - ilogb(mx) : 0; }
 
-// v mod p for an integer-valued double 0 <= v < 2^53, exactly.
-__device__ __forceinline__ int mod_exact(double v, int p, double invp) {
-  const double q = floor(v * invp);
-  int r = (int)fma(-q, (double)p, v);
-  if (r < 0) r += p;
-  if (r >= p) r -= p;
-  return r;
-}
 
-constexpr int kPw = 64;  // 2^s mod p_t for s < kPw (the scaled shift is at most kQ - 53)
-
-__device__ void load_pow2(int* pw, const Mods& m) {
-  for (int t = threadIdx.x + blockDim.x * threadIdx.y; t < kT; t += blockDim.x * blockDim.y) {
-    int v = 1 % m.p[t];
-    for (int s = 0; s < kPw; ++s) {
-      pw[t * kPw + s] = v;
-      v = (v * 2) % m.p[t];
-    }
-  }
-}
-
-// Symmetric residues of trunc(x 2^sc) for every modulus into out[t * plane].
-__device__ __forceinline__ void residues(double x, int sc, const int* pw, const Mods& m, int8_t* out, size_t plane) {
-  if (!(x != 0.0)) {
-#pragma unroll 4
-    for (int t = 0; t < kT; ++t) out[t * plane] = 0;
-    return;
-  }
-  const double ax = fabs(x);
-  const int e = ilogb(ax);
-  const double mant = ldexp(ax, 52 - e);  // integer in [2^52, 2^53)
-  const int sh = e - 52 + sc;             // trunc(|x| 2^sc) = mant 2^sh
-  const double base = sh >= 0 ? mant : (sh > -64 ? trunc(ldexp(mant, sh)) : 0.0);
-  const int s = sh >= 0 ? min(sh, kPw - 1) : 0;
-#pragma unroll 4
-  for (int t = 0; t < kT; ++t) {
-    const int p = m.p[t];
-    int r = mod_exact(base, p, m.invp[t]);
-    if (s) r = (r * pw[t * kPw + s]) % p;
-    if (x < 0.0 && r) r = p - r;
-    out[t * plane] = (int8_t)(r > (p - 1) / 2 ? r - p : r);
-  }
+// x mod p for x < 2^32 and p <= 256 (Barrett: the quotient estimate from the
+// multiplier ceil(2^32 / p) is exact or one too large).
+__device__ __forceinline__ unsigned bmod(unsigned x, unsigned p, unsigned mg) {
+  const int r = (int)(x - __umulhi(x, mg) * p);
+  return r < 0 ? (unsigned)(r + (int)p) : (unsigned)r;
 }
 
 // alpha[i] from max_k |K[i + k ldk]| (rows of K), one thread per row.
@@ -226,18 +206,71 @@ __global__ void exp_cols(const double* X, long long ldx, int Kd, int* e) {
   if (threadIdx.x == 0) e[j] = scale_exp(sh[0]);
 }
 
+// trunc(|x| 2^sc) (< 2^100) as five 20-bit chunks; false for x = 0.
+__device__ __forceinline__ bool chunks_scaled(double x, int sc, unsigned (&ch)[kChunks]) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+  if (bits == 0) {
+#pragma unroll
+    for (int b = 0; b < kChunks; ++b) ch[b] = 0;
+    return false;
+  }
+  const int eb = (int)(bits >> 52);
+  const unsigned long long mant = eb ? ((bits & 0xfffffffffffffull) | (1ull << 52)) : bits;
+  const int sh = (eb ? eb : 1) - 1075 + sc;  // |x| 2^sc = mant 2^sh
+  unsigned long long lo, hi;                 // the 128-bit integer trunc(mant 2^sh)
+  if (sh >= 0) {
+    lo = sh < 64 ? mant << sh : 0ull;
+    hi = sh == 0 ? 0ull : (sh < 64 ? mant >> (64 - sh) : mant << (sh - 64));
+  } else {
+    lo = sh > -64 ? mant >> -sh : 0ull;
+    hi = 0ull;
+  }
+  const unsigned m20 = (1u << 20) - 1;
+  ch[0] = (unsigned)lo & m20;
+  ch[1] = (unsigned)(lo >> 20) & m20;
+  ch[2] = (unsigned)(lo >> 40) & m20;
+  ch[3] = (unsigned)((lo >> 60) | (hi << 4)) & m20;
+  ch[4] = (unsigned)(hi >> 16) & m20;
+  return true;
+}
+
+// Residue in [0, p_t) of the chunked integer, negated modulo p_t for x < 0:
+// sum_b ch_b (2^(20 b) mod p) < 5 2^28 fits 32 bits; one Barrett reduction.
+__device__ __forceinline__ unsigned residue_chunks(const unsigned (&ch)[kChunks], bool neg, const Mods& m, int t) {
+  unsigned s = 0;
+#pragma unroll
+  for (int b = 0; b < kChunks; ++b) s += ch[b] * m.w[t][b];
+  const unsigned p = (unsigned)m.p[t];
+  const unsigned r = bmod(s, p, m.mg[t]);
+  return (neg && r) ? p - r : r;
+}
+
 // Row r of the operand is column r of src (A(r, k) = src[k + r ld]):
-// out[t][r][k] for r < rows_pad, k < Kpad (zero outside rows x Kd).
-__global__ void res_cols(const double* src, long long ld, int Kd, int rows, const int* ex, int Kpad, int rows_pad,
-                         Mods m, int8_t* out) {
-  __shared__ int pw[kT * kPw];
-  load_pow2(pw, m);
-  __syncthreads();
+// out[t][r][k] for r < rows_pad, k < Kpad (zero outside rows x Kd).  Each
+// thread takes 4 consecutive k and stores one 32-bit word per modulus.
+__global__ void __launch_bounds__(256) res_cols(const double* src, long long ld, int Kd, int rows, const int* ex,
+                                                int Kpad, int rows_pad, Mods m, int8_t* out) {
   const int r = blockIdx.y;
-  const size_t plane = (size_t)rows_pad * Kpad;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Kpad; k += gridDim.x * blockDim.x) {
-    const double x = (r < rows && k < Kd) ? src[k + (long long)r * ld] : 0.0;
-    residues(x, r < rows ? ex[r] : 0, pw, m, out + (size_t)r * Kpad + k, plane);
+  const size_t plane4 = (size_t)rows_pad * Kpad / 4;
+  const int sc = r < rows ? ex[r] : 0;
+  for (int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x); k0 < Kpad; k0 += 4 * gridDim.x * blockDim.x) {
+    unsigned ch[4][kChunks];
+    bool ng[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + q;
+      const double x = (r < rows && k < Kd) ? src[k + (long long)r * ld] : 0.0;
+      chunks_scaled(x, sc, ch[q]);
+      ng[q] = x < 0.0;
+    }
+    unsigned* o = reinterpret_cast<unsigned*>(out + (size_t)r * Kpad + k0);
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      unsigned w = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w |= residue_chunks(ch[q], ng[q], m, t) << (8 * q);
+      o[t * plane4] = w;
+    }
   }
 }
 
@@ -245,9 +278,7 @@ __global__ void res_cols(const double* src, long long ld, int Kd, int rows, cons
 // transposed through shared memory, out[t][i][k].
 __global__ void res_rows(const double* K, long long ldk, int n, const int* alpha, int Kpad, int Mpad, Mods m,
                          int8_t* out) {
-  __shared__ int pw[kT * kPw];
   __shared__ double tile[32][33];
-  load_pow2(pw, m);
   const int i0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int i = i0 + threadIdx.x, k = k0 + r;
@@ -257,20 +288,30 @@ __global__ void res_rows(const double* K, long long ldk, int n, const int* alpha
   const size_t plane = (size_t)Mpad * Kpad;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int i = i0 + r, k = k0 + threadIdx.x;
-    if (i < Mpad && k < Kpad) residues(tile[threadIdx.x][r], i < n ? alpha[i] : 0, pw, m, out + (size_t)i * Kpad + k, plane);
+    if (i < Mpad && k < Kpad) {
+      const double x = tile[threadIdx.x][r];
+      unsigned ch[kChunks];
+      chunks_scaled(x, i < n ? alpha[i] : 0, ch);
+      int8_t* o = out + (size_t)i * Kpad + k;
+#pragma unroll 4
+      for (int t = 0; t < kT; ++t) o[t * plane] = (int8_t)residue_chunks(ch, x < 0.0, m, t);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // the tcgen05 INT8 GEMM
 // ---------------------------------------------------------------------------
-constexpr int kStages = 4;
-constexpr int kAStage = kTileM * kBk;  // 16 KB
+constexpr int kStages = 3;
+constexpr int kCtaM = 2 * kTileM;      // two M = 128 accumulators per CTA: 256 rows
+constexpr int kAStage = kCtaM * kBk;   // 32 KB
 constexpr int kBStage = 256 * kBk;     // room for ntile <= 256: 32 KB
+constexpr int kGemmThreads = 256;
 constexpr size_t kGemmSmem = 1024 + (size_t)kStages * (kAStage + kBStage) + 256;
 
 struct I8Args {
   int Mpad, Wpad, Kpad, ntile, nk;
+  int sgn;        // 1: signed int8 operands (self-check), 0: unsigned residues
   uint8_t* cres;  // residue planes [T][Wpad][Mpad]
   int* raw;       // RAW: the int32 product [Wpad][Mpad]
   unsigned* err;
@@ -295,10 +336,11 @@ __device__ __forceinline__ uint64_t sw128_desc(const void* p) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// Instruction descriptor of kind::i8: int32 accumulator, signed A and B,
-// both K-major, N = ntile, M = 128.
-__host__ __device__ constexpr uint32_t i8_idesc(int n) {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+// Instruction descriptor of kind::i8: int32 accumulator, A and B signed
+// (sgn = 1) or unsigned (sgn = 0) 8-bit, both K-major, N = n, M = 128.
+__host__ __device__ constexpr uint32_t i8_idesc(int n, int sgn) {
+  return (2u << 4) | ((uint32_t)sgn << 7) | ((uint32_t)sgn << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kTileM >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -329,11 +371,11 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u; }
-
+// One CTA: a 256 x ntile output tile of residue plane z as two 128-row
+// accumulators in the 512 tensor-memory columns (half h at column 256 h).
 template <bool RAW>
-__global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtensorMap ta,
-                                                  const __grid_constant__ CUtensorMap tb, I8Args g) {
+__global__ void __launch_bounds__(kGemmThreads, 1) i8_gemm(const __grid_constant__ CUtensorMap ta,
+                                                           const __grid_constant__ CUtensorMap tb, I8Args g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* sA = base;
@@ -343,8 +385,8 @@ __global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtens
   uint64_t* done = empty + kStages;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * g.ntile, m0 = blockIdx.y * kTileM, z = blockIdx.z;
-  const uint32_t ncols = tmem_cols(g.ntile);
+  const int n0 = blockIdx.x * g.ntile, m0 = blockIdx.y * kCtaM, z = blockIdx.z;
+  constexpr uint32_t ncols = 512;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(full + s, 1);
@@ -382,7 +424,7 @@ __global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtens
     for (int kb = std::max(0, issued - kStages); kb < issued; ++kb)
       if (issued < g.nk && !mbar_wait_bounded(full + kb % kStages, (kb / kStages) & 1)) atomicOr(g.err, KERR_MBAR_TIMEOUT);
   } else if (warp == 1 && lane == 0) {  // MMAs
-    const uint32_t idesc = i8_idesc(g.ntile);
+    const uint32_t idesc = i8_idesc(g.ntile, g.sgn);
     for (int kb = 0; kb < g.nk; ++kb) {
       const int s = kb % kStages;
       if (!mbar_wait_bounded(full + s, (kb / kStages) & 1)) {
@@ -393,8 +435,11 @@ __global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtens
       const uint8_t* a = sA + (size_t)s * kAStage;
       const uint8_t* b = sB + (size_t)s * kBStage;
 #pragma unroll
-      for (int kk = 0; kk < kBk / 32; ++kk)
-        tc_mma(tmem, sw128_desc(a + kk * 32), sw128_desc(b + kk * 32), idesc, (kb | kk) != 0);
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int kk = 0; kk < kBk / 32; ++kk)
+          tc_mma(tmem + (uint32_t)(256 * h), sw128_desc(a + h * (kTileM * kBk) + kk * 32), sw128_desc(b + kk * 32),
+                 idesc, (kb | kk) != 0);
       tc_commit(empty + s);  // the stage is free once these MMAs have read it
     }
     tc_commit(done);  // everything issued has completed
@@ -406,12 +451,13 @@ __global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtens
   if (!have) {
     if (threadIdx.x == 0) atomicOr(g.err, KERR_MBAR_TIMEOUT);
   } else if ((*(volatile unsigned*)g.err & KERR_MBAR_TIMEOUT) == 0) {
-    const int i = m0 + warp * 32 + lane;  // accumulator lane = output row
-    const int p = RAW ? 1 : g.m.p[z];
+    const int h = warp >> 2, lq = warp & 3;                // accumulator half, tensor-memory lane quarter
+    const int i = m0 + h * kTileM + lq * 32 + lane;         // output row
+    const unsigned p = RAW ? 1u : (unsigned)g.m.p[z];
     const double invp = RAW ? 1.0 : g.m.invp[z];
     for (int c = 0; c < g.ntile; c += 32) {
       uint32_t v[32];
-      tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      tc_ld32(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(256 * h + c), v);
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
         if (c + q >= g.ntile) break;  // columns of the last load beyond the tile
@@ -420,9 +466,9 @@ __global__ void __launch_bounds__(128, 1) i8_gemm(const __grid_constant__ CUtens
         if (RAW) {
           g.raw[(size_t)j * g.Mpad + i] = d;
         } else {
-          int r = d - (int)floor((double)d * invp) * p;
-          if (r < 0) r += p;
-          if (r >= p) r -= p;
+          int r = d - (int)floor((double)d * invp) * (int)p;
+          if (r < 0) r += (int)p;
+          if (r >= (int)p) r -= (int)p;
           g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)r;
         }
       }
@@ -476,7 +522,7 @@ int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes,
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 int pick_ntile(int W) { return std::min(256, round_up(std::max(W, 16), 16)); }
 
-enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_BRES, SO_BETA, SO_CRES, SO_ERR, SO_TA, SO_TB, SO_TD };
+enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_BRES, SO_BETA, SO_CRES, SO_ERR, SO_TA, SO_TB, SO_TD, SO_Y };
 
 // The kT (or, RAW, one) planes of A (Mpad x Kpad) and B (Wpad x Kpad): the
 // int8 products into cres (or raw).
@@ -484,17 +530,17 @@ template <bool RAW>
 int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad, int Kpad, int ntile, int planes,
               uint8_t* cres, int* raw, cudaStream_t st) {
   CUtensorMap ta, tb;
-  if (int rc = make_map(&ta, A, Kpad, Mpad, planes, kTileM)) return rc;
+  if (int rc = make_map(&ta, A, Kpad, Mpad, planes, kCtaM)) return rc;
   if (int rc = make_map(&tb, B, Kpad, Wpad, planes, ntile)) return rc;
-  unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);
+  unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);  // cleared by reset_err()
   if (!err) return RWIG_E_NOMEM;
-  RWIG_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), st));
   I8Args g{};
   g.Mpad = Mpad;
   g.Wpad = Wpad;
   g.Kpad = Kpad;
   g.ntile = ntile;
   g.nk = Kpad / kBk;
+  g.sgn = RAW ? 1 : 0;
   g.cres = cres;
   g.raw = raw;
   g.err = err;
@@ -504,9 +550,18 @@ int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad
     RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
     attr = true;
   }
-  const dim3 grid(Wpad / ntile, Mpad / kTileM, planes);
-  i8_gemm<RAW><<<grid, 128, kGemmSmem, st>>>(ta, tb, g);
+  const dim3 grid(Wpad / ntile, Mpad / kCtaM, planes);
+  i8_gemm<RAW><<<grid, kGemmThreads, kGemmSmem, st>>>(ta, tb, g);
   RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// Clears the error word that the GEMMs of a sequence (prepare() .. status())
+// accumulate their bounded-wait failures into.
+int reset_err(Context* ctx, cudaStream_t st) {
+  unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);
+  if (!err) return RWIG_E_NOMEM;
+  RWIG_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), st));
   return 0;
 }
 
@@ -529,10 +584,11 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
   pr->K = K;
   pr->ldk = ldk;
   pr->Mo = pr->Kd = n;
-  pr->Mpad = round_up(n, kTileM);
+  pr->Mpad = round_up(n, kCtaM);
   pr->Kpad = round_up(n, kBk);
   const size_t planes = (size_t)kT * pr->Mpad * pr->Kpad;
   const Mods m = mods_of(crt_constants());
+  if (int rc = reset_err(ctx, st)) return rc;
   for (int tr = 0; tr < 2; ++tr) {
     pr->ares[tr] = (int8_t*)scratch(ctx, SO_ARES0 + tr, planes);
     pr->alpha[tr] = (int*)scratch(ctx, SO_ALPHA0 + tr, sizeof(int) * n);
@@ -544,7 +600,7 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
                                                                         pr->ares[0]);
   // trans = 1: columns of K
   exp_cols<<<n, 256, 0, st>>>(K, ldk, n, pr->alpha[1]);
-  res_cols<<<dim3((pr->Kpad + 255) / 256, pr->Mpad), 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m,
+  res_cols<<<dim3((pr->Kpad / 4 + 255) / 256, pr->Mpad), 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m,
                                                                     pr->ares[1]);
   if (launches) *launches += 4;
   RWIG_CUDA_TRY(cudaGetLastError());
@@ -562,7 +618,7 @@ int products(Context* ctx, const Prepared& pr, int trans, const double* X, long 
   if (!bres || !be || !cr) return RWIG_E_NOMEM;
   const Mods m = mods_of(crt_constants());
   exp_cols<<<W, 256, 0, st>>>(X, ldx, pr.Kd, be);
-  res_cols<<<dim3((pr.Kpad + 255) / 256, Wpad), 256, 0, st>>>(X, ldx, pr.Kd, W, be, pr.Kpad, Wpad, m, bres);
+  res_cols<<<dim3((pr.Kpad / 4 + 255) / 256, Wpad), 256, 0, st>>>(X, ldx, pr.Kd, W, be, pr.Kpad, Wpad, m, bres);
   if (int rc = launch_i8<false>(ctx, pr.ares[trans], pr.Mpad, bres, Wpad, pr.Kpad, ntile, kT, cr, nullptr, st)) return rc;
   if (launches) *launches += 3;
   *cres = cr;
@@ -570,6 +626,97 @@ int products(Context* ctx, const Prepared& pr, int trans, const double* X, long 
   *Wpad_out = Wpad;
   return 0;
 }
+
+// The signed fraction held in eight 32-bit limb sums (carries pending, top
+// limb first in significance), as |s| and its sign.
+__device__ __forceinline__ double limbs_to_fraction(const unsigned long long (&acc)[8], int l0, bool& neg) {
+  unsigned limb[8];
+  unsigned long long carry = 0ull;
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    const unsigned long long x = (l >= l0 ? acc[l] : 0ull) + carry;
+    limb[l] = (unsigned)x;
+    carry = x >> 32;
+  }
+  neg = (limb[7] >> 31) != 0;  // the fraction read in [-1/2, 1/2)
+  if (neg) {                     // two's complement negation of the 256-bit value
+    unsigned long long b = 1ull;
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      const unsigned long long x = (unsigned long long)(~limb[l]) + b;
+      limb[l] = (unsigned)x;
+      b = x >> 32;
+    }
+  }
+  return ldexp((double)(((unsigned long long)limb[7] << 32) | limb[6]), -64) +
+         ldexp((double)(((unsigned long long)limb[5] << 32) | limb[4]), -128) +
+         ldexp((double)(((unsigned long long)limb[3] << 32) | limb[2]), -192);
+}
+
+// Reconstruction (one thread per two consecutive rows of one column): the
+// 256-bit fraction frac(sum_t c_t e_t / P) is accumulated as eight 32-bit
+// limb sums in 64-bit registers (each below 24 * 255 * 2^32 < 2^45, so the
+// carries wait until the end) and read as a signed fraction s; Y = s P
+// 2^-(alpha + beta).  Fast path: the four upper limbs alone.  The lower ones
+// add less than 24 * 255 * 2^-128 < 2^-115 to s, which is within 2^-55 of
+// |s| once |s| >= 2^-60; smaller values are recomputed with all eight.
+__global__ void __launch_bounds__(256) crt_store(Crt c, const uint8_t* __restrict__ cres, int Mpad, int Wpad,
+                                                 const int* __restrict__ alpha, const int* __restrict__ beta, int Mo,
+                                                 int W, double* __restrict__ Y, long long ldy) {
+  const int npairs = (Mo + 1) / 2;
+  const size_t plane2 = (size_t)Wpad * Mpad / 2;  // plane stride in 16-bit words
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)npairs * W;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(e % npairs) * 2, j = (int)(e / npairs);
+    const unsigned short* q = reinterpret_cast<const unsigned short*>(cres + (size_t)j * Mpad + i0);
+    unsigned long long acc[2][8];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int l = 0; l < 8; ++l) acc[u][l] = 0ull;
+#pragma unroll 4
+    for (int t = 0; t < kT; ++t) {
+      const unsigned w = __ldg(q + t * plane2);
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const unsigned ct = (w >> (8 * u)) & 0xffu;
+#pragma unroll
+        for (int l = 4; l < 8; ++l) acc[u][l] += (unsigned long long)ct * c.F32[t][l];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int i = i0 + u;
+      if (i >= Mo) break;
+      bool neg;
+      double mag = limbs_to_fraction(acc[u], 4, neg);
+      if (mag < 0x1p-60) {  // small: the lower limbs matter
+        unsigned long long full[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) full[l] = 0ull;
+        for (int t = 0; t < kT; ++t) {
+          const unsigned ct = (__ldg(q + t * plane2) >> (8 * u)) & 0xffu;
+#pragma unroll
+          for (int l = 0; l < 8; ++l) full[l] += (unsigned long long)ct * c.F32[t][l];
+        }
+        mag = limbs_to_fraction(full, 0, neg);
+      }
+      Y[(long long)i + (long long)j * ldy] = ldexp(neg ? -mag * c.P : mag * c.P, -(alpha[i] + beta[j]));
+    }
+  }
+}
+
+int reconstruct(Context* ctx, const Prepared& pr, int trans, const uint8_t* cres, int Wpad, const int* beta, int W,
+                double* Y, long long ldy, cudaStream_t st, int* launches) {
+  const long long n = (long long)((pr.Mo + 1) / 2) * W;
+  const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx->sm_count));
+  crt_store<<<grid, 256, 0, st>>>(crt_constants(), cres, pr.Mpad, Wpad, pr.alpha[trans], beta, pr.Mo, W, Y, ldy);
+  if (launches) ++*launches;
+  RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+double* product_buffer(Context* ctx, size_t doubles) { return (double*)scratch(ctx, SO_Y, sizeof(double) * doubles); }
 
 // Bounded-wait status of the last products() launches (a host read).
 int status(Context* ctx, cudaStream_t st) { return check_err(ctx, st); }
@@ -591,7 +738,7 @@ extern "C" int rwig_selftest_i8gemm(const signed char* A, const signed char* B, 
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!oz::available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 tensor-core GEMM unavailable");
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  const int ntile = oz::pick_ntile(N), Mpad = oz::round_up(M, oz::kTileM), Npad = oz::round_up(N, ntile);
+  const int ntile = oz::pick_ntile(N), Mpad = oz::round_up(M, oz::kCtaM), Npad = oz::round_up(N, ntile);
   const int Kpad = oz::round_up(Kd, oz::kBk);
   int8_t* a = (int8_t*)scratch(ctx, oz::SO_TA, (size_t)Mpad * Kpad);
   int8_t* b = (int8_t*)scratch(ctx, oz::SO_TB, (size_t)Npad * Kpad);
@@ -601,6 +748,7 @@ extern "C" int rwig_selftest_i8gemm(const signed char* A, const signed char* B, 
   RWIG_CUDA_TRY(cudaMemsetAsync(b, 0, (size_t)Npad * Kpad, st));
   RWIG_CUDA_TRY(cudaMemcpy2DAsync(a, Kpad, A, Kd, Kd, M, cudaMemcpyDeviceToDevice, st));
   RWIG_CUDA_TRY(cudaMemcpy2DAsync(b, Kpad, B, Kd, Kd, N, cudaMemcpyDeviceToDevice, st));
+  if (int rc = oz::reset_err(ctx, st)) return rc;
   if (int rc = oz::launch_i8<true>(ctx, a, Mpad, b, Npad, Kpad, ntile, 1, nullptr, d, st)) return rc;
   RWIG_CUDA_TRY(cudaMemcpy2DAsync(D, sizeof(int) * M, d, sizeof(int) * Mpad, sizeof(int) * M, N,
                                   cudaMemcpyDeviceToDevice, st));

@@ -10,10 +10,10 @@
 //      row / column is just below 2^q; truncation toward zero gives integer
 //      matrices Ah, Xh with |entries| < 2^q (an entry loses bits only where it
 //      is below 2^(53-q) of its row's / column's largest).
-//   2. Residues.  For T pairwise coprime moduli p_t <= 256 the symmetric
-//      residues Ah mod p_t, Xh mod p_t fit in int8.
+//   2. Residues.  For T pairwise coprime moduli p_t <= 256 the residues
+//      Ah mod p_t, Xh mod p_t in [0, p_t) fit in uint8.
 //   3. Products.  D_t = (Ah mod p_t)(Xh mod p_t) is exact in the tensor
-//      cores' int32 accumulators (|D_t| <= Kd 2^14 < 2^31 for Kd <= 2^16);
+//      cores' int32 accumulators (0 <= D_t <= Kd 255^2 < 2^31 for Kd <= 33000);
 //      c_t = D_t mod p_t in [0, p_t) (ozaki.cu).
 //   4. Reconstruction.  With P = prod p_t, M_t = P / p_t and e_t = M_t
 //      (M_t^-1 mod p_t), Ch = Ah Xh is the representative in (-P/2, P/2) of
@@ -26,8 +26,9 @@
 // With T = 24 moduli (log2 P = 184.09) and q = 85 the product is exact for
 // the truncated inputs; the only errors are the truncation of entries far
 // below their row's / column's maximum (relative 2^-85 of that maximum) and
-// the final rounding.  The reconstruction kernel hands each output tile to
-// the same epilogue functors as the DMMA GEMM (dgemm.cuh contract).
+// the final rounding.  The reconstruction writes the FP64 product; a tile
+// kernel then hands each output tile to the same epilogue functors as the
+// DMMA GEMM (dgemm.cuh contract).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,15 +46,15 @@ constexpr int kQ = 85;        // bits of the scaled integers
 constexpr int kMaxKd = 8192;  // contraction length for which kQ is safe: Kd 2^(2 kQ) < P / 2
 constexpr int kTileM = 128;   // UMMA M
 constexpr int kBk = 128;      // bytes of K per pipeline stage (one 128-byte swizzle atom)
-constexpr int kCrtRows = 64;  // rows per reconstruction tile
-constexpr int kCrtCols = 64;  // most columns per reconstruction tile (the DMMA GEMM's widest tile)
+constexpr int kCrtRows = 32;  // rows per epilogue tile
+constexpr int kCrtCols = 64;  // most columns per epilogue tile (the DMMA GEMM's widest tile)
 constexpr int kCrtThreads = 256;
 
 // Reconstruction constants, passed by value to the kernels.
 struct Crt {
   int p[kT];
   double invp[kT];
-  unsigned long long F[kT][4];  // floor(2^256 e_t / P), little-endian 64-bit limbs
+  unsigned F32[kT][8];  // floor(2^256 e_t / P), little-endian 32-bit limbs
   double P;                     // P rounded to double
 };
 
@@ -61,7 +62,7 @@ struct Crt {
 const Crt& crt_constants();
 
 // op(K) as the tensor cores' A operand: residues [kT][Mpad][Kpad] (K-major
-// int8) and the row exponents alpha (Mo ints), for trans = 0 (K, rows of K)
+// uint8) and the row exponents alpha (Mo ints), for trans = 0 (K, rows of K)
 // and trans = 1 (K^T, columns of K).
 struct Prepared {
   const double* K = nullptr;
@@ -72,7 +73,8 @@ struct Prepared {
 };
 
 // Residues and exponents of op(K) for trans = 0 and 1 (square K: Mo = Kd),
-// into engine scratch slots.  Returns 0 or an engine error.
+// into engine scratch slots; starts a sequence of products whose bounded-wait
+// failures status() reports.  Returns 0 or an engine error.
 int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches);
 
 // X's residues and the kT integer products: cres[t][j][i] = (A_t X_t)_ij mod
@@ -81,63 +83,43 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
 int products(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, cudaStream_t st,
              const uint8_t** cres, const int** beta, int* Wpad, int* launches);
 
-// Status of the bounded waits of the INT8 GEMMs enqueued so far on `st`
-// (synchronises): 0 or RWIG_E_TIMEOUT.
+// Status of the bounded waits of the INT8 GEMMs enqueued on `st` since
+// prepare() (synchronises): 0 or RWIG_E_TIMEOUT.
 int status(Context* ctx, cudaStream_t st);
 
 // Whether the INT8 tensor-core path can run: sm_100 class device with the
 // driver's tensor-map entry point.
 bool available(Context* ctx);
 
-// Reconstruction of one kCrtRows x tc output tile, then the epilogue.
+// Y (Mo x W, ldy) = op(K) X from the residue planes of products():
+// reconstruction and scaling (ozaki.cu).
+int reconstruct(Context* ctx, const Prepared& pr, int trans, const uint8_t* cres, int Wpad, const int* beta, int W,
+                double* Y, long long ldy, cudaStream_t st, int* launches);
+
+// Scratch for the FP64 product of `products` (Mo x W doubles).
+double* product_buffer(Context* ctx, size_t doubles);
+
+// Tiles of kCrtRows x tc of Y handed to the epilogue (the dgemm.cuh
+// contract: value (r0 + r, c0 + c) at t[c * ldt + r], columns >= W zero,
+// 2 (kCrtCols + 1) ldt doubles of workspace).
 template <class Epi>
-__global__ void __launch_bounds__(kCrtThreads) crt_kernel(Crt c, const uint8_t* __restrict__ cres, int Mpad, int Wpad,
-                                                          const int* __restrict__ alpha, const int* __restrict__ beta,
-                                                          int Mo, int W, int tc, Epi epi) {
+__global__ void __launch_bounds__(kCrtThreads) epi_tiles(const double* __restrict__ Y, long long ldy, int Mo, int W,
+                                                         int tc, Epi epi) {
   extern __shared__ double sm[];
   constexpr int ldt = kCrtRows + 1;
-  double* tile = sm;                            // [tc][ldt]
-  double* ws = sm + (size_t)kCrtCols * ldt;      // 2 (BN + 1) ldt doubles
+  double* tile = sm;                         // [tc][ldt]
+  double* ws = sm + (size_t)kCrtCols * ldt;  // 2 (kCrtCols + 1) ldt doubles
   const int r0 = blockIdx.x * kCrtRows, c0 = blockIdx.y * tc;
   const int nr = min(kCrtRows, Mo - r0);
-  const size_t plane = (size_t)Wpad * Mpad;
   for (int e = threadIdx.x; e < kCrtRows * tc; e += blockDim.x) {
-    const int r = e % kCrtRows, cc = e / kCrtRows, i = r0 + r, j = c0 + cc;
-    double v = 0.0;
-    if (r < nr && j < W) {
-      const uint8_t* q = cres + (size_t)j * Mpad + i;
-      unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll 4
-      for (int t = 0; t < kT; ++t) {
-        const unsigned long long ct = q[(size_t)t * plane];
-        unsigned __int128 x = (unsigned __int128)ct * c.F[t][0] + a0;
-        a0 = (unsigned long long)x;
-        x = (unsigned __int128)ct * c.F[t][1] + a1 + (unsigned long long)(x >> 64);
-        a1 = (unsigned long long)x;
-        x = (unsigned __int128)ct * c.F[t][2] + a2 + (unsigned long long)(x >> 64);
-        a2 = (unsigned long long)x;
-        a3 = a3 + ct * c.F[t][3] + (unsigned long long)(x >> 64);
-      }
-      // frac(sum / P) as a signed fraction in [-1/2, 1/2)
-      const bool neg = (a3 >> 63) != 0;
-      if (neg) {  // two's complement negation of the 256-bit value
-        a0 = ~a0;
-        a1 = ~a1;
-        a2 = ~a2;
-        a3 = ~a3;
-        if (++a0 == 0 && ++a1 == 0 && ++a2 == 0) ++a3;
-      }
-      const double mag = ldexp((double)a3, -64) + ldexp((double)a2, -128) + ldexp((double)a1, -192);
-      const double ch = mag * c.P;  // |Ah Xh|_ij
-      v = ldexp(neg ? -ch : ch, -(alpha[i] + beta[j]));
-    }
-    tile[cc * ldt + r] = v;
+    const int r = e % kCrtRows, cc = e / kCrtRows;
+    tile[cc * ldt + r] = (r < nr && c0 + cc < W) ? Y[(long long)(r0 + r) + (long long)(c0 + cc) * ldy] : 0.0;
   }
   __syncthreads();
   epi(r0, nr, c0, tc, tile, ldt, ws);
 }
 
-inline size_t crt_smem_bytes() { return sizeof(double) * (size_t)(kCrtCols + 2 * (kCrtCols + 1)) * (kCrtRows + 1); }
+inline size_t epi_smem_bytes() { return sizeof(double) * (size_t)(kCrtCols + 2 * (kCrtCols + 1)) * (kCrtRows + 1); }
 
 // Y = op(K) X through the INT8 tensor cores, each output tile handed to
 // `epi` (the dgemm.cuh epilogue contract, tiles of kCrtRows rows and tc
@@ -149,16 +131,18 @@ int gemm(Context* ctx, const Prepared& pr, int trans, const double* X, long long
   const int* beta = nullptr;
   int Wpad = 0;
   if (int rc = products(ctx, pr, trans, X, ldx, W, st, &cres, &beta, &Wpad, launches)) return rc;
+  double* Y = product_buffer(ctx, (size_t)pr.Mo * W);
+  if (!Y) return RWIG_E_NOMEM;
+  if (int rc = reconstruct(ctx, pr, trans, cres, Wpad, beta, W, Y, pr.Mo, st, launches)) return rc;
   if (tc <= 0 || tc > kCrtCols) tc = kCrtCols;
   static bool attr = false;  // once per instantiation (callers hold the context lock)
-  const size_t smem = crt_smem_bytes();
+  const size_t smem = epi_smem_bytes();
   if (!attr) {
-    RWIG_CUDA_TRY(cudaFuncSetAttribute(crt_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RWIG_CUDA_TRY(cudaFuncSetAttribute(epi_tiles<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   const dim3 grid((pr.Mo + kCrtRows - 1) / kCrtRows, (W + tc - 1) / tc);
-  crt_kernel<Epi><<<grid, kCrtThreads, smem, st>>>(crt_constants(), cres, pr.Mpad, Wpad, pr.alpha[trans], beta,
-                                                    pr.Mo, W, tc, epi);
+  epi_tiles<Epi><<<grid, kCrtThreads, smem, st>>>(Y, pr.Mo, pr.Mo, W, tc, epi);
   if (launches) ++*launches;
   RWIG_CUDA_TRY(cudaGetLastError());
   return 0;

@@ -34,6 +34,7 @@
 #include "barycenter.h"
 #include "dgemm.cuh"
 #include "engine.h"
+#include "ozaki.cuh"
 
 namespace rwig {
 namespace wdl {
@@ -494,7 +495,7 @@ __global__ void infer_output(const double* bB, int N, double* Yhat) {
 // Inference of documents [0, M): A (N x S), W (S x M), K padded (ldk); Yhat
 // (N x M).  Chunks of at most wdl.infer_docs documents (default 1024).
 int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const double* K, long long ldk, int N,
-          int S, int M, int L, double tol, double* Yhat, int* launches) {
+          int S, int M, int L, double tol, double* Yhat, int* launches, const oz::Prepared* pr) {
   const int chunk = std::max(1, std::min(M, (int)option("wdl.infer_docs", 1024.0)));
   const size_t NWc = (size_t)N * S * chunk;
   double* UB = (double*)scratch(ctx, SW_IU, sizeof(double) * NWc);
@@ -512,6 +513,7 @@ int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const
     const double* Wb = W + (size_t)m0 * S;
     const int tc = tile_cols(S, SD);
     auto gemm = [&](int trans, const double* X, auto epi) -> int {
+      if (pr) return oz::gemm(ctx, *pr, trans, X, N, SD, tc, epi, st, launches);
       const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
       return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
     };
@@ -555,7 +557,8 @@ int infer(Context* ctx, cudaStream_t st, const double* A, const double* W, const
 // 2 (L - k') extra products (k' the last segment's length) and holds
 // ceil(L / k) + 4 k + 3 state slots of N x S D doubles instead of 4 (L + 1).
 int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const double* A, const double* Wb,
-               const double* Yb, const double* K, long long ldk, int N, int S, int D, int L, int* launches) {
+               const double* Yb, const double* K, long long ldk, int N, int S, int D, int L, int* launches,
+               const oz::Prepared* pr) {
   const int SD = S * D;
   const size_t NW = (size_t)N * SD, ND = (size_t)N * D;
   if (L <= 0) {
@@ -589,6 +592,7 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   auto seg_len = [&](int j) { return std::min(k, L - j * k); };
   const int tc = tile_cols(S, SD);
   auto gemm = [&](int trans, const double* X, auto epi) -> int {
+    if (pr) return oz::gemm(ctx, *pr, trans, X, N, SD, tc, epi, st, launches);
     const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
     return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
   };
@@ -634,6 +638,15 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   return 0;
 }
 
+// Whether the WDL products of an N x N kernel run on the INT8 tensor cores
+// (ozaki.cuh) rather than the FP64 ones: option "wdl.int8" 0 never, 2
+// whenever the device and size allow, 1 (default) from N = 1024 up.
+bool use_int8(Context* ctx, int N) {
+  const int o = (int)option("wdl.int8", 1.0);
+  if (o == 0 || N > oz::kMaxKd || !oz::available(ctx)) return false;
+  return o == 2 || N >= 1024;
+}
+
 int check_dims(int N, int S, int D) {
   if (N < 1 || S < 1 || D < 1) return set_error(RWIG_E_INVALID, "N, S and D must be >= 1");
   if (S > 64) return set_error(RWIG_E_UNSUPPORTED, "more than 64 topics");
@@ -670,8 +683,12 @@ int batch_grad_entry(Context* ctx, cudaStream_t st, double* gA, double* gl, cons
   rc = make_k(ctx, st, KorC, N, reg, mode, &K, &ldk);
   if (rc) return rc;
   int launches = 1;
-  rc = batch_grad(ctx, st, gA, gl, A, Wb, Yb, K, ldk, N, S, D, L, &launches);
+  oz::Prepared pr;
+  const bool i8 = use_int8(ctx, N) && L > 0;
+  if (i8 && (rc = oz::prepare(ctx, K, ldk, N, &pr, st, &launches))) return rc;
+  rc = batch_grad(ctx, st, gA, gl, A, Wb, Yb, K, ldk, N, S, D, L, &launches, i8 ? &pr : nullptr);
   if (rc) return rc;
+  if (i8 && (rc = oz::status(ctx, st))) return rc;
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
   float ms = 0.f;
@@ -790,6 +807,9 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   long long ldk = 0;
   int rc = make_k(ctx, st, dC, N, reg, 1, &K, &ldk);  // K = exp(-C/reg) (wdl_impl.cpp:297)
   if (rc) return rc;
+  oz::Prepared pr;  // K's residue planes, once for the whole training and inference
+  const bool i8 = use_int8(ctx, N);
+  if (i8 && (rc = oz::prepare(ctx, K, ldk, N, &pr, st, &launches))) return rc;
   col_softmax<<<S, TPB, 0, st>>>(dAl, N, dA);
   col_softmax<<<M, TPB, 0, st>>>(dLa, S, dW);
   launches += 3;
@@ -800,7 +820,7 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
       if (max_steps > 0 && steps >= max_steps) break;
       const int D = (bi == M / B) ? (M % B) : B;  // wdl_impl.cpp:91
       rc = batch_grad(ctx, st, gA, gl, dA, dW + (size_t)bi * B * S, dY + (size_t)bi * B * N, K, ldk, N, S, D,
-                      max_iter, &launches);
+                      max_iter, &launches, i8 ? &pr : nullptr);
       if (rc) return rc;
       ++steps;
       const double c1 = 1.0 - std::pow(beta1, steps), c2 = 1.0 - std::pow(beta2, steps);
@@ -820,6 +840,7 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   }
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev1, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (i8 && (rc = oz::status(ctx, st))) return rc;
   float train_ms = 0.f;
   cudaEventElapsedTime(&train_ms, ctx->ev0, ctx->ev1);
   if (A) RWIG_CUDA_TRY(cudaMemcpyAsync(A, dA, sizeof(double) * NS, cudaMemcpyDeviceToHost, st));
@@ -831,8 +852,9 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
     double* dYh = (double*)scratch(ctx, SW_YHAT, sizeof(double) * NM);
     if (!dYh) return RWIG_E_NOMEM;
     if (max_iter >= 1) {
-      rc = infer(ctx, st, dA, dW, K, ldk, N, S, M, max_iter, zero_tol, dYh, &launches);
+      rc = infer(ctx, st, dA, dW, K, ldk, N, S, M, max_iter, zero_tol, dYh, &launches, i8 ? &pr : nullptr);
       if (rc < 0) return rc;
+      if (i8 && (rc = oz::status(ctx, st))) return rc;
     } else {
       for (int m = 0; m < M; ++m) {
         rc = bary::run(ctx, st, false, nullptr, nullptr, dYh + (size_t)m * N, nullptr, nullptr, nullptr, nullptr,

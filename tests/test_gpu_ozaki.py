@@ -64,3 +64,39 @@ def test_emulated_fp64_product(n, W, trans, signed):
     assert err.max() <= 1e-14, err.max()
     if not signed:  # positive operands: no cancellation, relative to each entry
         assert (np.abs(Y - ref) / np.abs(ref)).max() <= 1e-13
+
+
+@pytest.mark.parametrize("trans", [0, 1])
+def test_emulated_product_with_cancellation(trans):
+    """Two identical support points make two identical columns of K; X's
+    columns e_0 (1 + 2^-52) - e_1 and e_0 - e_1 give products 2^-52 K[:, 0]
+    and exactly 0, far below the scale of the operands, where the
+    reconstruction needs all 256 bits of its fraction."""
+    import torch
+    g = np.random.default_rng(5)
+    n = 300
+    x = g.standard_normal((n, 8))
+    x[1] = x[0]
+    C = synth.sq_euclid_cost(x, x)
+    K = np.asfortranarray(np.exp(-C / 0.05))
+    X = np.zeros((n, 4), order="F")
+    X[0, 0], X[1, 0] = 1.0 + 2.0 ** -52, -1.0
+    X[0, 2], X[1, 2] = 1.0, -1.0
+    X[:, 1] = np.exp(g.uniform(-8, 8, n))
+    X[:, 3] = g.standard_normal(n)
+    d = torch.device("cuda:0")
+    tK = torch.from_numpy(np.ascontiguousarray(K.T)).to(d)
+    tX = torch.from_numpy(np.ascontiguousarray(X.T)).to(d)
+    tY = torch.zeros((4, n), dtype=torch.float64, device=d)
+    _lib.check(_lib.load().rwig_selftest_ozaki(_vp(tK), n, trans, n, _vp(tX), n, 4, _vp(tY), n, None))
+    Y = tY.cpu().numpy().T
+    op = K.T if trans else K
+    exact0 = op[:, 0] * 2.0 ** -52  # op[:, 0] == op[:, 1] exactly
+    assert np.array_equal(op[:, 0], op[:, 1])
+    assert np.abs(Y[:, 0] - exact0).max() <= 2.0 ** -52 * np.abs(exact0).max()
+    assert np.all(np.abs(Y[:, 0] - exact0) <= 2.0 ** -51 * np.abs(exact0))
+    assert not Y[:, 2].any()
+    ref = _exact(op, X)
+    for j in (1, 3):
+        err = np.abs(Y[:, j] - ref[:, j]) / (np.abs(op) @ np.abs(X[:, j]))
+        assert err.max() <= 1e-14, (j, err.max())

@@ -166,3 +166,34 @@ def test_checkpointed_training_matches_full_history():
                          Lambda0=L0)
     for k in ("A", "W", "Yhat"):
         assert np.array_equal(got[k], full[k]), k
+
+
+@pytest.mark.parametrize("N,D,S,L", [(200, 8, 4, 5), (333, 5, 16, 3), (257, 3, 64, 2), (100, 4, 5, 1),
+                                     (1100, 6, 8, 4)])
+def test_batch_grad_on_int8_tensor_cores_matches_oracle(N, D, S, L):
+    """wdl.int8 = 2: every product of the step emulated on the INT8 tensor
+    cores (24 modular planes, CRT); the gradient still within 1e-10 of the
+    oracle's, and bitwise repeatable."""
+    reg = 0.1
+    Y, C, K, A, W = _batch(N, D, S, 8, reg, salt=N + 2 * D)
+    ref_gA, ref_gl = oracle.wdl_batch_grad(A, W, Y, K, L)
+    with _Option("wdl.int8", 2):
+        gA, gl = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        again = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+    assert rel_err(gA, ref_gA) <= PARITY_TOL, rel_err(gA, ref_gA)
+    assert rel_err(gl, ref_gl) <= PARITY_TOL, rel_err(gl, ref_gl)
+    assert np.array_equal(again[0], gA) and np.array_equal(again[1], gl)
+
+
+def test_training_and_inference_on_int8_tensor_cores():
+    N, M, S, B, L, reg = 150, 10, 3, 4, 6, 0.1
+    Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=71)
+    ref = oracle.wdl_train(Y, C, S, reg, L, B, 3, A0, L0, opt=1, eta=5e-3, max_steps=4)
+    with _Option("wdl.int8", 2):
+        got = rw.wdl_cpp(Y, C, reg, S, B, 3, max_iter=L, zero_tol=1e-6, optimizer=1, eta=5e-3, Alpha0=A0,
+                         Lambda0=L0, max_steps=4)
+    assert rel_err(got["A"], ref["A"]) <= PARITY_TOL and rel_err(got["W"], ref["W"]) <= PARITY_TOL
+    for m in range(M):
+        b = oracle.barycenter_parallel(ref["A"], C, ref["W"][:, m], None, reg, with_grad=False, max_iter=L,
+                                       zero_tol=1e-6)["b"]
+        assert rel_err(got["Yhat"][:, m], b) <= 1e-9, m
