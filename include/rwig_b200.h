@@ -100,6 +100,12 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       modular integer products and CRT reconstruction), else on the FP64
  *       tensor cores; 2 on the INT8 tensor cores whenever N <= 8192; 0
  *       always on the FP64 tensor cores;
+ *   "wdl.halves": 2 (default) runs the two halves of the document batch of
+ *       an INT8-path WDL gradient on two streams (same gradient bits), 1 on
+ *       one stream;
+ *   "oz.tile_m": rows per tile of the INT8 GEMM: 256 (default; one
+ *       accumulator per CTA) or 128 (two accumulators, the MMAs of one tile
+ *       beside the epilogue of the last);
  *   "wdl.checkpoint": k > 0 keeps the WDL forward state only every k-th
  *       iteration plus one segment of k iterations and recomputes the other
  *       segments during the backward (same gradient bits; 2 (L - k) more

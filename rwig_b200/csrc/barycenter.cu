@@ -788,17 +788,8 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
   return status;
 }
 
-// Side stream i of the batched entry on this context's device, created on
-// first use (the caller holds ctx->mu and has ctx->device current).
+// Side streams of the batched entry: the context's (engine.h).
 constexpr int kSideStreams = Context::kSideStreams;
-cudaStream_t side_stream(Context* ctx, int i) {
-  cudaStream_t& q = ctx->side[i];
-  if (!q && cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess) {
-    (void)cudaGetLastError();
-    q = nullptr;
-  }
-  return q;
-}
 
 // First scratch slot of the solves enqueued on side stream i (clear of every
 // other entry's slot numbers).  Solves on one stream run in stream order, so

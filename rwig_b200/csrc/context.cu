@@ -42,6 +42,8 @@ int init_device(int dev, Context** out) {
     RWIG_CUDA_TRY(cudaEventCreate(&c->evk));
     RWIG_CUDA_TRY(cudaEventCreate(&c->evs0));
     RWIG_CUDA_TRY(cudaEventCreate(&c->evs1));
+    RWIG_CUDA_TRY(cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming));
+    RWIG_CUDA_TRY(cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming));
     g_ctx[dev] = std::move(c);
   }
   *out = g_ctx[dev].get();
@@ -56,7 +58,7 @@ const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "
                                    "batch.strip_kb", "batch.max_team", "batch.redundant_rows",
                                    "batch.l2_keep_mb", "batch.max_elems", "batch.resident_team",
                                    "batch.stream_strip_kb", "batch.backfill_us",
-                                   "wdl.infer_docs", "wdl.checkpoint", "wdl.int8", "dgemm.kshape", "dgemm.tile", "barycenter.log_path"};
+                                   "wdl.infer_docs", "wdl.checkpoint", "wdl.int8", "wdl.halves", "dgemm.kshape", "dgemm.tile", "barycenter.log_path", "oz.tile_m"};
 }  // namespace
 
 double option(const char* name, double dflt) {
@@ -93,6 +95,15 @@ Context* get_context() {
   }
   if (init_device(dev, &c) != 0) return nullptr;
   return c;
+}
+
+cudaStream_t side_stream(Context* ctx, int i) {
+  cudaStream_t& q = ctx->side[i];
+  if (!q && cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess) {
+    (void)cudaGetLastError();
+    q = nullptr;
+  }
+  return q;
 }
 
 void* scratch(Context* ctx, int k, size_t bytes) {
@@ -148,6 +159,8 @@ extern "C" void rwig_shutdown(void) {
     cudaEventDestroy(c->evk);
     cudaEventDestroy(c->evs0);
     cudaEventDestroy(c->evs1);
+    cudaEventDestroy(c->evfork);
+    cudaEventDestroy(c->evjoin);
     for (cudaStream_t& q : c->side)
       if (q) {
         cudaStreamSynchronize(q);

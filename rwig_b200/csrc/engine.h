@@ -28,6 +28,7 @@ struct Context {
   int smem_optin = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk = nullptr, evs0 = nullptr, evs1 = nullptr;
+  cudaEvent_t evfork = nullptr, evjoin = nullptr;  // ordering only (no timing)
   std::mutex mu;
   std::vector<void*> slots;
   std::vector<size_t> slot_bytes;
@@ -44,6 +45,11 @@ struct Context {
 // Returns the context of the current (or first) device, initialising it on
 // first use.  nullptr on failure (last error set).
 Context* get_context();
+
+// Side stream i (< Context::kSideStreams) of the context's device, created on
+// first use (the caller holds ctx->mu with the device current); nullptr on
+// failure.
+cudaStream_t side_stream(Context* ctx, int i);
 
 // Grow-only scratch slot `k` of at least `bytes`; nullptr on failure.
 void* scratch(Context* ctx, int k, size_t bytes);

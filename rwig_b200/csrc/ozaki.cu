@@ -2,18 +2,21 @@
 // (ozaki.cuh): reconstruction constants, scaling exponents, residues, and
 // the tcgen05 kind::i8 GEMM of the residue planes.
 //
-// GEMM kernel (one CTA per 128 x ntile output tile of one modulus, 128
+// GEMM kernel (one CTA per 256 x ntile output tile of one modulus, 256
 // threads):
-//   * operands are K-major int8 planes [T][rows][Kpad]; TMA (3-D tensor maps,
-//     128-byte swizzle) copies 128 x 128-byte A tiles and ntile x 128-byte B
-//     tiles into a 4-stage shared-memory ring, full / empty mbarriers;
-//   * thread 0 issues the copies, thread 32 the MMAs: per stage four
-//     tcgen05.mma.cta_group::1.kind::i8 of K = 32 (the shared-memory
-//     descriptors advanced by 32 bytes inside the swizzle atom) into an int32
-//     accumulator in tensor memory, then tcgen05.commit frees the stage;
-//   * the four warps read the accumulator back (tcgen05.ld 32x32b, warp w
-//     owns lanes 32w..32w+31 = rows), reduce it modulo p_t and store one byte
-//     per entry.
+//   * operands are K-major uint8 planes [T][rows][Kpad]; TMA (3-D tensor
+//     maps, 64-byte swizzle) copies 256 x 64-byte A tiles and ntile x 64-byte
+//     B tiles into a 6-stage shared-memory ring, full / empty mbarriers (a
+//     deep ring of small stages: the copies' latency, not the L2 bandwidth,
+//     bounds a shallower one);
+//   * thread 0 issues the copies, thread 32 the MMAs: per stage and per
+//     128-row half two tcgen05.mma.cta_group::1.kind::i8 of K = 32 (the
+//     shared-memory descriptors advanced by 32 bytes inside the swizzle
+//     atom) into int32 accumulators in tensor memory, then tcgen05.commit
+//     frees the stage;
+//   * the eight warps read the accumulators back (tcgen05.ld 32x32b, warp w
+//     owns lanes 32 (w % 4) .. +31 = rows of half w / 4), reduce them modulo
+//     p_t and store one byte per entry.
 // Every wait is bounded (2 s): a wait that runs out sets the error word and
 // the kernel winds down (the MMA thread still commits what it issued, the
 // tensor memory is freed), and the host reports RWIG_E_TIMEOUT.
@@ -302,12 +305,11 @@ __global__ void res_rows(const double* K, long long ldk, int n, const int* alpha
 // ---------------------------------------------------------------------------
 // the tcgen05 INT8 GEMM
 // ---------------------------------------------------------------------------
-constexpr int kStages = 3;
+constexpr int kStages = 6;
 constexpr int kCtaM = 2 * kTileM;      // two M = 128 accumulators per CTA: 256 rows
-constexpr int kAStage = kCtaM * kBk;   // 32 KB
-constexpr int kBStage = 256 * kBk;     // room for ntile <= 256: 32 KB
-constexpr int kGemmThreads = 256;
-constexpr size_t kGemmSmem = 1024 + (size_t)kStages * (kAStage + kBStage) + 256;
+constexpr int kAStage = kCtaM * kBk;   // 16 KB
+constexpr int kBStage = 256 * kBk;     // room for ntile <= 256: 16 KB
+constexpr size_t kGemmSmem = 1024 + (size_t)kStages * (kAStage + kBStage) + 256;  // + barriers and the TMEM slot
 
 struct I8Args {
   int Mpad, Wpad, Kpad, ntile, nk;
@@ -326,14 +328,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Shared-memory matrix descriptor of a K-major tile in the 128-byte swizzle
-// layout: start address >> 4, leading byte offset 16 (unused by this
-// layout), stride byte offset 1024 (eight 128-byte rows), descriptor version
-// 1, base offset 0 (tiles are 1024-byte aligned), layout type 2 (128B).
-__device__ __forceinline__ uint64_t sw128_desc(const void* p) {
+// Shared-memory matrix descriptor of a K-major tile in the 64-byte swizzle
+// layout (rows of 64 bytes, eight-row atoms of 512 bytes): start address
+// >> 4, leading byte offset 16 (unused by this layout), stride byte offset
+// 512 (eight 64-byte rows), descriptor version 1, base offset 0 (tiles are
+// 1024-byte aligned), layout type 4 (64B).
+__device__ __forceinline__ uint64_t sw64_desc(const void* p) {
   const uint32_t a = smem_u32(p);
-  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
 }
 
 // Instruction descriptor of kind::i8: int32 accumulator, A and B signed
@@ -371,28 +374,54 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// One CTA: a 256 x ntile output tile of residue plane z as two 128-row
-// accumulators in the 512 tensor-memory columns (half h at column 256 h).
-template <bool RAW>
-__global__ void __launch_bounds__(kGemmThreads, 1) i8_gemm(const __grid_constant__ CUtensorMap ta,
-                                                           const __grid_constant__ CUtensorMap tb, I8Args g) {
+__device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent: one CTA per SM walks the tiles blockIdx.x, + gridDim.x, ...
+// (column tiles fastest, then row tiles, then residue planes).  A tile is MT
+// x ntile of the output, accumulated in tensor memory as MT / 128 row halves
+// of 128 lanes; MT = 256 holds one tile in the 512 columns (half h at column
+// 256 h), MT = 128 holds two (buffer b at column 256 b), so that the MMAs of
+// the next tile run while the epilogue drains the last one.  Warp 0 (one
+// thread) issues the copies, warp 1 (one thread) the MMAs, warps 2..9 read
+// the accumulators back (warp w reaches tensor-memory lanes 32 (w % 4) ..
+// +31).  The copy ring runs on across tiles (a global k-block count keeps its
+// barrier phases); tfull[b] / tempty[b] hand accumulator buffer b between
+// the MMA thread and the epilogue warps.
+constexpr int kEpiWarps = 8;
+constexpr int kPersistThreads = 64 + 32 * kEpiWarps;
+
+template <bool RAW, int MT>
+__global__ void __launch_bounds__(kPersistThreads, 1) i8_gemm(const __grid_constant__ CUtensorMap ta,
+                                                              const __grid_constant__ CUtensorMap tb, I8Args g,
+                                                              int ntn, int ntm, int planes) {
+  constexpr int kHalves = MT / kTileM;
+  constexpr int kBufs = 2 / kHalves;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* sA = base;
   uint8_t* sB = base + (size_t)kStages * kAStage;
   uint64_t* full = reinterpret_cast<uint64_t*>(sB + (size_t)kStages * kBStage);
   uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* tfull = empty + kStages;  // [kBufs]
+  uint64_t* tempty = tfull + 2;       // [kBufs]
+  uint64_t* fin = tempty + 2;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * g.ntile, m0 = blockIdx.y * kCtaM, z = blockIdx.z;
   constexpr uint32_t ncols = 512;
+  const int tiles = ntn * ntm * planes;
+  const uint32_t stage_bytes = (uint32_t)(MT * kBk + g.ntile * kBk);
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < kBufs; ++b) {
+      mbar_init(tfull + b, 1);
+      mbar_init(tempty + b, kEpiWarps);
+    }
+    mbar_init(fin, 1);
     fence_mbar_init();
   }
   if (warp == 0) {
@@ -405,73 +434,111 @@ __global__ void __launch_bounds__(kGemmThreads, 1) i8_gemm(const __grid_constant
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t stage_bytes = (uint32_t)(kAStage + g.ntile * kBk);
 
-  if (warp == 0 && lane == 0) {  // copies
-    int issued = 0;
-    for (int kb = 0; kb < g.nk; ++kb) {
-      const int s = kb % kStages;
-      if (kb >= kStages && !mbar_wait_bounded(empty + s, ((kb / kStages) - 1) & 1)) {
-        atomicOr(g.err, KERR_MBAR_TIMEOUT);
-        break;
+  if (warp == 0) {
+    if (lane == 0) {  // copies
+      long long kbg = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x) {
+        const int n0 = (tile % ntn) * g.ntile, m0 = ((tile / ntn) % ntm) * MT, z = tile / (ntn * ntm);
+        for (int kb = 0; kb < g.nk; ++kb, ++kbg) {
+          const int s = (int)(kbg % kStages);
+          if (kbg >= kStages && !mbar_wait_bounded(empty + s, (unsigned)((kbg / kStages) - 1) & 1)) {
+            atomicOr(g.err, KERR_MBAR_TIMEOUT);
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(full + s, stage_bytes);
+          tma_load_3d(sA + (size_t)s * kAStage, &ta, kb * kBk, m0, z, full + s);
+          tma_load_3d(sB + (size_t)s * kBStage, &tb, kb * kBk, n0, z, full + s);
+        }
       }
-      mbar_arrive_expect_tx(full + s, stage_bytes);
-      tma_load_3d(sA + (size_t)s * kAStage, &ta, kb * kBk, m0, z, full + s);
-      tma_load_3d(sB + (size_t)s * kBStage, &tb, kb * kBk, n0, z, full + s);
-      ++issued;
+      // the copies of the last use of each stage land before the CTA leaves
+      for (long long u = std::max(0LL, kbg - kStages); u < kbg; ++u)
+        if (!mbar_wait_bounded(full + u % kStages, (unsigned)(u / kStages) & 1)) atomicOr(g.err, KERR_MBAR_TIMEOUT);
     }
-    // copies still in flight when the loop stopped early complete before exit
-    for (int kb = std::max(0, issued - kStages); kb < issued; ++kb)
-      if (issued < g.nk && !mbar_wait_bounded(full + kb % kStages, (kb / kStages) & 1)) atomicOr(g.err, KERR_MBAR_TIMEOUT);
-  } else if (warp == 1 && lane == 0) {  // MMAs
-    const uint32_t idesc = i8_idesc(g.ntile, g.sgn);
-    for (int kb = 0; kb < g.nk; ++kb) {
-      const int s = kb % kStages;
-      if (!mbar_wait_bounded(full + s, (kb / kStages) & 1)) {
-        atomicOr(g.err, KERR_MBAR_TIMEOUT);
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMAs
+      const uint32_t idesc = i8_idesc(g.ntile, g.sgn);
+      long long kbg = 0;
+      int it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x, ++it) {
+        const int b = it % kBufs, use = it / kBufs;
+        if (use > 0 && !mbar_wait_bounded(tempty + b, (unsigned)(use - 1) & 1)) {  // buffer b drained
+          atomicOr(g.err, KERR_MBAR_TIMEOUT);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = tmem + (uint32_t)(256 * b);
+        for (int kb = 0; kb < g.nk; ++kb, ++kbg) {
+          const int s = (int)(kbg % kStages);
+          if (!mbar_wait_bounded(full + s, (unsigned)(kbg / kStages) & 1)) {
+            atomicOr(g.err, KERR_MBAR_TIMEOUT);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint8_t* a = sA + (size_t)s * kAStage;
+          const uint8_t* bb = sB + (size_t)s * kBStage;
+#pragma unroll
+          for (int h = 0; h < kHalves; ++h)
+#pragma unroll
+            for (int kk = 0; kk < kBk / 32; ++kk)
+              tc_mma(acc + (uint32_t)(256 * h), sw64_desc(a + h * (kTileM * kBk) + kk * 32), sw64_desc(bb + kk * 32),
+                     idesc, (kb | kk) != 0);
+          tc_commit(empty + s);  // the stage is free once these MMAs have read it
+        }
+        if (ok) tc_commit(tfull + b);  // this tile's accumulators are complete
+      }
+      // every MMA issued has completed before the tensor memory is freed
+      tc_commit(fin);
+      if (!mbar_wait_bounded(fin, 0)) atomicOr(g.err, KERR_MBAR_TIMEOUT);
+    }
+  } else {  // epilogue warps
+    const int ew = warp - 2, lq = warp & 3;
+    const int h = kHalves == 2 ? ew >> 2 : 0;
+    const int cfirst = kHalves == 2 ? 0 : (ew >> 2) * 32, cstep = kHalves == 2 ? 32 : 64;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+      const int n0 = (tile % ntn) * g.ntile, m0 = ((tile / ntn) % ntm) * MT, z = tile / (ntn * ntm);
+      const int b = it % kBufs;
+      const unsigned par = (unsigned)(it / kBufs) & 1;
+      bool have = mbar_try_wait(tfull + b, par);
+      if (!have) {
+        const unsigned long long t0 = globaltimer_ns();
+        while (!(have = mbar_try_wait(tfull + b, par)) && globaltimer_ns() - t0 <= kWaitLimitNs) __nanosleep(100);
+      }
+      if (!have) {
+        if (lane == 0) atomicOr(g.err, KERR_MBAR_TIMEOUT);
         break;
       }
       tc_fence_after();
-      const uint8_t* a = sA + (size_t)s * kAStage;
-      const uint8_t* b = sB + (size_t)s * kBStage;
+      const int i = m0 + h * kTileM + lq * 32 + lane;  // output row
+      const unsigned p = RAW ? 1u : (unsigned)g.m.p[z];
+      const double invp = RAW ? 1.0 : g.m.invp[z];
+      const uint32_t acc = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(256 * (b + h));
+      for (int c = cfirst; c < g.ntile; c += cstep) {
+        uint32_t v[32];
+        tc_ld32(acc + (uint32_t)c, v);
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int kk = 0; kk < kBk / 32; ++kk)
-          tc_mma(tmem + (uint32_t)(256 * h), sw128_desc(a + h * (kTileM * kBk) + kk * 32), sw128_desc(b + kk * 32),
-                 idesc, (kb | kk) != 0);
-      tc_commit(empty + s);  // the stage is free once these MMAs have read it
-    }
-    tc_commit(done);  // everything issued has completed
-  }
-  __syncwarp();
-
-  const bool have = mbar_wait_bounded(done, 0);
-  tc_fence_after();
-  if (!have) {
-    if (threadIdx.x == 0) atomicOr(g.err, KERR_MBAR_TIMEOUT);
-  } else if ((*(volatile unsigned*)g.err & KERR_MBAR_TIMEOUT) == 0) {
-    const int h = warp >> 2, lq = warp & 3;                // accumulator half, tensor-memory lane quarter
-    const int i = m0 + h * kTileM + lq * 32 + lane;         // output row
-    const unsigned p = RAW ? 1u : (unsigned)g.m.p[z];
-    const double invp = RAW ? 1.0 : g.m.invp[z];
-    for (int c = 0; c < g.ntile; c += 32) {
-      uint32_t v[32];
-      tc_ld32(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(256 * h + c), v);
-#pragma unroll
-      for (int q = 0; q < 32; ++q) {
-        if (c + q >= g.ntile) break;  // columns of the last load beyond the tile
-        const int j = n0 + c + q;
-        const int d = (int)v[q];
-        if (RAW) {
-          g.raw[(size_t)j * g.Mpad + i] = d;
-        } else {
-          int r = d - (int)floor((double)d * invp) * (int)p;
-          if (r < 0) r += (int)p;
-          if (r >= (int)p) r -= (int)p;
-          g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)r;
+        for (int q = 0; q < 32; ++q) {
+          if (c + q >= g.ntile) break;  // columns of the last load beyond the tile
+          const int j = n0 + c + q;
+          const int d = (int)v[q];
+          if (RAW) {
+            g.raw[(size_t)j * g.Mpad + i] = d;
+          } else {
+            int r = d - (int)floor((double)d * invp) * (int)p;
+            if (r < 0) r += (int)p;
+            if (r >= (int)p) r -= (int)p;
+            g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)r;
+          }
         }
       }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_local(tempty + b);  // this warp is done with buffer b
     }
   }
   tc_fence_before();
@@ -504,7 +571,8 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 3-D map over int8 planes [planes][rows][Kpad], boxes of 128 bytes x box_rows x 1.
+// 3-D map over int8 planes [planes][rows][Kpad], boxes of kBk bytes x box_rows x 1
+// in the 64-byte swizzle layout.
 int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return set_error(RWIG_E_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
@@ -513,7 +581,7 @@ int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes,
   const cuuint32_t box[3] = {(cuuint32_t)kBk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(RWIG_E_CUDA, "cuTensorMapEncodeTiled failed");
   return 0;
@@ -522,7 +590,11 @@ int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes,
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 int pick_ntile(int W) { return std::min(256, round_up(std::max(W, 16), 16)); }
 
-enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_BRES, SO_BETA, SO_CRES, SO_ERR, SO_TA, SO_TB, SO_TD, SO_Y };
+enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_ERR, SO_TA, SO_TB, SO_TD };
+// per-lane scratch of the product pipeline: lanes are products in flight on
+// different streams at once
+enum { SO_LANE = 420, SO_BRES = 0, SO_BETA, SO_CRES, SO_Y, SO_PER_LANE = 4 };
+int lane_slot(int lane, int k) { return SO_LANE + SO_PER_LANE * lane + k; }
 
 // The kT (or, RAW, one) planes of A (Mpad x Kpad) and B (Wpad x Kpad): the
 // int8 products into cres (or raw).
@@ -530,8 +602,6 @@ template <bool RAW>
 int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad, int Kpad, int ntile, int planes,
               uint8_t* cres, int* raw, cudaStream_t st) {
   CUtensorMap ta, tb;
-  if (int rc = make_map(&ta, A, Kpad, Mpad, planes, kCtaM)) return rc;
-  if (int rc = make_map(&tb, B, Kpad, Wpad, planes, ntile)) return rc;
   unsigned* err = (unsigned*)scratch(ctx, SO_ERR, sizeof(unsigned) * 4);  // cleared by reset_err()
   if (!err) return RWIG_E_NOMEM;
   I8Args g{};
@@ -545,13 +615,28 @@ int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad
   g.raw = raw;
   g.err = err;
   g.m = mods_of(crt_constants());
-  static bool attr = false;
-  if (!attr) {
-    RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-    attr = true;
+  // 256-row tiles (one accumulator) by default: measured faster than 128-row
+  // tiles with two accumulators on the 5000 x 1024 products; option "oz.tile_m".
+  const int tm_opt = (int)option("oz.tile_m", 0.0);
+  const int MT = tm_opt == 128 || tm_opt == 256 ? tm_opt : 256;
+  if (int rc = make_map(&ta, A, Kpad, Mpad, planes, MT)) return rc;
+  if (int rc = make_map(&tb, B, Kpad, Wpad, planes, ntile)) return rc;
+  static bool attr[2] = {false, false};
+  const int ntn = Wpad / ntile, ntm = Mpad / MT, tiles = ntn * ntm * planes;
+  const int grid = std::min(tiles, ctx->sm_count);  // persistent: one CTA per SM
+  if (MT == 256) {
+    if (!attr[0]) {
+      RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+      attr[0] = true;
+    }
+    i8_gemm<RAW, 256><<<grid, kPersistThreads, kGemmSmem, st>>>(ta, tb, g, ntn, ntm, planes);
+  } else {
+    if (!attr[1]) {
+      RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+      attr[1] = true;
+    }
+    i8_gemm<RAW, 128><<<grid, kPersistThreads, kGemmSmem, st>>>(ta, tb, g, ntn, ntm, planes);
   }
-  const dim3 grid(Wpad / ntile, Mpad / kCtaM, planes);
-  i8_gemm<RAW><<<grid, kGemmThreads, kGemmSmem, st>>>(ta, tb, g);
   RWIG_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -585,7 +670,7 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
   pr->ldk = ldk;
   pr->Mo = pr->Kd = n;
   pr->Mpad = round_up(n, kCtaM);
-  pr->Kpad = round_up(n, kBk);
+  pr->Kpad = round_up(n, kKpadTo);
   const size_t planes = (size_t)kT * pr->Mpad * pr->Kpad;
   const Mods m = mods_of(crt_constants());
   if (int rc = reset_err(ctx, st)) return rc;
@@ -608,13 +693,13 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
 }
 
 int products(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, cudaStream_t st,
-             const uint8_t** cres, const int** beta, int* Wpad_out, int* launches) {
+             const uint8_t** cres, const int** beta, int* Wpad_out, int* launches, int lane) {
   if (W < 1 || !X) return set_error(RWIG_E_INVALID, "INT8 product path: empty operand");
   const int ntile = pick_ntile(W);
   const int Wpad = round_up(W, ntile);
-  int8_t* bres = (int8_t*)scratch(ctx, SO_BRES, (size_t)kT * Wpad * pr.Kpad);
-  int* be = (int*)scratch(ctx, SO_BETA, sizeof(int) * W);
-  uint8_t* cr = (uint8_t*)scratch(ctx, SO_CRES, (size_t)kT * Wpad * pr.Mpad);
+  int8_t* bres = (int8_t*)scratch(ctx, lane_slot(lane, SO_BRES), (size_t)kT * Wpad * pr.Kpad);
+  int* be = (int*)scratch(ctx, lane_slot(lane, SO_BETA), sizeof(int) * W);
+  uint8_t* cr = (uint8_t*)scratch(ctx, lane_slot(lane, SO_CRES), (size_t)kT * Wpad * pr.Mpad);
   if (!bres || !be || !cr) return RWIG_E_NOMEM;
   const Mods m = mods_of(crt_constants());
   exp_cols<<<W, 256, 0, st>>>(X, ldx, pr.Kd, be);
@@ -716,7 +801,9 @@ int reconstruct(Context* ctx, const Prepared& pr, int trans, const uint8_t* cres
   return 0;
 }
 
-double* product_buffer(Context* ctx, size_t doubles) { return (double*)scratch(ctx, SO_Y, sizeof(double) * doubles); }
+double* product_buffer(Context* ctx, size_t doubles, int lane) {
+  return (double*)scratch(ctx, lane_slot(lane, SO_Y), sizeof(double) * doubles);
+}
 
 // Bounded-wait status of the last products() launches (a host read).
 int status(Context* ctx, cudaStream_t st) { return check_err(ctx, st); }
@@ -739,7 +826,7 @@ extern "C" int rwig_selftest_i8gemm(const signed char* A, const signed char* B, 
   if (!oz::available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 tensor-core GEMM unavailable");
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
   const int ntile = oz::pick_ntile(N), Mpad = oz::round_up(M, oz::kCtaM), Npad = oz::round_up(N, ntile);
-  const int Kpad = oz::round_up(Kd, oz::kBk);
+  const int Kpad = oz::round_up(Kd, oz::kKpadTo);
   int8_t* a = (int8_t*)scratch(ctx, oz::SO_TA, (size_t)Mpad * Kpad);
   int8_t* b = (int8_t*)scratch(ctx, oz::SO_TB, (size_t)Npad * Kpad);
   int* d = (int*)scratch(ctx, oz::SO_TD, sizeof(int) * (size_t)Mpad * Npad);

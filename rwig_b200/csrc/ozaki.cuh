@@ -45,8 +45,9 @@ constexpr int kT = 24;        // moduli
 constexpr int kQ = 85;        // bits of the scaled integers
 constexpr int kMaxKd = 8192;  // contraction length for which kQ is safe: Kd 2^(2 kQ) < P / 2
 constexpr int kTileM = 128;   // UMMA M
-constexpr int kBk = 128;      // bytes of K per pipeline stage (one 128-byte swizzle atom)
-constexpr int kCrtRows = 32;  // rows per epilogue tile
+constexpr int kBk = 64;       // bytes of K per pipeline stage (one 64-byte swizzle atom)
+constexpr int kKpadTo = 128;  // the contraction is padded to a multiple of this
+constexpr int kCrtRows = 16;  // rows per epilogue tile (26 KB of shared memory: fits beside a GEMM CTA)
 constexpr int kCrtCols = 64;  // most columns per epilogue tile (the DMMA GEMM's widest tile)
 constexpr int kCrtThreads = 256;
 
@@ -79,9 +80,10 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
 
 // X's residues and the kT integer products: cres[t][j][i] = (A_t X_t)_ij mod
 // p_t for i < Mo, j < W (pitch Mpad per column, Wpad columns per modulus),
-// beta (W ints).  Returns 0 or an engine error.
+// beta (W ints), in the scratch of `lane` (products on different streams at
+// once use different lanes).  Returns 0 or an engine error.
 int products(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, cudaStream_t st,
-             const uint8_t** cres, const int** beta, int* Wpad, int* launches);
+             const uint8_t** cres, const int** beta, int* Wpad, int* launches, int lane);
 
 // Status of the bounded waits of the INT8 GEMMs enqueued on `st` since
 // prepare() (synchronises): 0 or RWIG_E_TIMEOUT.
@@ -96,8 +98,8 @@ bool available(Context* ctx);
 int reconstruct(Context* ctx, const Prepared& pr, int trans, const uint8_t* cres, int Wpad, const int* beta, int W,
                 double* Y, long long ldy, cudaStream_t st, int* launches);
 
-// Scratch for the FP64 product of `products` (Mo x W doubles).
-double* product_buffer(Context* ctx, size_t doubles);
+// Scratch of `lane` for the FP64 product (Mo x W doubles).
+double* product_buffer(Context* ctx, size_t doubles, int lane);
 
 // Tiles of kCrtRows x tc of Y handed to the epilogue (the dgemm.cuh
 // contract: value (r0 + r, c0 + c) at t[c * ldt + r], columns >= W zero,
@@ -126,12 +128,12 @@ inline size_t epi_smem_bytes() { return sizeof(double) * (size_t)(kCrtCols + 2 *
 // columns).  *launches += the kernels launched.
 template <class Epi>
 int gemm(Context* ctx, const Prepared& pr, int trans, const double* X, long long ldx, int W, int tc, const Epi& epi,
-         cudaStream_t st, int* launches) {
+         cudaStream_t st, int* launches, int lane = 0) {
   const uint8_t* cres = nullptr;
   const int* beta = nullptr;
   int Wpad = 0;
-  if (int rc = products(ctx, pr, trans, X, ldx, W, st, &cres, &beta, &Wpad, launches)) return rc;
-  double* Y = product_buffer(ctx, (size_t)pr.Mo * W);
+  if (int rc = products(ctx, pr, trans, X, ldx, W, st, &cres, &beta, &Wpad, launches, lane)) return rc;
+  double* Y = product_buffer(ctx, (size_t)pr.Mo * W, lane);
   if (!Y) return RWIG_E_NOMEM;
   if (int rc = reconstruct(ctx, pr, trans, cres, Wpad, beta, W, Y, pr.Mo, st, launches)) return rc;
   if (tc <= 0 || tc > kCrtCols) tc = kCrtCols;

@@ -570,6 +570,11 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   const int k = (kopt <= 0 || kopt >= L) ? L : kopt;  // segment length
   const int nseg = (L + k - 1) / k;
   const int ngrp = (N + 7) / 8;
+  // With the products on the INT8 tensor cores the batch's documents run as
+  // two independent halves on two streams, so that one half's tensor-core
+  // products overlap the other half's residue, reconstruction and epilogue
+  // kernels (the documents of a batch share nothing until the final means).
+  const int halves = (pr && D >= 2 && (int)option("wdl.halves", 2.0) >= 2) ? 2 : 1;
   // segment buffers, local index t = l - j k (t = 0..k); V's slot 0 is the checkpoint
   double* Us = (double*)scratch(ctx, SW_UH, sizeof(double) * NW * (k + 1));
   double* Vs = (double*)scratch(ctx, SW_VH, sizeof(double) * NW * (k + 1));
@@ -580,60 +585,86 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   double* T = (double*)scratch(ctx, SW_T, sizeof(double) * NW);
   double* T2 = (double*)scratch(ctx, SW_T2, sizeof(double) * NW);
   double* AB = (double*)scratch(ctx, SW_AB, sizeof(double) * NW);
-  double* gwp = (double*)scratch(ctx, SW_GWP, sizeof(double) * (size_t)ngrp * SD);
+  double* gwp = (double*)scratch(ctx, SW_GWP, sizeof(double) * (size_t)ngrp * SD);  // per half: [ngrp][W_h]
   double* dot = (double*)scratch(ctx, SW_DOT, sizeof(double) * SD);
   double* wbar = (double*)scratch(ctx, SW_WBAR, sizeof(double) * SD);
   if (!Us || !Vs || !KVs || !KTs || !Bs || !Vck || !T || !T2 || !AB || !gwp || !dot || !wbar) return RWIG_E_NOMEM;
-  auto U = [&](int t) { return Us + NW * t; };
-  auto V = [&](int j, int t) { return t == 0 ? Vck + NW * j : Vs + NW * t; };
-  auto KV = [&](int t) { return KVs + NW * t; };
-  auto KT = [&](int t) { return KTs + NW * t; };
-  auto Bb = [&](int t) { return Bs + ND * t; };
+  cudaStream_t qs[2] = {st, st};
+  if (halves == 2) {
+    qs[1] = side_stream(ctx, 0);
+    if (!qs[1]) return set_error(RWIG_E_CUDA, "could not create a side stream");
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->evfork, st));
+    RWIG_CUDA_TRY(cudaStreamWaitEvent(qs[1], ctx->evfork, 0));
+  }
   auto seg_len = [&](int j) { return std::min(k, L - j * k); };
-  const int tc = tile_cols(S, SD);
-  auto gemm = [&](int trans, const double* X, auto epi) -> int {
-    if (pr) return oz::gemm(ctx, *pr, trans, X, N, SD, tc, epi, st, launches);
-    const dg::GemmArgs g{K, ldk, N, N, SD, X, N, 0, tc};
-    return trans ? dg::gemm<1>(ctx, g, epi, st, 0, launches) : dg::gemm<0>(ctx, g, epi, st, 0, launches);
-  };
-  // forward iterations j k .. j k + len - 1 (wdl_impl.cpp:124-160)
-  auto forward_segment = [&](int j) -> int {
-    for (int t = 0; t < seg_len(j); ++t) {
-      if (int rc = gemm(0, V(j, t), EpiY{A, N, S, SD, KV(t), U(t + 1)})) return rc;
-      if (int rc = gemm(1, U(t + 1), EpiZ{Wb, N, S, SD, KT(t + 1), V(j, t + 1), Bb(t + 1)})) return rc;
+  // one half: documents [d0, d1), columns [c0, c0 + Wh) of every buffer
+  auto run_half = [&](int h, int d0, int d1) -> int {
+    cudaStream_t q = qs[h];
+    const int c0 = d0 * S, Wh = (d1 - d0) * S;
+    const size_t o = (size_t)N * c0, od = (size_t)N * d0;
+    double* gw = gwp + (size_t)ngrp * c0;  // [ngrp][Wh]
+    auto U = [&](int t) { return Us + NW * t + o; };
+    auto V = [&](int j, int t) { return (t == 0 ? Vck + NW * j : Vs + NW * t) + o; };
+    auto KV = [&](int t) { return KVs + NW * t + o; };
+    auto KT = [&](int t) { return KTs + NW * t + o; };
+    auto Bb = [&](int t) { return Bs + ND * t + od; };
+    const int tc = tile_cols(S, Wh);
+    auto gemm = [&](int trans, const double* X, auto epi) -> int {
+      if (pr) return oz::gemm(ctx, *pr, trans, X, N, Wh, tc, epi, q, launches, h);
+      const dg::GemmArgs g{K, ldk, N, N, Wh, X, N, 0, tc};
+      return trans ? dg::gemm<1>(ctx, g, epi, q, 0, launches) : dg::gemm<0>(ctx, g, epi, q, 0, launches);
+    };
+    const double* Wbh = Wb + c0;
+    // forward iterations j k .. j k + len - 1 (wdl_impl.cpp:124-160)
+    auto forward_segment = [&](int j) -> int {
+      for (int t = 0; t < seg_len(j); ++t) {
+        if (int rc = gemm(0, V(j, t), EpiY{A, N, S, Wh, KV(t), U(t + 1)})) return rc;
+        if (int rc = gemm(1, U(t + 1), EpiZ{Wbh, N, S, Wh, KT(t + 1), V(j, t + 1), Bb(t + 1)})) return rc;
+      }
+      return 0;
+    };
+    fill<<<grid_for(ctx, (long long)N * Wh), TPB, 0, q>>>(V(0, 0), (long long)N * Wh, 1.0);
+    ++*launches;
+    int rc;
+    for (int j = 0; j < nseg; ++j) {
+      if ((rc = forward_segment(j))) return rc;
+      if (j + 1 < nseg)  // VB_{(j+1) k}, the next segment's checkpoint
+        RWIG_CUDA_TRY(
+            cudaMemcpyAsync(V(j + 1, 0), V(j, k), sizeof(double) * N * Wh, cudaMemcpyDeviceToDevice, q));
     }
+    RWIG_CUDA_TRY(cudaMemsetAsync(AB + o, 0, sizeof(double) * N * Wh, q));
+    RWIG_CUDA_TRY(cudaMemsetAsync(gw, 0, sizeof(double) * (size_t)ngrp * Wh, q));
+    for (int j = nseg - 1; j >= 0; --j) {  // :169-218, segments newest first
+      if (j != nseg - 1 && (rc = forward_segment(j))) return rc;  // recompute from VB_{j k}
+      for (int t = seg_len(j); t >= 1; --t) {
+        const bool seed = (j * k + t == L);
+        const EpiB1 e1{KT(t), V(j, t), Wbh, Bb(t), Yb + od, N, S, Wh, seed ? 1 : 0, T2 + o, gw};
+        if (seed) {
+          dim3 grid(ngrp, (Wh + tc - 1) / tc);
+          seed_b1<<<grid, TPB, sizeof(double) * 2 * tc * 8, q>>>(e1, N, tc);
+          ++*launches;
+        } else {
+          if ((rc = gemm(1, T + o, e1))) return rc;  // K^T T
+        }
+        if ((rc = gemm(0, T2 + o, EpiB2{U(t), KV(t - 1), N, Wh, AB + o, T + o}))) return rc;  // K T2
+      }
+    }
+    reduce_cols<<<Wh, TPB, 0, q>>>(gw, ngrp, Wh, wbar + c0);
+    ++*launches;
+    RWIG_CUDA_TRY(cudaGetLastError());
     return 0;
   };
-  fill<<<grid_for(ctx, NW), TPB, 0, st>>>(V(0, 0), NW, 1.0);
-  ++*launches;
-  int rc;
-  for (int j = 0; j < nseg; ++j) {
-    if ((rc = forward_segment(j))) return rc;
-    if (j + 1 < nseg)  // VB_{(j+1) k}, the next segment's checkpoint
-      RWIG_CUDA_TRY(cudaMemcpyAsync(V(j + 1, 0), V(j, k), sizeof(double) * NW, cudaMemcpyDeviceToDevice, st));
-  }
-  RWIG_CUDA_TRY(cudaMemsetAsync(AB, 0, sizeof(double) * NW, st));
-  RWIG_CUDA_TRY(cudaMemsetAsync(gwp, 0, sizeof(double) * (size_t)ngrp * SD, st));
-  for (int j = nseg - 1; j >= 0; --j) {  // :169-218, segments newest first
-    if (j != nseg - 1 && (rc = forward_segment(j))) return rc;  // recompute from VB_{j k}
-    for (int t = seg_len(j); t >= 1; --t) {
-      const bool seed = (j * k + t == L);
-      const EpiB1 e1{KT(t), V(j, t), Wb, Bb(t), Yb, N, S, SD, seed ? 1 : 0, T2, gwp};
-      if (seed) {
-        dim3 grid(ngrp, (SD + tc - 1) / tc);
-        seed_b1<<<grid, TPB, sizeof(double) * 2 * tc * 8, st>>>(e1, N, tc);
-        ++*launches;
-      } else {
-        if ((rc = gemm(1, T, e1))) return rc;  // K^T T
-      }
-      if ((rc = gemm(0, T2, EpiB2{U(t), KV(t - 1), N, SD, AB, T}))) return rc;  // K T2
-    }
+  const int dsplit = halves == 2 ? D / 2 : D;
+  if (int rc = run_half(0, 0, dsplit)) return rc;
+  if (halves == 2) {
+    if (int rc = run_half(1, dsplit, D)) return rc;
+    RWIG_CUDA_TRY(cudaEventRecord(ctx->evjoin, qs[1]));
+    RWIG_CUDA_TRY(cudaStreamWaitEvent(st, ctx->evjoin, 0));
   }
   col_dots<<<SD, TPB, 0, st>>>(A, AB, N, S, dot);
   alpha_grad<<<grid_for(ctx, (long long)N * S), TPB, 0, st>>>(A, AB, dot, N, S, D, gA);
-  reduce_cols<<<SD, TPB, 0, st>>>(gwp, ngrp, SD, wbar);
   lambda_grad<<<1, TPB, 0, st>>>(Wb, wbar, S, D, gl);
-  *launches += 4;
+  *launches += 3;
   RWIG_CUDA_TRY(cudaGetLastError());
   return 0;
 }

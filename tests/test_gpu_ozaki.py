@@ -21,9 +21,12 @@ def _vp(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+@pytest.mark.parametrize("tile_m", [0, 128, 256])
 @pytest.mark.parametrize("M,N,Kd", [(128, 16, 128), (256, 256, 512), (200, 40, 300), (1000, 300, 5000),
                                     (5000, 1024, 256), (130, 257, 129)])
-def test_int8_gemm_is_exact(M, N, Kd):
+def test_int8_gemm_is_exact(M, N, Kd, tile_m):
+    """Both tile shapes (256 rows with one accumulator, 128 rows with two)
+    and the default choice; persistent CTAs walk several tiles each."""
     import torch
     g = np.random.default_rng(M + N + Kd)
     A = g.integers(-128, 128, size=(M, Kd), dtype=np.int8)
@@ -31,7 +34,12 @@ def test_int8_gemm_is_exact(M, N, Kd):
     d = torch.device("cuda:0")
     tA, tB = torch.from_numpy(A).to(d), torch.from_numpy(B).to(d)
     tD = torch.zeros((N, M), dtype=torch.int32, device=d)
-    _lib.check(_lib.load().rwig_selftest_i8gemm(_vp(tA), _vp(tB), M, N, Kd, _vp(tD), None))
+    lib = _lib.load()
+    lib.rwig_set_option(b"oz.tile_m", float(tile_m) if tile_m else float("nan"))
+    try:
+        _lib.check(lib.rwig_selftest_i8gemm(_vp(tA), _vp(tB), M, N, Kd, _vp(tD), None))
+    finally:
+        lib.rwig_set_option(b"oz.tile_m", float("nan"))
     ref = A.astype(np.int64) @ B.astype(np.int64).T
     assert np.array_equal(tD.cpu().numpy().T.astype(np.int64), ref)
 
