@@ -360,6 +360,34 @@ def measured_dgemm_tflops(dev):
     return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
+def measured_i8gemm_tops(dev):
+    """cuBLASLt INT8 GEMM throughput on this GPU (torch._int_mm, int8 operands,
+    int32 result, 8192^3, best of 5) in TOP/s: the denominator for the INT8
+    tensor-core GEMM of the emulated FP64 products; None if torch has no
+    INT8 GEMM here."""
+    import torch
+    n = 8192
+    try:
+        a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev)
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+    except (RuntimeError, AttributeError):
+        return None
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
 class BarycenterWorkload:
     """One log-barycenter solve with its gradient per step (fixed L iterations)."""
 
@@ -1032,7 +1060,10 @@ class StreamWorkload:
                "steps_timed": steps, "ms_per_step": rep["device_ms"] / steps,
                "roofline": {"bound": "tensor", "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
                             "frac": achieved / tf_peak, "flops_per_step": wl.step_flops(),
-                            "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU"},
+                            "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
+                            "note": "FP64-equivalent rate: the step's products counted as FP64 GEMM flops over "
+                                    "the FP64 tensor-core peak; the products run emulated on the INT8 tensor "
+                                    "cores, so frac > 1 means faster than any FP64 tensor-core step"},
                "gpu_launches_per_step": rep["kernel_launches"] / steps}
         # one batched adjoint step on batch 0, device-resident K: engine vs the reference's wdl_batch
         Ah = oracle.col_softmax(A0)
@@ -1075,6 +1106,26 @@ class StreamWorkload:
                               "INT8 tensor cores (wdl.int8 default)",
                "engine_fp64_tensor_ms": dmma_ms,
                "max_rel_diff_int8_vs_fp64_tensor": float(np.abs(full_gA - dmma_gA).max() / np.abs(dmma_gA).max())}
+        # the INT8 GEMM launches of one adjoint step, each bracketed by CUDA events
+        # in the engine (option profile.gemm), against cuBLASLt's INT8 GEMM
+        L.rwig_set_option(b"profile.gemm", 1.0)
+        try:
+            engine_step()
+            torch.cuda.synchronize()
+            grep = rw.last_report()
+        finally:
+            L.rwig_set_option(b"profile.gemm", float("nan"))
+        i8_peak = measured_i8gemm_tops(dev)
+        if grep["gemm_launches"] > 0:
+            ops = 24.0 * wl.step_flops()  # 24 residue planes per emulated FP64 product, unpadded sizes
+            ach = ops / (grep["gemm_ms"] / 1e3) / 1e12
+            adj["int8_gemm_roofline"] = {
+                "kernel": "i8_gemm (ozaki.cu)", "bound": "tensor", "launches": grep["gemm_launches"],
+                "ms_per_launch": grep["gemm_ms"] / grep["gemm_launches"], "share_of_step": grep["gemm_ms"] / eng_ms,
+                "achieved": ach, "unit": "TOP/s", "peak": i8_peak,
+                "frac": (ach / i8_peak) if i8_peak else None,
+                "ops_per_launch": ops / grep["gemm_launches"],
+                "peak_source": "measured cuBLASLt INT8 GEMM (torch._int_mm 8192^3) on this GPU; nominal 4500 TOP/s"}
         # checkpointed adjoint (wdl.checkpoint = k): history footprint and step time
         NW, ND = N * S * B * 8, N * B * 8
         ck = {}

@@ -57,6 +57,9 @@ typedef struct rwig_report {
   int support_n;         /* columns kept after dropping zero-mass entries of b */
   double bary_norm;      /* barycenters: sum of the un-normalised barycenter b */
   double grad_ms;        /* Sinkhorn with withgrad: device time of the backward launch */
+  double gemm_ms;        /* with option "profile.gemm" = 1: summed device time of the
+                            call's INT8 tensor-core GEMM launches (CUDA events) */
+  int gemm_launches;     /* those launches (0 when the timer was off) */
 } rwig_report;
 
 /* ---- context ---------------------------------------------------------- */
@@ -100,9 +103,9 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       modular integer products and CRT reconstruction), else on the FP64
  *       tensor cores; 2 on the INT8 tensor cores whenever N <= 8192; 0
  *       always on the FP64 tensor cores;
- *   "wdl.halves": 2 (default) runs the two halves of the document batch of
- *       an INT8-path WDL gradient on two streams (same gradient bits), 1 on
- *       one stream;
+ *   "wdl.halves": 2 runs the two halves of the document batch of an
+ *       INT8-path WDL gradient on two streams (same gradient bits), 1
+ *       (default) on one stream;
  *   "oz.tile_m": rows per tile of the INT8 GEMM: 256 (default; one
  *       accumulator per CTA) or 128 (two accumulators, the MMAs of one tile
  *       beside the epilogue of the last);
@@ -112,6 +115,9 @@ RWIG_API int rwig_last_report(rwig_report* out); /* report of the last call on t
  *       products; ceil(L/k) + 4k + 3 history slots of N x S D doubles
  *       instead of 4 (L + 1)); 0 (default) or k >= L keeps every
  *       iteration;
+ *   "profile.gemm": 1 brackets each INT8 tensor-core GEMM launch of a call
+ *       with CUDA events and reports their summed duration
+ *       (rwig_report.gemm_ms, gemm_launches); 0 (default) off;
  *   "dgemm.kshape", "dgemm.tile": DMMA instruction shape (k = 4, 8 or 16)
  *       and tile height (0 automatic, 64, 128) of rwig_selftest_dgemm only;
  *   "barycenter.log_path": the log barycenter's route: 0 (default) the

@@ -55,6 +55,8 @@ class Report(ctypes.Structure):
         ("support_n", _i),
         ("bary_norm", _d),
         ("grad_ms", _d),
+        ("gemm_ms", _d),
+        ("gemm_launches", _i),
     ]
 
     def as_dict(self):

@@ -58,7 +58,7 @@ const char* const kOptionNames[] = {"log_sinkhorn.scaled", "log_sinkhorn.tau", "
                                    "batch.strip_kb", "batch.max_team", "batch.redundant_rows",
                                    "batch.l2_keep_mb", "batch.max_elems", "batch.resident_team",
                                    "batch.stream_strip_kb", "batch.backfill_us",
-                                   "wdl.infer_docs", "wdl.checkpoint", "wdl.int8", "wdl.halves", "dgemm.kshape", "dgemm.tile", "barycenter.log_path", "oz.tile_m"};
+                                   "wdl.infer_docs", "wdl.checkpoint", "wdl.int8", "wdl.halves", "dgemm.kshape", "dgemm.tile", "barycenter.log_path", "oz.tile_m", "profile.gemm"};
 }  // namespace
 
 double option(const char* name, double dflt) {
@@ -80,6 +80,38 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 rwig_report& report() { return t_report; }
+
+int gemm_timer_begin(Context* ctx) {
+  ctx->gemm_ev_used = 0;
+  ctx->gemm_timing = option("profile.gemm", 0.0) == 1.0;
+  if (ctx->gemm_timing && ctx->gemm_ev.empty()) {
+    ctx->gemm_ev.resize(2 * Context::kTimedGemms, nullptr);
+    for (cudaEvent_t& e : ctx->gemm_ev) RWIG_CUDA_TRY(cudaEventCreate(&e));
+  }
+  return 0;
+}
+
+bool gemm_timer_mark(Context* ctx, cudaStream_t st) {
+  if (!ctx->gemm_timing || ctx->gemm_ev_used >= (int)ctx->gemm_ev.size()) return false;
+  return cudaEventRecord(ctx->gemm_ev[ctx->gemm_ev_used++], st) == cudaSuccess;
+}
+
+void gemm_timer_end(Context* ctx, double* ms_out, int* n_out) {
+  double ms = 0.0;
+  int n = 0;
+  for (int k = 0; ctx->gemm_timing && k + 1 < ctx->gemm_ev_used; k += 2) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ctx->gemm_ev[k], ctx->gemm_ev[k + 1]) == cudaSuccess) {
+      ms += t;
+      ++n;
+    }
+  }
+  (void)cudaGetLastError();
+  *ms_out = ms;
+  *n_out = n;
+  ctx->gemm_timing = false;
+  ctx->gemm_ev_used = 0;
+}
 
 void reset_report() {
   std::memset(&t_report, 0, sizeof(t_report));
@@ -161,6 +193,7 @@ extern "C" void rwig_shutdown(void) {
     cudaEventDestroy(c->evs1);
     cudaEventDestroy(c->evfork);
     cudaEventDestroy(c->evjoin);
+    for (cudaEvent_t e : c->gemm_ev) cudaEventDestroy(e);
     for (cudaStream_t& q : c->side)
       if (q) {
         cudaStreamSynchronize(q);

@@ -40,6 +40,12 @@ struct Context {
   // first use (under mu) and destroyed by rwig_shutdown
   static constexpr int kSideStreams = 8;
   cudaStream_t side[kSideStreams] = {};
+  // GEMM launch timer (option "profile.gemm"): event pairs around each
+  // tensor-core GEMM launch of a call, created on first use
+  static constexpr int kTimedGemms = 512;
+  std::vector<cudaEvent_t> gemm_ev;
+  int gemm_ev_used = 0;
+  bool gemm_timing = false;
 };
 
 // Returns the context of the current (or first) device, initialising it on
@@ -50,6 +56,15 @@ Context* get_context();
 // first use (the caller holds ctx->mu with the device current); nullptr on
 // failure.
 cudaStream_t side_stream(Context* ctx, int i);
+
+// GEMM timer of a call: gemm_timer_begin() arms it when option
+// "profile.gemm" is 1; gemm_timer_mark() records an event on `st` (before and
+// after each timed launch); gemm_timer_end() (after the timed work has
+// completed) returns the summed launch durations and their count, and
+// disarms the timer.
+int gemm_timer_begin(Context* ctx);
+bool gemm_timer_mark(Context* ctx, cudaStream_t st);
+void gemm_timer_end(Context* ctx, double* ms, int* launches);
 
 // Grow-only scratch slot `k` of at least `bytes`; nullptr on failure.
 void* scratch(Context* ctx, int k, size_t bytes);

@@ -194,21 +194,6 @@ __global__ void exp_rows(const double* K, long long ldk, int n, int* alpha) {
   }
 }
 
-// e[j] from max_k |X[k + j ldx]| (columns), one block per column.
-__global__ void exp_cols(const double* X, long long ldx, int Kd, int* e) {
-  __shared__ double sh[256];
-  const int j = blockIdx.x;
-  double mx = 0.0;
-  for (int k = threadIdx.x; k < Kd; k += blockDim.x) mx = fmax(mx, fabs(X[k + (long long)j * ldx]));
-  sh[threadIdx.x] = mx;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) e[j] = scale_exp(sh[0]);
-}
-
 // trunc(|x| 2^sc) (< 2^100) as five 20-bit chunks; false for x = 0.
 __device__ __forceinline__ bool chunks_scaled(double x, int sc, unsigned (&ch)[kChunks]) {
   const unsigned long long bits = (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
@@ -248,21 +233,36 @@ __device__ __forceinline__ unsigned residue_chunks(const unsigned (&ch)[kChunks]
   return (neg && r) ? p - r : r;
 }
 
-// Row r of the operand is column r of src (A(r, k) = src[k + r ld]):
-// out[t][r][k] for r < rows_pad, k < Kpad (zero outside rows x Kd).  Each
-// thread takes 4 consecutive k and stores one 32-bit word per modulus.
-__global__ void __launch_bounds__(256) res_cols(const double* src, long long ld, int Kd, int rows, const int* ex,
-                                                int Kpad, int rows_pad, Mods m, int8_t* out) {
-  const int r = blockIdx.y;
+// Row r of the operand is column r of src (A(r, k) = src[k + r ld]): one
+// block per row finds the row's largest magnitude, stores its exponent
+// ex[r] (r < rows), then writes out[t][r][k] for k < Kpad (zero outside rows
+// x Kd), each thread 4 consecutive k as one 32-bit word per modulus.
+__global__ void __launch_bounds__(256) res_cols(const double* __restrict__ src, long long ld, int Kd, int rows,
+                                                int* __restrict__ ex, int Kpad, int rows_pad, Mods m,
+                                                int8_t* __restrict__ out) {
+  __shared__ double red[256 / 32];
+  const int r = blockIdx.x;
+  const double* col = src + (long long)r * ld;
+  double mx = 0.0;
+  if (r < rows)
+    for (int k = threadIdx.x; k < Kd; k += blockDim.x) mx = fmax(mx, fabs(col[k]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  mx = red[0];
+#pragma unroll
+  for (int w = 1; w < 256 / 32; ++w) mx = fmax(mx, red[w]);
+  const int sc = scale_exp(mx);
+  if (threadIdx.x == 0 && r < rows) ex[r] = sc;
   const size_t plane4 = (size_t)rows_pad * Kpad / 4;
-  const int sc = r < rows ? ex[r] : 0;
-  for (int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x); k0 < Kpad; k0 += 4 * gridDim.x * blockDim.x) {
+  for (int k0 = 4 * threadIdx.x; k0 < Kpad; k0 += 4 * blockDim.x) {
     unsigned ch[4][kChunks];
     bool ng[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int k = k0 + q;
-      const double x = (r < rows && k < Kd) ? src[k + (long long)r * ld] : 0.0;
+      const double x = (r < rows && k < Kd) ? col[k] : 0.0;
       chunks_scaled(x, sc, ch[q]);
       ng[q] = x < 0.0;
     }
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) i8_gemm(const __grid_const
       tc_fence_after();
       const int i = m0 + h * kTileM + lq * 32 + lane;  // output row
       const unsigned p = RAW ? 1u : (unsigned)g.m.p[z];
-      const double invp = RAW ? 1.0 : g.m.invp[z];
+      const unsigned mg = RAW ? 1u : g.m.mg[z];
       const uint32_t acc = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(256 * (b + h));
       for (int c = cfirst; c < g.ntile; c += cstep) {
         uint32_t v[32];
@@ -528,11 +528,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1) i8_gemm(const __grid_const
           const int d = (int)v[q];
           if (RAW) {
             g.raw[(size_t)j * g.Mpad + i] = d;
-          } else {
-            int r = d - (int)floor((double)d * invp) * (int)p;
-            if (r < 0) r += (int)p;
-            if (r >= (int)p) r -= (int)p;
-            g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)r;
+          } else {  // 0 <= d < Kpad 255^2 < 2^31: one Barrett step in integer arithmetic
+            g.cres[((size_t)z * g.Wpad + j) * g.Mpad + i] = (uint8_t)bmod((unsigned)d, p, mg);
           }
         }
       }
@@ -593,7 +590,7 @@ int pick_ntile(int W) { return std::min(256, round_up(std::max(W, 16), 16)); }
 enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_ERR, SO_TA, SO_TB, SO_TD };
 // per-lane scratch of the product pipeline: lanes are products in flight on
 // different streams at once
-enum { SO_LANE = 420, SO_BRES = 0, SO_BETA, SO_CRES, SO_Y, SO_PER_LANE = 4 };
+enum { SO_LANE = 420, SO_BRES = 0, SO_BETA, SO_CRES, SO_PER_LANE = 3 };
 int lane_slot(int lane, int k) { return SO_LANE + SO_PER_LANE * lane + k; }
 
 // The kT (or, RAW, one) planes of A (Mpad x Kpad) and B (Wpad x Kpad): the
@@ -624,6 +621,7 @@ int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad
   static bool attr[2] = {false, false};
   const int ntn = Wpad / ntile, ntm = Mpad / MT, tiles = ntn * ntm * planes;
   const int grid = std::min(tiles, ctx->sm_count);  // persistent: one CTA per SM
+  const bool timed = gemm_timer_mark(ctx, st);
   if (MT == 256) {
     if (!attr[0]) {
       RWIG_CUDA_TRY(cudaFuncSetAttribute(i8_gemm<RAW, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
@@ -638,6 +636,7 @@ int launch_i8(Context* ctx, const int8_t* A, int Mpad, const int8_t* B, int Wpad
     i8_gemm<RAW, 128><<<grid, kPersistThreads, kGemmSmem, st>>>(ta, tb, g, ntn, ntm, planes);
   }
   RWIG_CUDA_TRY(cudaGetLastError());
+  if (timed) gemm_timer_mark(ctx, st);
   return 0;
 }
 
@@ -684,10 +683,8 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
   res_rows<<<dim3(pr->Kpad / 32, pr->Mpad / 32), dim3(32, 8), 0, st>>>(K, ldk, n, pr->alpha[0], pr->Kpad, pr->Mpad, m,
                                                                         pr->ares[0]);
   // trans = 1: columns of K
-  exp_cols<<<n, 256, 0, st>>>(K, ldk, n, pr->alpha[1]);
-  res_cols<<<dim3((pr->Kpad / 4 + 255) / 256, pr->Mpad), 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m,
-                                                                    pr->ares[1]);
-  if (launches) *launches += 4;
+  res_cols<<<pr->Mpad, 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m, pr->ares[1]);
+  if (launches) *launches += 3;
   RWIG_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -702,107 +699,13 @@ int products(Context* ctx, const Prepared& pr, int trans, const double* X, long 
   uint8_t* cr = (uint8_t*)scratch(ctx, lane_slot(lane, SO_CRES), (size_t)kT * Wpad * pr.Mpad);
   if (!bres || !be || !cr) return RWIG_E_NOMEM;
   const Mods m = mods_of(crt_constants());
-  exp_cols<<<W, 256, 0, st>>>(X, ldx, pr.Kd, be);
-  res_cols<<<dim3((pr.Kpad / 4 + 255) / 256, Wpad), 256, 0, st>>>(X, ldx, pr.Kd, W, be, pr.Kpad, Wpad, m, bres);
+  res_cols<<<Wpad, 256, 0, st>>>(X, ldx, pr.Kd, W, be, pr.Kpad, Wpad, m, bres);
   if (int rc = launch_i8<false>(ctx, pr.ares[trans], pr.Mpad, bres, Wpad, pr.Kpad, ntile, kT, cr, nullptr, st)) return rc;
-  if (launches) *launches += 3;
+  if (launches) *launches += 2;
   *cres = cr;
   *beta = be;
   *Wpad_out = Wpad;
   return 0;
-}
-
-// The signed fraction held in eight 32-bit limb sums (carries pending, top
-// limb first in significance), as |s| and its sign.
-__device__ __forceinline__ double limbs_to_fraction(const unsigned long long (&acc)[8], int l0, bool& neg) {
-  unsigned limb[8];
-  unsigned long long carry = 0ull;
-#pragma unroll
-  for (int l = 0; l < 8; ++l) {
-    const unsigned long long x = (l >= l0 ? acc[l] : 0ull) + carry;
-    limb[l] = (unsigned)x;
-    carry = x >> 32;
-  }
-  neg = (limb[7] >> 31) != 0;  // the fraction read in [-1/2, 1/2)
-  if (neg) {                     // two's complement negation of the 256-bit value
-    unsigned long long b = 1ull;
-#pragma unroll
-    for (int l = 0; l < 8; ++l) {
-      const unsigned long long x = (unsigned long long)(~limb[l]) + b;
-      limb[l] = (unsigned)x;
-      b = x >> 32;
-    }
-  }
-  return ldexp((double)(((unsigned long long)limb[7] << 32) | limb[6]), -64) +
-         ldexp((double)(((unsigned long long)limb[5] << 32) | limb[4]), -128) +
-         ldexp((double)(((unsigned long long)limb[3] << 32) | limb[2]), -192);
-}
-
-// Reconstruction (one thread per two consecutive rows of one column): the
-// 256-bit fraction frac(sum_t c_t e_t / P) is accumulated as eight 32-bit
-// limb sums in 64-bit registers (each below 24 * 255 * 2^32 < 2^45, so the
-// carries wait until the end) and read as a signed fraction s; Y = s P
-// 2^-(alpha + beta).  Fast path: the four upper limbs alone.  The lower ones
-// add less than 24 * 255 * 2^-128 < 2^-115 to s, which is within 2^-55 of
-// |s| once |s| >= 2^-60; smaller values are recomputed with all eight.
-__global__ void __launch_bounds__(256) crt_store(Crt c, const uint8_t* __restrict__ cres, int Mpad, int Wpad,
-                                                 const int* __restrict__ alpha, const int* __restrict__ beta, int Mo,
-                                                 int W, double* __restrict__ Y, long long ldy) {
-  const int npairs = (Mo + 1) / 2;
-  const size_t plane2 = (size_t)Wpad * Mpad / 2;  // plane stride in 16-bit words
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)npairs * W;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int i0 = (int)(e % npairs) * 2, j = (int)(e / npairs);
-    const unsigned short* q = reinterpret_cast<const unsigned short*>(cres + (size_t)j * Mpad + i0);
-    unsigned long long acc[2][8];
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-      for (int l = 0; l < 8; ++l) acc[u][l] = 0ull;
-#pragma unroll 4
-    for (int t = 0; t < kT; ++t) {
-      const unsigned w = __ldg(q + t * plane2);
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const unsigned ct = (w >> (8 * u)) & 0xffu;
-#pragma unroll
-        for (int l = 4; l < 8; ++l) acc[u][l] += (unsigned long long)ct * c.F32[t][l];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int i = i0 + u;
-      if (i >= Mo) break;
-      bool neg;
-      double mag = limbs_to_fraction(acc[u], 4, neg);
-      if (mag < 0x1p-60) {  // small: the lower limbs matter
-        unsigned long long full[8];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) full[l] = 0ull;
-        for (int t = 0; t < kT; ++t) {
-          const unsigned ct = (__ldg(q + t * plane2) >> (8 * u)) & 0xffu;
-#pragma unroll
-          for (int l = 0; l < 8; ++l) full[l] += (unsigned long long)ct * c.F32[t][l];
-        }
-        mag = limbs_to_fraction(full, 0, neg);
-      }
-      Y[(long long)i + (long long)j * ldy] = ldexp(neg ? -mag * c.P : mag * c.P, -(alpha[i] + beta[j]));
-    }
-  }
-}
-
-int reconstruct(Context* ctx, const Prepared& pr, int trans, const uint8_t* cres, int Wpad, const int* beta, int W,
-                double* Y, long long ldy, cudaStream_t st, int* launches) {
-  const long long n = (long long)((pr.Mo + 1) / 2) * W;
-  const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx->sm_count));
-  crt_store<<<grid, 256, 0, st>>>(crt_constants(), cres, pr.Mpad, Wpad, pr.alpha[trans], beta, pr.Mo, W, Y, ldy);
-  if (launches) ++*launches;
-  RWIG_CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-double* product_buffer(Context* ctx, size_t doubles, int lane) {
-  return (double*)scratch(ctx, lane_slot(lane, SO_Y), sizeof(double) * doubles);
 }
 
 // Bounded-wait status of the last products() launches (a host read).
@@ -855,7 +758,12 @@ extern "C" int rwig_selftest_ozaki(const double* K, long long ldk, int trans, in
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
   oz::Prepared pr;
   int launches = 0;
+  reset_report();
+  if (int rc = gemm_timer_begin(ctx)) return rc;
   if (int rc = oz::prepare(ctx, K, ldk, n, &pr, st, &launches)) return rc;
   if (int rc = oz::gemm(ctx, pr, trans, X, ldx, W, oz::kCrtCols, dg::EpiStore{Y, ldy, W}, st, &launches)) return rc;
-  return oz::status(ctx, st);
+  const int rc = oz::status(ctx, st);
+  gemm_timer_end(ctx, &report().gemm_ms, &report().gemm_launches);
+  report().kernel_launches = launches;
+  return rc;
 }

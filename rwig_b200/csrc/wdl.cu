@@ -570,11 +570,12 @@ int batch_grad(Context* ctx, cudaStream_t st, double* gA, double* gl, const doub
   const int k = (kopt <= 0 || kopt >= L) ? L : kopt;  // segment length
   const int nseg = (L + k - 1) / k;
   const int ngrp = (N + 7) / 8;
-  // With the products on the INT8 tensor cores the batch's documents run as
-  // two independent halves on two streams, so that one half's tensor-core
-  // products overlap the other half's residue, reconstruction and epilogue
-  // kernels (the documents of a batch share nothing until the final means).
-  const int halves = (pr && D >= 2 && (int)option("wdl.halves", 2.0) >= 2) ? 2 : 1;
+  // Option wdl.halves = 2 runs the batch's documents as two independent
+  // halves on two streams (the documents of a batch share nothing until the
+  // final means), for one half's tensor-core products to overlap the other
+  // half's residue and reconstruction kernels; one stream is the default,
+  // measured as fast on the 5000-word batch.
+  const int halves = (pr && D >= 2 && (int)option("wdl.halves", 1.0) >= 2) ? 2 : 1;
   // segment buffers, local index t = l - j k (t = 0..k); V's slot 0 is the checkpoint
   double* Us = (double*)scratch(ctx, SW_UH, sizeof(double) * NW * (k + 1));
   double* Vs = (double*)scratch(ctx, SW_VH, sizeof(double) * NW * (k + 1));
@@ -708,6 +709,7 @@ int batch_grad_entry(Context* ctx, cudaStream_t st, double* gA, double* gl, cons
   if (mode != 0 && mode != 1) return set_error(RWIG_E_INVALID, "mode must be 0 (K given) or 1 (C given)");
   if (mode == 1 && (!(reg > 0.0) || !std::isfinite(reg))) return set_error(RWIG_E_INVALID, "reg must be > 0");
   if (L < 0) return set_error(RWIG_E_INVALID, "L must be >= 0");
+  if ((rc = gemm_timer_begin(ctx))) return rc;
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
   double* K = nullptr;
   long long ldk = 0;
@@ -729,6 +731,7 @@ int batch_grad_entry(Context* ctx, cudaStream_t st, double* gA, double* gl, cons
   R.device_ms = ms;
   R.kernel_ms = ms;
   R.kernel_launches = launches;
+  gemm_timer_end(ctx, &R.gemm_ms, &R.gemm_launches);
   return 0;
 }
 
@@ -832,11 +835,13 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   RWIG_CUDA_TRY(cudaMemsetAsync(vA, 0, sizeof(double) * NS, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(mL, 0, sizeof(double) * SM, st));
   RWIG_CUDA_TRY(cudaMemsetAsync(vL, 0, sizeof(double) * SM, st));
+  int rc = gemm_timer_begin(ctx);  // training GEMMs only
+  if (rc) return rc;
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
   int launches = 0;
   double* K = nullptr;
   long long ldk = 0;
-  int rc = make_k(ctx, st, dC, N, reg, 1, &K, &ldk);  // K = exp(-C/reg) (wdl_impl.cpp:297)
+  rc = make_k(ctx, st, dC, N, reg, 1, &K, &ldk);  // K = exp(-C/reg) (wdl_impl.cpp:297)
   if (rc) return rc;
   oz::Prepared pr;  // K's residue planes, once for the whole training and inference
   const bool i8 = use_int8(ctx, N);
@@ -874,6 +879,9 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   if (i8 && (rc = oz::status(ctx, st))) return rc;
   float train_ms = 0.f;
   cudaEventElapsedTime(&train_ms, ctx->ev0, ctx->ev1);
+  double gemm_ms = 0.0;
+  int gemm_n = 0;
+  gemm_timer_end(ctx, &gemm_ms, &gemm_n);
   if (A) RWIG_CUDA_TRY(cudaMemcpyAsync(A, dA, sizeof(double) * NS, cudaMemcpyDeviceToHost, st));
   if (W) RWIG_CUDA_TRY(cudaMemcpyAsync(W, dW, sizeof(double) * SM, cudaMemcpyDeviceToHost, st));
   RWIG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -902,5 +910,7 @@ extern "C" int rwig_wdl(double* A, double* W, double* Yhat, const double* Y, con
   R.device_ms = train_ms;
   R.kernel_ms = train_ms;
   R.kernel_launches = launches;
+  R.gemm_ms = gemm_ms;
+  R.gemm_launches = gemm_n;
   return 0;
 }
