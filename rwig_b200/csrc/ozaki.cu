@@ -148,10 +148,11 @@ const Crt& crt_constants() {
 // ---------------------------------------------------------------------------
 // scaling exponents and residues
 // ---------------------------------------------------------------------------
-constexpr int kChunks = 5;  // 20-bit chunks of a scaled integer (100 bits >= kQ)
+constexpr int kChunks = 4;     // chunks of a scaled integer (88 bits >= kQ)
+constexpr int kChunkBits = 22;  // sum_b chunk_b w_b < 4 (2^22 - 1) 255 < 2^32
 
 // Per-modulus constants, passed by value (uniform across a launch): p, 1/p,
-// the reduction multiplier ceil(2^32 / p) and the chunk weights 2^(20 b) mod p.
+// the reduction multiplier ceil(2^32 / p) and the chunk weights 2^(22 b) mod p.
 struct Mods {
   int p[kT];
   double invp[kT];
@@ -169,7 +170,7 @@ Mods mods_of(const Crt& c) {
     unsigned long long v = 1 % p;
     for (int b = 0; b < kChunks; ++b) {
       m.w[t][b] = (unsigned)v;
-      v = (v << 20) % p;
+      v = (v << kChunkBits) % p;
     }
   }
   return m;
@@ -194,7 +195,7 @@ __global__ void exp_rows(const double* K, long long ldk, int n, int* alpha) {
   }
 }
 
-// trunc(|x| 2^sc) (< 2^100) as five 20-bit chunks; false for x = 0.
+// trunc(|x| 2^sc) (< 2^88) as four 22-bit chunks; false for x = 0.
 __device__ __forceinline__ bool chunks_scaled(double x, int sc, unsigned (&ch)[kChunks]) {
   const unsigned long long bits = (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
   if (bits == 0) {
@@ -213,17 +214,16 @@ __device__ __forceinline__ bool chunks_scaled(double x, int sc, unsigned (&ch)[k
     lo = sh > -64 ? mant >> -sh : 0ull;
     hi = 0ull;
   }
-  const unsigned m20 = (1u << 20) - 1;
-  ch[0] = (unsigned)lo & m20;
-  ch[1] = (unsigned)(lo >> 20) & m20;
-  ch[2] = (unsigned)(lo >> 40) & m20;
-  ch[3] = (unsigned)((lo >> 60) | (hi << 4)) & m20;
-  ch[4] = (unsigned)(hi >> 16) & m20;
+  const unsigned m22 = (1u << kChunkBits) - 1;
+  ch[0] = (unsigned)lo & m22;
+  ch[1] = (unsigned)(lo >> 22) & m22;
+  ch[2] = (unsigned)((lo >> 44) | (hi << 20)) & m22;
+  ch[3] = (unsigned)(hi >> 2) & m22;
   return true;
 }
 
 // Residue in [0, p_t) of the chunked integer, negated modulo p_t for x < 0:
-// sum_b ch_b (2^(20 b) mod p) < 5 2^28 fits 32 bits; one Barrett reduction.
+// sum_b ch_b (2^(22 b) mod p) < 4 (2^22 - 1) 255 < 2^32; one Barrett reduction.
 __device__ __forceinline__ unsigned residue_chunks(const unsigned (&ch)[kChunks], bool neg, const Mods& m, int t) {
   unsigned s = 0;
 #pragma unroll
