@@ -46,6 +46,11 @@ struct Context {
   std::vector<cudaEvent_t> gemm_ev;
   int gemm_ev_used = 0;
   bool gemm_timing = false;
+  // the K whose INT8 residue planes the scratch holds (oz::prepare_reuse):
+  // its size and leading dimension, valid while no other prepare ran
+  bool oz_kept = false;
+  int oz_kept_n = 0;
+  long long oz_kept_ldk = 0;
 };
 
 // Returns the context of the current (or first) device, initialising it on

@@ -587,7 +587,7 @@ int make_map(CUtensorMap* map, const void* base, int Kpad, int rows, int planes,
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 int pick_ntile(int W) { return std::min(256, round_up(std::max(W, 16), 16)); }
 
-enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_ERR, SO_TA, SO_TB, SO_TD };
+enum { SO_ARES0 = 400, SO_ARES1, SO_ALPHA0, SO_ALPHA1, SO_ERR, SO_TA, SO_TB, SO_TD, SO_KKEEP, SO_KDIFF };
 // per-lane scratch of the product pipeline: lanes are products in flight on
 // different streams at once
 enum { SO_LANE = 420, SO_BRES = 0, SO_BETA, SO_CRES, SO_PER_LANE = 3 };
@@ -662,7 +662,17 @@ int check_err(Context* ctx, cudaStream_t st) {
 
 bool available(Context* ctx) { return ctx && ctx->smem_optin >= (int)kGemmSmem && encode_fn() != nullptr; }
 
+// Counts the positions where a and b differ bitwise (n doubles), into *diff.
+__global__ void count_diff(const unsigned long long* __restrict__ a, const unsigned long long* __restrict__ b,
+                           long long n, unsigned* diff) {
+  unsigned d = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    d |= (unsigned)(__ldcs(a + i) != __ldcs(b + i));
+  if (__syncthreads_or(d) && threadIdx.x == 0) atomicOr(diff, 1u);
+}
+
 int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches) {
+  ctx->oz_kept = false;  // the residue planes are about to hold another K
   if (n < 1 || n > kMaxKd) return set_error(RWIG_E_UNSUPPORTED, "INT8 product path: size above 8192");
   if (!available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 product path unavailable on this device");
   pr->K = K;
@@ -686,6 +696,45 @@ int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, c
   res_cols<<<pr->Mpad, 256, 0, st>>>(K, ldk, n, n, pr->alpha[1], pr->Kpad, pr->Mpad, m, pr->ares[1]);
   if (launches) *launches += 3;
   RWIG_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int prepare_reuse(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches) {
+  if (n < 1 || n > kMaxKd) return set_error(RWIG_E_UNSUPPORTED, "INT8 product path: size above 8192");
+  const long long len = ldk * (long long)n;
+  double* keep = (double*)scratch(ctx, SO_KKEEP, sizeof(double) * (size_t)len);
+  unsigned* diff = (unsigned*)scratch(ctx, SO_KDIFF, sizeof(unsigned) * 4);
+  if (!keep || !diff) return RWIG_E_NOMEM;
+  if (ctx->oz_kept && ctx->oz_kept_n == n && ctx->oz_kept_ldk == ldk) {
+    RWIG_CUDA_TRY(cudaMemsetAsync(diff, 0, sizeof(unsigned), st));
+    const int grid = (int)std::max<long long>(1, std::min<long long>((len + 255) / 256, 4LL * ctx->sm_count));
+    count_diff<<<grid, 256, 0, st>>>(reinterpret_cast<const unsigned long long*>(K),
+                                     reinterpret_cast<const unsigned long long*>(keep), len, diff);
+    RWIG_CUDA_TRY(cudaGetLastError());
+    if (launches) ++*launches;
+    unsigned h = 1;
+    RWIG_CUDA_TRY(cudaMemcpyAsync(&h, diff, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    RWIG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h == 0) {  // the same K, bit for bit: its residue planes are still in the scratch
+      pr->K = K;
+      pr->ldk = ldk;
+      pr->Mo = pr->Kd = n;
+      pr->Mpad = round_up(n, kCtaM);
+      pr->Kpad = round_up(n, kKpadTo);
+      const size_t planes = (size_t)kT * pr->Mpad * pr->Kpad;
+      for (int tr = 0; tr < 2; ++tr) {
+        pr->ares[tr] = (int8_t*)scratch(ctx, SO_ARES0 + tr, planes);
+        pr->alpha[tr] = (int*)scratch(ctx, SO_ALPHA0 + tr, sizeof(int) * n);
+        if (!pr->ares[tr] || !pr->alpha[tr]) return RWIG_E_NOMEM;
+      }
+      return reset_err(ctx, st);
+    }
+  }
+  if (int rc = prepare(ctx, K, ldk, n, pr, st, launches)) return rc;
+  RWIG_CUDA_TRY(cudaMemcpyAsync(keep, K, sizeof(double) * (size_t)len, cudaMemcpyDeviceToDevice, st));
+  ctx->oz_kept = true;
+  ctx->oz_kept_n = n;
+  ctx->oz_kept_ldk = ldk;
   return 0;
 }
 

@@ -80,6 +80,13 @@ struct Prepared {
 // failures status() reports.  Returns 0 or an engine error.
 int prepare(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st, int* launches);
 
+// prepare(), unless the scratch already holds the residue planes of a K equal
+// to this one bit for bit (compared against a device copy of the K they were
+// made from: one read of both, a host synchronisation); then only the
+// sequence's error word is reset.
+int prepare_reuse(Context* ctx, const double* K, long long ldk, int n, Prepared* pr, cudaStream_t st,
+                  int* launches);
+
 // X's residues and the kT integer products: cres[t][j][i] = (A_t X_t)_ij mod
 // p_t for i < Mo, j < W (pitch Mpad per column, Wpad columns per modulus),
 // beta (W ints), in the scratch of `lane` (products on different streams at

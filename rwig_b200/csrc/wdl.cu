@@ -718,7 +718,7 @@ int batch_grad_entry(Context* ctx, cudaStream_t st, double* gA, double* gl, cons
   int launches = 1;
   oz::Prepared pr;
   const bool i8 = use_int8(ctx, N) && L > 0;
-  if (i8 && (rc = oz::prepare(ctx, K, ldk, N, &pr, st, &launches))) return rc;
+  if (i8 && (rc = oz::prepare_reuse(ctx, K, ldk, N, &pr, st, &launches))) return rc;
   rc = batch_grad(ctx, st, gA, gl, A, Wb, Yb, K, ldk, N, S, D, L, &launches, i8 ? &pr : nullptr);
   if (rc) return rc;
   if (i8 && (rc = oz::status(ctx, st))) return rc;

@@ -185,6 +185,38 @@ def test_batch_grad_on_int8_tensor_cores_matches_oracle(N, D, S, L):
     assert np.array_equal(again[0], gA) and np.array_equal(again[1], gl)
 
 
+def test_int8_residues_reused_only_for_the_same_K():
+    """The K residue planes of the last INT8-path call are reused only when
+    the new K equals it bit for bit: the same K skips the preparation (fewer
+    launches, the same bits); a K with one row changed, or a K differing in a
+    single last bit, is prepared anew (its gradient is its own)."""
+    N, D, S, L, reg = 300, 4, 6, 3, 0.1
+    Y, C, K, A, W = _batch(N, D, S, 8, reg, salt=17)
+    K2 = K.copy()
+    K2[5, :] *= 0.9
+    K3 = K.copy()
+    K3[N - 1, N - 1] = np.nextafter(K3[N - 1, N - 1], 2.0)
+    with _Option("wdl.int8", 2):
+        g1 = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        n1 = rw.last_report()["kernel_launches"]
+        g1b = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        n1b = rw.last_report()["kernel_launches"]
+        g2 = rw.wdl_batch_grad(A, W, Y, K2, reg, L, mode=0)
+        n2 = rw.last_report()["kernel_launches"]
+        g3 = rw.wdl_batch_grad(A, W, Y, K3, reg, L, mode=0)
+        n3 = rw.last_report()["kernel_launches"]
+        g1c = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        n1c = rw.last_report()["kernel_launches"]
+    assert np.array_equal(g1[0], g1b[0]) and np.array_equal(g1[1], g1b[1])
+    assert np.array_equal(g1[0], g1c[0]) and np.array_equal(g1[1], g1c[1])
+    assert n1b < n1 and n2 > n1b and n3 > n1b and n1c > n1b
+    ref2 = oracle.wdl_batch_grad(A, W, Y, K2, L)
+    assert rel_err(g2[0], ref2[0]) <= PARITY_TOL and rel_err(g2[1], ref2[1]) <= PARITY_TOL
+    ref3 = oracle.wdl_batch_grad(A, W, Y, K3, L)
+    assert rel_err(g3[0], ref3[0]) <= PARITY_TOL
+    assert not np.array_equal(g2[0], g1[0])
+
+
 def test_training_and_inference_on_int8_tensor_cores():
     N, M, S, B, L, reg = 150, 10, 3, 4, 6, 0.1
     Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=71)
