@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--s", type=int, default=32, help="histograms / topics (barycenter, wdl --single)")
     ap.add_argument("--l2-hot", type=float, default=None, help="engine option log_sinkhorn.l2_hot")
+    ap.add_argument("--stream-profile", action="store_true",
+                    help="with --single --workload stream: one batched call over the whole 200-request stream "
+                         "with engine option batch.profile (per-class phase times on stderr)")
     return ap.parse_args()
 
 
@@ -1506,6 +1509,24 @@ def run_single(args):
         rep = rw.last_report()
         print(json.dumps({"m": args.m, "n": args.n, "iter": r["iter"], "device_ms": rep["device_ms"],
                           "grad_ms": rep["grad_ms"], "launches": rep["kernel_launches"]}))
+        return 0
+    if args.workload == "stream" and args.stream_profile:
+        from rwig_b200 import _lib
+        dev = torch.device("cuda", 0)
+        L = _lib.load()
+        wl = WORKLOADS["stream"]
+        data = wl.build(dev)
+        probs, res = wl.problems(data), (_lib.Result * len(data))()
+        sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, len(data), res, sp))  # sizes the scratch
+        torch.cuda.synchronize()
+        L.rwig_set_option(b"batch.profile", 1.0)
+        try:
+            _lib.check(L.rwig_batch_sinkhorn_log_dev(probs, len(data), res, sp))
+            torch.cuda.synchronize()
+        finally:
+            L.rwig_set_option(b"batch.profile", float("nan"))
+        print(json.dumps({"problems": len(data), "device_ms": rw.last_report()["sweep_ms"]}))
         return 0
     if args.workload == "stream":
         # two batched calls of --iters fixed iterations: one streamed 2048 x 2048

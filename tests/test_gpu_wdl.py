@@ -217,6 +217,28 @@ def test_int8_residues_reused_only_for_the_same_K():
     assert not np.array_equal(g2[0], g1[0])
 
 
+def test_int8_options_keep_the_gradient_bits():
+    """wdl.halves = 2 (the batch's two document halves on two streams) and
+    oz.tile_m = 128 (the double-buffered GEMM) change scheduling only: the
+    same gradient bits.  profile.gemm = 1 times every INT8 GEMM launch of the
+    call and reports them."""
+    N, D, S, L, reg = 400, 6, 8, 3, 0.1
+    Y, C, K, A, W = _batch(N, D, S, 8, reg, salt=23)
+    with _Option("wdl.int8", 2):
+        base = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        with _Option("wdl.halves", 2):
+            halves = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        with _Option("oz.tile_m", 128):
+            tiles = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+        with _Option("profile.gemm", 1):
+            timed = rw.wdl_batch_grad(A, W, Y, K, reg, L, mode=0)
+            rep = rw.last_report()
+    for got in (halves, tiles, timed):
+        assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1])
+    assert rep["gemm_launches"] == 4 * L - 1 and rep["gemm_ms"] > 0.0
+    assert rep["gemm_ms"] < rep["device_ms"]
+
+
 def test_training_and_inference_on_int8_tensor_cores():
     N, M, S, B, L, reg = 150, 10, 3, 4, 6, 0.1
     Y, C, A0, L0 = synth.wdl_config(V=N, M=M, S=S, dim=5, salt=71)
