@@ -700,7 +700,10 @@ class WdlWorkload:
         roof = {"bound": "tensor", "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
                 "frac": achieved / tf_peak, "traffic": None,
                 "peak_source": "measured cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
-                "kernel": "dgemm_kernel with fused WDL epilogues (whole step, device time)",
+                "kernel": "the whole step (device time): products emulated on the INT8 tensor cores "
+                          "(i8_gemm, res_cols, crt_tiles with fused WDL epilogues)",
+                "note": "FP64-equivalent rate: the step's products counted as FP64 GEMM flops over the FP64 "
+                        "tensor-core peak; frac > 1 means faster than any FP64 tensor-core step",
                 "flops_per_step": self.step_flops(), "products_per_step": self.products()}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
