@@ -892,8 +892,14 @@ class StreamWorkload:
         elems = [d["q"]["m"] * d["q"]["n"] for d in data]
         alg = sum((bres[i]["iter"] + 2) * elems[i] * 8.0 for i in range(R))
         achieved = alg / (batch_ms / 1e3) / 1e9
+        # DRAM bytes of one service_kernel launch over this stream, from a single-pass
+        # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
+        # `bench.py --single --workload stream --stream-profile`: 297.99 GB read, 7.51 GB
+        # written in 119.94 ms (the stream and its iteration counts are deterministic)
+        traffic = 297.99e9 + 7.51e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "peak_source": src,
+                "traffic": traffic, "traffic_unit": "bytes per launch (ncu, one capture)",
+                "dram_gbs_in_capture": traffic / 119.94e-3 / 1e9, "peak_source": src,
                 "kernel": "service_kernel (a team of CTAs per problem), whole batched call",
                 "alg_bytes_per_step": alg,
                 "note": "K read once per iteration plus the K build and final passes per request; strips of "
