@@ -283,6 +283,20 @@ RWIG_API int rwig_wdl_batch_grad(double* g_Alpha, double* g_lambda, const double
 RWIG_API int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const double* A,
                                      const double* W_B, const double* Y_B, const double* K_or_C, int N,
                                      int S, int D, double reg, int L, int mode, void* stream);
+/* One optimizer step of WDL training on device buffers, the step rwig_wdl
+ * takes after each batch (src/wdl_impl.cpp:332-336, inst/include/optimizer.hpp:72-99,
+ * src/cuda_optimizer.cu:64): Alpha (N x S) -= update(g_Alpha); every column
+ * of Lambda (S x M) -= update(g_lambda) (the batch's Lambda gradient applied
+ * to all documents, wdl_impl.cpp:246); then A = column softmax of Alpha and
+ * W = column softmax of Lambda.  opt 0 SGD, 1 Adam, 2 AdamW (gamma the
+ * decay); mA, vA (N x S) and mL, vL (S x M) are the moments (zero before the
+ * first step); step >= 1 counts the steps taken, for the bias corrections.
+ * With the same inputs every rank of a data-parallel run takes the same
+ * step (the data-parallel training of rwig_b200/api.py). */
+RWIG_API int rwig_wdl_update_dev(double* Alpha, double* Lambda, double* A, double* W, double* mA, double* vA,
+                                 double* mL, double* vL, const double* g_Alpha, const double* g_lambda, int N,
+                                 int S, int M, int opt, double eta, double gamma, double beta1, double beta2,
+                                 double eps, int step, void* stream);
 
 /* ---- batched log-Sinkhorn ---------------------------------------------
  * Many independent problems with the semantics of rwig_sinkhorn_log in one

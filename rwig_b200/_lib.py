@@ -124,6 +124,8 @@ SIGNATURES = {
                       _dp, _dp, _i]),
     "rwig_wdl_batch_grad": (_i, [_dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _i, _d, _i, _i]),
     "rwig_wdl_batch_grad_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _i, _i, _vp]),
+    "rwig_wdl_update_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _d, _d, _d, _d,
+                                 _d, _i, _vp]),
     "rwig_batch_sinkhorn_log": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result)]),
     "rwig_batch_sinkhorn_log_dev": (_i, [ctypes.POINTER(Problem), _i, ctypes.POINTER(Result), _vp]),
     "rwig_batch_barycenter_dev": (_i, [ctypes.POINTER(BaryProblem), _i, ctypes.POINTER(BaryResult), _vp]),

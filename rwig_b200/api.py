@@ -347,9 +347,15 @@ def wdl_batch_grad_dp_dev(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0, group=None
         raise ValueError("A (S, N), W_B (D, S), Y_B (D, N) and K_or_C (N, N) do not match")
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     lo, hi = rank * D // world, (rank + 1) * D // world
-    buf = torch.zeros(N * S + S, dtype=torch.float64, device=A.device)
-    st = stream if stream is not None else torch.cuda.current_stream(A.device)
-    st.wait_stream(torch.cuda.current_stream(A.device))  # buf zeroed, inputs written
+    caller = torch.cuda.current_stream(A.device)
+    st = stream if stream is not None else caller
+    if st.cuda_stream == 0:
+        # the engine reads a null stream as its own stream, unordered with torch's
+        # legacy default stream: run on a side stream joined to the caller's
+        st = torch.cuda.Stream(A.device)
+    with torch.cuda.stream(st):
+        st.wait_stream(caller)  # inputs written
+        buf = torch.zeros(N * S + S, dtype=torch.float64, device=A.device)
     if hi > lo:
         gA, gl = buf[:N * S], buf[N * S:]
         rc = _lib.load().rwig_wdl_batch_grad_dev(_ptr(gA), _ptr(gl), _ptr(A), _ptr(W_B[lo:hi]), _ptr(Y_B[lo:hi]),
@@ -358,10 +364,86 @@ def wdl_batch_grad_dp_dev(A, W_B, Y_B, K_or_C, reg=0.1, L=20, mode=0, group=None
         _lib.check(rc)
         with torch.cuda.stream(st):
             buf.mul_(float(hi - lo))
+    host_collective = dist.get_backend(group) == "gloo"  # gloo reduces CUDA tensors through host copies
+    if host_collective:
+        st.synchronize()  # the shard's gradient is complete before the host copy starts
     with torch.cuda.stream(st):
         dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+    if host_collective:
+        st.synchronize()  # the reduced buffer is back on the device before any later kernel reads it
+    with torch.cuda.stream(st):
         buf.div_(float(D))
+    if st.cuda_stream != caller.cuda_stream:
+        caller.wait_stream(st)  # the caller's later work sees the reduced gradient
+        buf.record_stream(caller)
     return buf[:N * S].view(S, N), buf[N * S:]
+
+
+def wdl_train_dp_dev(Y, C, S, reg=0.1, L=20, B=64, E=1, optimizer=1, eta=1e-3, gamma=0.01, beta1=0.9,
+                     beta2=0.999, eps=1e-8, Alpha0=None, Lambda0=None, max_steps=0, group=None):
+    """Data-parallel WDL training on device buffers (one process per GPU,
+    torch.distributed group), the training loop of rwig_wdl
+    (src/wdl_impl.cpp:254-340) with each batch's documents split over the
+    ranks: every rank computes its shard's gradient (rwig_wdl_batch_grad_dev,
+    C given, K built on the device and its INT8 residue planes reused across
+    batches), one all-reduce gives every rank the batch mean
+    (wdl_batch_grad_dp_dev), and every rank takes the same optimizer step and
+    softmaxes on the device (rwig_wdl_update_dev), so the parameters stay
+    identical on all ranks.  Y (N x M) and C (N x N) are host arrays or
+    column-major device tensors ((M, N), (N, N)); Alpha0 (N x S) and Lambda0
+    (S x M) the initial logits (required: the ranks must start equal).
+    Returns A (N x S) and W (S x M) as host arrays, like wdl_cpp."""
+    import torch
+    if Alpha0 is None or Lambda0 is None:
+        raise ValueError("Alpha0 and Lambda0 are required (every rank must start from the same logits)")
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def col_major(x, rows, cols):
+        if isinstance(x, torch.Tensor):
+            t = x.to(device=dev, dtype=torch.float64).contiguous()
+        else:
+            t = torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.float64).T)).to(dev)
+        if t.shape != (cols, rows):
+            raise ValueError(f"expected a {rows} x {cols} matrix")
+        return t
+
+    Alpha0 = np.asarray(Alpha0, dtype=np.float64)
+    N, S_ = Alpha0.shape
+    if S_ != S:
+        raise ValueError("Alpha0 must be N x S")
+    M = np.asarray(Lambda0).shape[1]
+    tY, tC = col_major(Y, N, M), col_major(C, N, N)
+    Al, La = col_major(Alpha0, N, S), col_major(Lambda0, S, M)
+    A, W = torch.empty_like(Al), torch.empty_like(La)
+    mA, vA, mL, vL = (torch.zeros_like(Al), torch.zeros_like(Al), torch.zeros_like(La), torch.zeros_like(La))
+    lib = _lib.load()
+    # one side stream for every engine call and torch operation of the loop (the
+    # engine reads a null stream handle as its own stream)
+    st = torch.cuda.Stream(dev)
+    st.wait_stream(torch.cuda.current_stream(dev))  # inputs copied
+    sp = ctypes.c_void_p(st.cuda_stream)
+    with torch.cuda.stream(st):
+        zero = torch.zeros(N * S + S, dtype=torch.float64, device=dev)
+    # A, W from the initial logits: a step with a zero gradient under SGD leaves them unchanged
+    _lib.check(lib.rwig_wdl_update_dev(_ptr(Al), _ptr(La), _ptr(A), _ptr(W), None, None, None, None, _ptr(zero),
+                                       _ptr(zero[N * S:]), N, S, M, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 1, sp))
+    batches = -(-M // B)
+    steps = 0
+    for _ in range(E):
+        for bi in range(batches):
+            if max_steps > 0 and steps >= max_steps:
+                break
+            b0 = bi * B
+            D = (M % B) if (bi == M // B) else B  # src/wdl_impl.cpp:91
+            with torch.cuda.stream(st):
+                gA, gl = wdl_batch_grad_dp_dev(A, W[b0:b0 + D], tY[b0:b0 + D], tC, reg, L, mode=1, group=group,
+                                               stream=st)
+            steps += 1
+            _lib.check(lib.rwig_wdl_update_dev(_ptr(Al), _ptr(La), _ptr(A), _ptr(W), _ptr(mA), _ptr(vA), _ptr(mL),
+                                               _ptr(vL), _ptr(gA), _ptr(gl), N, S, M, int(optimizer), float(eta),
+                                               float(gamma), float(beta1), float(beta2), float(eps), steps, sp))
+    torch.cuda.synchronize(dev)
+    return {"A": A.cpu().numpy().T.copy(), "W": W.cpu().numpy().T.copy(), "steps": steps}
 
 
 def _cost_or_points(q):

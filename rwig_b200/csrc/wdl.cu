@@ -750,6 +750,33 @@ extern "C" int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const 
                                K_or_C, N, S, D, reg, L, mode);
 }
 
+extern "C" int rwig_wdl_update_dev(double* Alpha, double* Lambda, double* A, double* W, double* mA, double* vA,
+                                   double* mL, double* vL, const double* g_Alpha, const double* g_lambda, int N,
+                                   int S, int M, int opt, double eta, double gamma, double beta1, double beta2,
+                                   double eps, int step, void* stream) {
+  reset_report();
+  if (!Alpha || !Lambda || !A || !W || !g_Alpha || !g_lambda || (opt != 0 && (!mA || !vA || !mL || !vL)))
+    return set_error(RWIG_E_INVALID, "null pointer argument");
+  if (N < 1 || S < 1 || M < 1 || step < 1) return set_error(RWIG_E_INVALID, "N, S, M and step must be >= 1");
+  if (opt < 0 || opt > 2) return set_error(RWIG_E_INVALID, "opt must be 0 (SGD), 1 (Adam) or 2 (AdamW)");
+  Context* ctx = get_context();
+  if (!ctx) return RWIG_E_NODEVICE;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const long long NS = (long long)N * S, SM = (long long)S * M;
+  // the same bias corrections and kernels as the training loop of rwig_wdl
+  const double c1 = 1.0 - std::pow(beta1, step), c2 = 1.0 - std::pow(beta2, step);
+  wdl::opt_step<<<wdl::grid_for(ctx, NS), wdl::TPB, 0, st>>>(Alpha, mA, vA, g_Alpha, 0, NS, opt, eta, gamma, beta1,
+                                                            beta2, eps, c1, c2);
+  wdl::opt_step<<<wdl::grid_for(ctx, SM), wdl::TPB, 0, st>>>(Lambda, mL, vL, g_lambda, S, SM, opt, eta, gamma,
+                                                            beta1, beta2, eps, c1, c2);
+  wdl::col_softmax<<<S, wdl::TPB, 0, st>>>(Alpha, N, A);
+  wdl::col_softmax<<<M, wdl::TPB, 0, st>>>(Lambda, S, W);
+  RWIG_CUDA_TRY(cudaGetLastError());
+  report().kernel_launches = 4;
+  return 0;
+}
+
 extern "C" int rwig_wdl_batch_grad(double* g_Alpha, double* g_lambda, const double* A, const double* W_B,
                                    const double* Y_B, const double* K_or_C, int N, int S, int D, double reg, int L,
                                    int mode) {
