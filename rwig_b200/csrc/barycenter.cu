@@ -1007,7 +1007,7 @@ extern "C" int rwig_barycenter_parallel_dev(double* U, double* V, double* b, dou
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  return bary::run(ctx, stream ? (cudaStream_t)stream : ctx->stream, false, U, V, b, grad_A, grad_w, loss, iter,
+  return bary::run(ctx, call_stream(ctx, stream), false, U, V, b, grad_A, grad_w, loss, iter,
                    err, A, w, C, b_ext, M, N, S, reg, withgrad, max_iter, zero_tol);
 }
 
@@ -1018,7 +1018,7 @@ extern "C" int rwig_batch_barycenter_dev(const rwig_bary_problem* probs, int cou
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  return bary::run_batch(ctx, stream ? (cudaStream_t)stream : ctx->stream, probs, count, out);
+  return bary::run_batch(ctx, call_stream(ctx, stream), probs, count, out);
 }
 
 extern "C" int rwig_barycenter_log_dev(double* F, double* G, double* b, double* grad_A, double* grad_w,
@@ -1028,6 +1028,6 @@ extern "C" int rwig_barycenter_log_dev(double* F, double* G, double* b, double* 
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  return bary::run(ctx, stream ? (cudaStream_t)stream : ctx->stream, true, F, G, b, grad_A, grad_w, loss, iter,
+  return bary::run(ctx, call_stream(ctx, stream), true, F, G, b, grad_A, grad_w, loss, iter,
                    err, A, w, C, b_ext, M, N, S, reg, withgrad, max_iter, zero_tol);
 }

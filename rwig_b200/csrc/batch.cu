@@ -1591,7 +1591,7 @@ extern "C" int rwig_batch_sinkhorn_log_dev(const rwig_problem* probs, int count,
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   RWIG_CUDA_TRY(cudaEventRecord(ctx->ev0, st));
   const int rc = batch_device(ctx, st, probs, count, out);
   if (rc) return rc;

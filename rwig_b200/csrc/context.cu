@@ -43,6 +43,7 @@ int init_device(int dev, Context** out) {
     RWIG_CUDA_TRY(cudaEventCreate(&c->evs0));
     RWIG_CUDA_TRY(cudaEventCreate(&c->evs1));
     RWIG_CUDA_TRY(cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming));
+    RWIG_CUDA_TRY(cudaEventCreateWithFlags(&c->evlegacy, cudaEventDisableTiming));
     RWIG_CUDA_TRY(cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming));
     g_ctx[dev] = std::move(c);
   }
@@ -80,6 +81,14 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 rwig_report& report() { return t_report; }
+
+cudaStream_t call_stream(Context* ctx, void* stream) {
+  if (stream) return (cudaStream_t)stream;
+  if (cudaEventRecord(ctx->evlegacy, cudaStreamLegacy) == cudaSuccess)
+    (void)cudaStreamWaitEvent(ctx->stream, ctx->evlegacy, 0);
+  (void)cudaGetLastError();
+  return ctx->stream;
+}
 
 int gemm_timer_begin(Context* ctx) {
   ctx->gemm_ev_used = 0;
@@ -192,6 +201,7 @@ extern "C" void rwig_shutdown(void) {
     cudaEventDestroy(c->evs0);
     cudaEventDestroy(c->evs1);
     cudaEventDestroy(c->evfork);
+    cudaEventDestroy(c->evlegacy);
     cudaEventDestroy(c->evjoin);
     for (cudaEvent_t e : c->gemm_ev) cudaEventDestroy(e);
     for (cudaStream_t& q : c->side)

@@ -11,7 +11,7 @@ extern "C" int rwig_selftest_dgemm(const double* K, long long ldk, int trans, in
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!K || !X || !Y || Mo < 1 || Kd < 1 || S < 1 || ldy < Mo) return set_error(RWIG_E_INVALID, "bad arguments");
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   // dgemm.kshape: the DMMA instruction's k extent (4, 8 or 16); dgemm.tile:
   // the tile height (0 automatic, 64, 128) for this check
   const int km = (int)option("dgemm.kshape", (double)dg::kDmmaK);

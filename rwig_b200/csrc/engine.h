@@ -29,6 +29,7 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk = nullptr, evs0 = nullptr, evs1 = nullptr;
   cudaEvent_t evfork = nullptr, evjoin = nullptr;  // ordering only (no timing)
+  cudaEvent_t evlegacy = nullptr;                   // orders the engine's stream after the legacy default stream
   std::mutex mu;
   std::vector<void*> slots;
   std::vector<size_t> slot_bytes;
@@ -56,6 +57,12 @@ struct Context {
 // Returns the context of the current (or first) device, initialising it on
 // first use.  nullptr on failure (last error set).
 Context* get_context();
+
+// The stream a *_dev entry runs on: the caller's, or for a null handle the
+// engine's own stream, first made to wait for the work already queued on the
+// legacy default stream (the engine's stream is non-blocking, so nothing else
+// orders it after a caller that wrote the inputs there).
+cudaStream_t call_stream(Context* ctx, void* stream);
 
 // Side stream i (< Context::kSideStreams) of the context's device, created on
 // first use (the caller holds ctx->mu with the device current); nullptr on

@@ -776,7 +776,7 @@ extern "C" int rwig_selftest_i8gemm(const signed char* A, const signed char* B, 
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!oz::available(ctx)) return set_error(RWIG_E_UNSUPPORTED, "INT8 tensor-core GEMM unavailable");
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   const int ntile = oz::pick_ntile(N), Mpad = oz::round_up(M, oz::kCtaM), Npad = oz::round_up(N, ntile);
   const int Kpad = oz::round_up(Kd, oz::kKpadTo);
   int8_t* a = (int8_t*)scratch(ctx, oz::SO_TA, (size_t)Mpad * Kpad);
@@ -804,7 +804,7 @@ extern "C" int rwig_selftest_ozaki(const double* K, long long ldk, int trans, in
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   oz::Prepared pr;
   int launches = 0;
   reset_report();

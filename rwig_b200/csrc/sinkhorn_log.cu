@@ -1134,7 +1134,7 @@ extern "C" int rwig_sinkhorn_log_dev(double* P, double* grad_a, double* f, doubl
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   return sinkhorn_device(ctx, st, false, P, grad_a, f, g, loss, iter, err, a, b, C, M, N, reg, withgrad,
                          max_iter, zero_tol);
 }
@@ -1146,7 +1146,7 @@ extern "C" int rwig_sinkhorn_vanilla_dev(double* P, double* grad_a, double* u, d
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   return sinkhorn_device(ctx, st, true, P, grad_a, u, v, loss, iter, err, a, b, C, M, N, reg, withgrad,
                          max_iter, zero_tol);
 }

@@ -746,7 +746,7 @@ extern "C" int rwig_wdl_batch_grad_dev(double* g_Alpha, double* g_lambda, const 
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  return wdl::batch_grad_entry(ctx, stream ? (cudaStream_t)stream : ctx->stream, g_Alpha, g_lambda, A, W_B, Y_B,
+  return wdl::batch_grad_entry(ctx, call_stream(ctx, stream), g_Alpha, g_lambda, A, W_B, Y_B,
                                K_or_C, N, S, D, reg, L, mode);
 }
 
@@ -762,7 +762,7 @@ extern "C" int rwig_wdl_update_dev(double* Alpha, double* Lambda, double* A, dou
   Context* ctx = get_context();
   if (!ctx) return RWIG_E_NODEVICE;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = call_stream(ctx, stream);
   const long long NS = (long long)N * S, SM = (long long)S * M;
   // the same bias corrections and kernels as the training loop of rwig_wdl
   const double c1 = 1.0 - std::pow(beta1, step), c2 = 1.0 - std::pow(beta2, step);
