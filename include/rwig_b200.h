@@ -11,7 +11,9 @@
  *     or a negative RWIG_E_* code on failure, with a message in rwig_last_error().
  * Calls are blocking and serialised per device; they may be made from any host
  * thread.  Host-pointer entries copy inputs in and results out themselves; the
- * *_dev entries take device pointers (inputs resident in HBM) and a CUDA stream.
+ * *_dev entries take device pointers (inputs resident in HBM) and a CUDA stream
+ * (NULL: the engine's own stream, made to wait first for the work already
+ * queued on the legacy default stream).
  */
 #ifndef RWIG_B200_H
 #define RWIG_B200_H
