@@ -44,3 +44,29 @@ def test_input_validation(a, b, C, msg):
 def test_reg_must_be_scalar():
     with pytest.raises(ValueError, match="reg must be a single value"):
         rw.sinkhorn(np.ones(2) / 2, np.ones(2) / 2, np.eye(2), {"reg": [0.1, 0.2]})
+
+
+def test_dp_training_needs_common_initial_logits():
+    """Every rank must start from the same logits: the data-parallel training
+    refuses to draw them itself (checked before any device work)."""
+    import numpy as np
+    with pytest.raises(ValueError, match="Alpha0 and Lambda0"):
+        rw.wdl_train_dp_dev(np.ones((5, 3)), np.zeros((5, 5)), 2)
+
+
+def test_update_entry_validates_before_any_device_work(engine):
+    """rwig_wdl_update_dev rejects null buffers, sizes and step counts below 1
+    and unknown optimizers with RWIG_E_INVALID, without a GPU."""
+    import ctypes
+    buf = (ctypes.c_double * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    args = [p] * 10 + [2, 2, 2, 1, 1e-3, 0.01, 0.9, 0.999, 1e-8, 1, None]
+    bad = list(args)
+    bad[0] = None
+    assert engine.rwig_wdl_update_dev(*bad) == -1
+    bad = list(args)
+    bad[19] = 0  # step
+    assert engine.rwig_wdl_update_dev(*bad) == -1
+    bad = list(args)
+    bad[13] = 3  # optimizer
+    assert engine.rwig_wdl_update_dev(*bad) == -1
