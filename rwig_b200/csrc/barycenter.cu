@@ -698,7 +698,7 @@ int run(Context* ctx, cudaStream_t st, bool logdomain, double* X1, double* X2, d
     unsigned long long r;
     std::memcpy(&r, &reg, sizeof(r));
     for (unsigned long long v : {(unsigned long long)M, (unsigned long long)N, (unsigned long long)S, r,
-                                 (unsigned long long)withgrad, (unsigned long long)L})
+                                 (unsigned long long)withgrad, (unsigned long long)L, options_generation()})
       key.push_back(v);
   }
   const int site = logdomain ? kGraphBaryLog : kGraphBaryParallel;

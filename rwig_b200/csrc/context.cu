@@ -2,6 +2,7 @@
 // entry points of the C ABI.
 #include <cstdio>
 #include <cmath>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -217,6 +218,11 @@ extern "C" void rwig_shutdown(void) {
 
 extern "C" const char* rwig_last_error(void) { return t_last_error.c_str(); }
 
+namespace rwig {
+std::atomic<unsigned long long> g_opt_generation{0};
+unsigned long long options_generation() { return g_opt_generation.load(std::memory_order_relaxed); }
+}  // namespace rwig
+
 extern "C" int rwig_set_option(const char* name, double value) {
   if (!name) return set_error(RWIG_E_INVALID, "option name is null");
   for (const char* known : kOptionNames)
@@ -224,6 +230,7 @@ extern "C" int rwig_set_option(const char* name, double value) {
       std::lock_guard<std::mutex> lk(g_opt_mu);
       if (std::isnan(value)) g_opts.erase(name);  // back to the built-in default
       else g_opts[name] = value;
+      g_opt_generation.fetch_add(1, std::memory_order_relaxed);
       return 0;
     }
   return set_error(RWIG_E_INVALID, std::string("unknown option: ") + name);

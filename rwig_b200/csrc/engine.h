@@ -83,6 +83,9 @@ void* scratch(Context* ctx, int k, size_t bytes);
 
 // Engine options (rwig_set_option); unknown names return `dflt`.
 double option(const char* name, double dflt);
+// Count of rwig_set_option calls so far: part of the key of a captured launch
+// sequence, so that a sequence captured under other options is not replayed.
+unsigned long long options_generation();
 
 // Error / report plumbing (thread-local).
 int set_error(int code, const std::string& msg);
