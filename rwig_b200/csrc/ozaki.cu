@@ -111,7 +111,6 @@ Crt make_crt() {
   for (int t = 0; t < kT; ++t) {
     const uint32_t p = (uint32_t)mods[t];
     c.p[t] = (int)p;
-    c.invp[t] = 1.0 / (double)p;
     const Big Mt = div_small(P, p);
     const uint32_t mt = mod_small(Mt, p);
     uint32_t inv = 0;
@@ -151,11 +150,10 @@ const Crt& crt_constants() {
 constexpr int kChunks = 4;     // chunks of a scaled integer (88 bits >= kQ)
 constexpr int kChunkBits = 22;  // sum_b chunk_b w_b < 4 (2^22 - 1) 255 < 2^32
 
-// Per-modulus constants, passed by value (uniform across a launch): p, 1/p,
-// the reduction multiplier ceil(2^32 / p) and the chunk weights 2^(22 b) mod p.
+// Per-modulus constants, passed by value (uniform across a launch): p, the
+// reduction multiplier ceil(2^32 / p) and the chunk weights 2^(22 b) mod p.
 struct Mods {
   int p[kT];
-  double invp[kT];
   unsigned mg[kT];
   unsigned w[kT][kChunks];
 };
@@ -165,7 +163,6 @@ Mods mods_of(const Crt& c) {
   for (int t = 0; t < kT; ++t) {
     const unsigned long long p = (unsigned long long)c.p[t];
     m.p[t] = c.p[t];
-    m.invp[t] = c.invp[t];
     m.mg[t] = (unsigned)((0x100000000ull + p - 1) / p);
     unsigned long long v = 1 % p;
     for (int b = 0; b < kChunks; ++b) {

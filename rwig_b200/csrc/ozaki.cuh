@@ -56,7 +56,6 @@ constexpr int kCrtRowsPerThread = 2;
 // Reconstruction constants, passed by value to the kernels.
 struct Crt {
   int p[kT];
-  double invp[kT];
   unsigned F32[kT][8];  // floor(2^256 e_t / P), little-endian 32-bit limbs
   double P;                     // P rounded to double
 };
